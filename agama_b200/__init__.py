@@ -1,0 +1,146 @@
+"""agama_b200: a B200-native engine for Agama's orbit-and-action hot path.
+
+Python mirror of the parts of the reference's Python interface (src/interface_python.cpp) that
+sit on this path:
+
+    Potential(file=...) / Potential(type='Multipole', file=...)      agama.Potential
+        .potential(points), .force(points), .forceDeriv(points), .eval(...)
+    ActionFinder(potential)(points)                                   agama.ActionFinder
+    actions(potential, points, fd=...)                                agama.actions
+    orbit(potential=..., ic=..., time=..., Omega=..., accuracy=...)   agama.orbit
+
+Inputs may be numpy arrays (host; copied to the device and back) or CUDA tensors exposing
+__cuda_array_interface__ / torch tensors (device; processed in place on the current stream).
+All computation runs in the CUDA kernels of libagama_b200.so -- there is no CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import check, ptr
+
+__all__ = ["Potential", "ActionFinder", "actions", "orbit"]
+
+
+def _is_device_array(a):
+    return hasattr(a, "__cuda_array_interface__") or (hasattr(a, "is_cuda") and a.is_cuda)
+
+
+def _dev_ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.__cuda_array_interface__["data"][0])
+
+
+def _current_stream():
+    try:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    except Exception:
+        return None
+
+
+def _points(a, ncol):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    single = a.ndim == 1
+    a = a.reshape(-1, ncol)
+    return a, single
+
+
+class Potential:
+    """A Multipole potential resident on the current CUDA device.
+
+    Potential(file='coefs.ini')                     -- coefficient file of the reference format
+    Potential(type='Multipole', file='coefs.ini')
+    Potential(radii=r, Phi=P, dPhi=dP)              -- arrays as in Multipole(gridRadii, Phi, dPhi)
+    """
+
+    def __init__(self, file=None, type="Multipole", radii=None, Phi=None, dPhi=None):
+        L = _native.lib()
+        if file is not None:
+            params = "type=%s, file=%s" % (type, file)
+            h = L.agama_createPotential(params.encode())
+        elif radii is not None:
+            radii = np.ascontiguousarray(radii, dtype=np.float64)
+            Phi = np.ascontiguousarray(Phi, dtype=np.float64)
+            dPhi = np.ascontiguousarray(dPhi, dtype=np.float64)
+            if Phi.shape != dPhi.shape or Phi.shape[1] != len(radii):
+                raise ValueError("Phi and dPhi must have shape (numCoefs, len(radii))")
+            h = L.agama_createMultipoleFromCoefs(len(radii), ptr(radii), Phi.shape[0], ptr(Phi), ptr(dPhi))
+        else:
+            raise ValueError("Potential: give file=... or radii/Phi/dPhi arrays")
+        if not h:
+            raise RuntimeError("agama_b200: " + _native.error())
+        self._h = ctypes.c_void_p(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _native._lib is not None:
+            _native._lib.agama_deletePotential(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        v = [ctypes.c_int() for _ in range(5)]
+        check(_native.lib().agama_getPotentialInfo(self._h, *[ctypes.byref(x) for x in v]))
+        lmax, mmax, sym, nr, nt = (x.value for x in v)
+        return dict(lmax=lmax, mmax=mmax, symmetry=sym, gridSizeR=nr, gridSizeTau=nt)
+
+    # ---------------- evaluation ----------------
+    def eval(self, points, pot=True, acc=False, der=False):
+        """Potential, acceleration (-grad Phi) and/or Hessian (xx,yy,zz,xy,yz,zx) at points."""
+        if _is_device_array(points):
+            return self._eval_device(points, pot, acc, der)
+        p, single = _points(points, 3)
+        n = len(p)
+        phi = np.empty(n)
+        grad = np.empty((n, 3)) if (acc or der) else None
+        hess = np.empty((n, 6)) if der else None
+        check(_native.lib().agama_evalPotentialMany(self._h, n, ptr(p), 0.0, ptr(phi), ptr(grad), ptr(hess)))
+        out = []
+        if pot:
+            out.append(phi[0] if single else phi)
+        if acc:
+            out.append(-grad[0] if single else -grad)
+        if der:
+            out.append(hess[0] if single else hess)
+        return out[0] if len(out) == 1 else tuple(out)
+
+    def _eval_device(self, points, pot, acc, der):
+        import torch
+        p = points.contiguous().view(-1, 3)
+        n = p.shape[0]
+        phi = torch.empty(n, dtype=torch.float64, device=p.device)
+        grad = torch.empty((n, 3), dtype=torch.float64, device=p.device) if (acc or der) else None
+        hess = torch.empty((n, 6), dtype=torch.float64, device=p.device) if der else None
+        check(_native.lib().agama_evalPotentialManyDevice(
+            self._h, n, _dev_ptr(p), _dev_ptr(phi), _dev_ptr(grad), _dev_ptr(hess), _current_stream()))
+        out = []
+        if pot:
+            out.append(phi)
+        if acc:
+            out.append(-grad)
+        if der:
+            out.append(hess)
+        return out[0] if len(out) == 1 else tuple(out)
+
+    def potential(self, points):
+        return self.eval(points, pot=True)
+
+    def force(self, points):
+        return self.eval(points, pot=False, acc=True)
+
+    def forceDeriv(self, points):
+        """force and the derivatives of force (= minus the Hessian), as agama's forceDeriv"""
+        f, h = self.eval(points, pot=False, acc=True, der=True)
+        return f, -h
+
+
+from .actions import ActionFinder, actions  # noqa: E402,F401
+from .orbit import orbit  # noqa: E402,F401

@@ -1,0 +1,61 @@
+"""Loader of the engine's native library (agama_b200/_lib/libagama_b200.so) through ctypes.
+
+There is no CPU implementation behind this module: if the library is missing, importing the
+engine's classes raises immediately, and every compute call requires a CUDA device.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "_lib", "libagama_b200.so")
+
+D = ctypes.POINTER(ctypes.c_double)
+L = ctypes.POINTER(ctypes.c_long)
+I = ctypes.POINTER(ctypes.c_int)
+F = ctypes.POINTER(ctypes.c_float)
+VP = ctypes.c_void_p
+
+# name -> (restype, argtypes); kept in the order of include/agama_b200.h
+SIGNATURES = {
+    "agama_getError": (ctypes.c_char_p, []),
+    "agama_createPotential": (VP, [ctypes.c_char_p]),
+    "agama_deletePotential": (None, [VP]),
+    "agama_evalPotential": (ctypes.c_double, [VP, D, ctypes.c_double, D, D]),
+    "agama_createMultipoleFromCoefs": (VP, [ctypes.c_int, D, ctypes.c_int, D, D]),
+    "agama_getPotentialInfo": (ctypes.c_int, [VP, I, I, I, I, I]),
+    "agama_inspectMultipoleFile": (ctypes.c_int, [ctypes.c_char_p, I, I, I, I, I]),
+    "agama_evalPotentialMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
+    "agama_evalPotentialManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library, with argument types declared; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(
+                "agama_b200 native library not found at %s; build it with `python -m agama_b200.build`" % LIBPATH)
+        L_ = ctypes.CDLL(LIBPATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L_, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L_
+    return _lib
+
+
+def error():
+    return lib().agama_getError().decode()
+
+
+def check(rc):
+    if rc != 0:
+        raise RuntimeError("agama_b200: " + error())
+
+
+def ptr(a, t=D):
+    """ctypes pointer to a numpy array (None stays None)"""
+    return None if a is None else a.ctypes.data_as(t)

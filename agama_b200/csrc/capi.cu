@@ -1,0 +1,165 @@
+// C-ABI of the B200 engine: the entry points of the reference's plain-C interface
+// (src/interface_c.h) for the Multipole / orbit / Staeckel-fudge path, plus batched and
+// device-pointer variants.  No exception crosses this boundary: constructors return NULL and
+// batched calls return a non-zero status, with the message in agama_getError().
+#include "runtime.h"
+#include "../../include/agama_b200.h"
+#include <cstring>
+#include <sstream>
+#include <cctype>
+
+using namespace agb;
+
+struct agama_Potential { DevicePotential* pot; };
+
+namespace {
+
+std::string trimStr(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t"), b = s.find_last_not_of(" \t");
+    return a == std::string::npos ? "" : s.substr(a, b - a + 1);
+}
+std::string lowerStr(std::string s) { for(auto& c : s) c = static_cast<char>(tolower(c)); return s; }
+
+/// the subset of the reference's key=value potential parameters this engine accepts:
+/// "file=<Multipole coefficient file>" with an optional "type=Multipole"
+std::string coefFileFromParams(const char* params)
+{
+    if(!params) throw std::invalid_argument("createPotential: null parameter string");
+    std::stringstream ss(params);
+    std::string item, file, type;
+    while(std::getline(ss, item, ',')) {
+        size_t eq = item.find('=');
+        if(eq == std::string::npos) continue;
+        std::string key = lowerStr(trimStr(item.substr(0, eq))), val = trimStr(item.substr(eq + 1));
+        if(key == "file") file = val;
+        else if(key == "type") type = lowerStr(val);
+        else throw std::invalid_argument("createPotential: parameter '" + key +
+            "' is not supported by the B200 engine (supply a Multipole coefficient file)");
+    }
+    if(!type.empty() && type != "multipole")
+        throw std::invalid_argument("createPotential: only type=Multipole is supported");
+    if(file.empty())
+        throw std::invalid_argument("createPotential: no coefficient file given");
+    return file;
+}
+
+template<class F>
+int guarded(F&& f) {
+    try { f(); return 0; }
+    catch(std::exception& e) { setError(e.what()); return -1; }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* agama_getError() { return lastError(); }
+
+agama_Potential* agama_createPotential(const char* params)
+{
+    try {
+        std::vector<double> radii;
+        std::vector<std::vector<double>> Phi, dPhi;
+        readMultipoleCoefFile(coefFileFromParams(params), radii, Phi, dPhi);
+        return new agama_Potential{ createDevicePotential(radii, Phi, dPhi) };
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+agama_Potential* agama_createMultipoleFromCoefs(int gridSizeR, const double* radii, int numCoefs,
+    const double* Phi, const double* dPhi)
+{
+    try {
+        if(gridSizeR < 2 || numCoefs < 1 || !radii || !Phi || !dPhi)
+            throw std::invalid_argument("createMultipoleFromCoefs: invalid arguments");
+        std::vector<double> r(radii, radii + gridSizeR);
+        std::vector<std::vector<double>> P(numCoefs), D(numCoefs);
+        for(int c = 0; c < numCoefs; c++) {
+            P[c].assign(Phi + static_cast<size_t>(c) * gridSizeR, Phi + static_cast<size_t>(c + 1) * gridSizeR);
+            D[c].assign(dPhi + static_cast<size_t>(c) * gridSizeR, dPhi + static_cast<size_t>(c + 1) * gridSizeR);
+        }
+        return new agama_Potential{ createDevicePotential(r, P, D) };
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+void agama_deletePotential(agama_Potential* p)
+{
+    if(!p) return;
+    delete p->pot;
+    delete p;
+}
+
+int agama_getPotentialInfo(const agama_Potential* p, int* lmax, int* mmax, int* symmetry,
+    int* gridSizeR, int* gridSizeTau)
+{
+    return guarded([&] {
+        if(!p) throw std::invalid_argument("null potential");
+        const MultipoleHost& H = p->pot->host;
+        if(lmax) *lmax = H.ind.lmax;
+        if(mmax) *mmax = H.ind.mmax;
+        if(symmetry) *symmetry = H.ind.sym;
+        if(gridSizeR) *gridSizeR = static_cast<int>(H.radii.size());
+        if(gridSizeTau) *gridSizeTau = static_cast<int>(H.tau.size());
+    });
+}
+
+int agama_evalPotentialManyDevice(const agama_Potential* p, long n, const double* pos,
+    double* phi, double* deriv, double* deriv2, void* stream)
+{
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && !pos)) throw std::invalid_argument("evalPotentialManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        launchEvalPotential(p->pot->view, n, pos, phi, deriv, deriv2, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int agama_evalPotentialMany(const agama_Potential* p, long n, const double* pos, double time,
+    double* phi, double* deriv, double* deriv2)
+{
+    (void)time;   // the Multipole potential is static
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && !pos)) throw std::invalid_argument("evalPotentialMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        DevBuf<double> dpos(3 * n), dphi(n), dg(deriv ? 3 * n : 0), dh(deriv2 ? 6 * n : 0);
+        AGB_CUDA(cudaMemcpy(dpos.ptr, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+        launchEvalPotential(p->pot->view, n, dpos.ptr, dphi.ptr, dg.ptr, dh.ptr, 0);
+        if(phi) AGB_CUDA(cudaMemcpy(phi, dphi.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+        if(deriv) AGB_CUDA(cudaMemcpy(deriv, dg.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        if(deriv2) AGB_CUDA(cudaMemcpy(deriv2, dh.ptr, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        AGB_CUDA(cudaDeviceSynchronize());
+    });
+}
+
+double agama_evalPotential(const agama_Potential* p, const double pos[3], double time,
+    double deriv[3], double deriv2[6])
+{
+    double phi = NAN;
+    if(agama_evalPotentialMany(p, 1, pos, time, &phi, deriv, deriv2) != 0)
+        return NAN;
+    return phi;
+}
+
+}  // extern "C"
+
+extern "C" int agama_inspectMultipoleFile(const char* file, int* lmax, int* mmax, int* symmetry,
+    int* gridSizeR, int* gridSizeTau)
+{
+    // host-only: parse the file and build the tables without touching a device
+    return guarded([&] {
+        std::vector<double> radii;
+        std::vector<std::vector<double>> Phi, dPhi;
+        readMultipoleCoefFile(file ? file : "", radii, Phi, dPhi);
+        MultipoleHost H = buildMultipole(radii, Phi, dPhi);
+        if(lmax) *lmax = H.ind.lmax;
+        if(mmax) *mmax = H.ind.mmax;
+        if(symmetry) *symmetry = H.ind.sym;
+        if(gridSizeR) *gridSizeR = static_cast<int>(H.radii.size());
+        if(gridSizeTau) *gridSizeTau = static_cast<int>(H.tau.size());
+    });
+}

@@ -1,0 +1,97 @@
+// Multipole potential on the device: table upload and the batched evaluation kernel.
+#include "runtime.h"
+#include "multipole_eval.cuh"
+
+namespace agb {
+
+namespace {
+thread_local std::string g_error;
+
+/// One point per thread; 256 threads per block.  NQ = 1 (potential), 3 (+gradient), 6 (+Hessian).
+template<int NQ>
+__global__ void __launch_bounds__(256) evalPotentialKernel(const MultipoleView M, long n,
+    const double* __restrict__ pos, double* __restrict__ phi, double* __restrict__ grad,
+    double* __restrict__ hess)
+{
+    const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    if(i >= n) return;
+    const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    double p, g[3], h[6];
+    evalMultipoleCar<NQ>(M, x, y, z, &p, g, h);
+    if(phi) phi[i] = p;
+    if(NQ >= 3 && grad) { grad[3 * i] = g[0]; grad[3 * i + 1] = g[1]; grad[3 * i + 2] = g[2]; }
+    if(NQ == 6 && hess)
+        for(int k = 0; k < 6; k++) hess[6 * i + k] = h[k];
+}
+}  // namespace
+
+void setError(const std::string& msg) { g_error = msg; }
+const char* lastError() { return g_error.c_str(); }
+
+void requireDevice()
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if(e != cudaSuccess || count == 0)
+        throw std::runtime_error("no CUDA device available: the B200 engine has no CPU fallback");
+}
+
+void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
+    double* grad, double* hess, cudaStream_t stream)
+{
+    if(n <= 0) return;
+    const int block = 256;
+    const long grid = (n + block - 1) / block;
+    if(hess)
+        evalPotentialKernel<6><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess);
+    else if(grad)
+        evalPotentialKernel<3><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess);
+    else
+        evalPotentialKernel<1><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess);
+    AGB_CUDA(cudaGetLastError());
+}
+
+DevicePotential* createDevicePotential(const std::vector<double>& radii,
+    const std::vector<std::vector<double>>& Phi, const std::vector<std::vector<double>>& dPhi)
+{
+    requireDevice();
+    DevicePotential* P = new DevicePotential;
+    try {
+        AGB_CUDA(cudaGetDevice(&P->device));
+        P->host = buildMultipole(radii, Phi, dPhi);
+        const MultipoleHost& H = P->host;
+        P->lnr.upload(H.lnr);
+        P->tau.upload(H.tau);
+        P->spl2d.upload(H.spl2d);
+        P->spl1d.upload(H.spl1d);
+        P->innerS.upload(H.inner.S); P->innerU.upload(H.inner.U); P->innerW.upload(H.inner.W);
+        P->outerS.upload(H.outer.S); P->outerU.upload(H.outer.U); P->outerW.upload(H.outer.W);
+        MultipoleView& V = P->view;
+        V.ind = H.ind;
+        V.is2d = H.is2d;
+        // switching radii (reference src/potential_multipole.cpp:1538-1548, GRID_SAFETY_FACTOR = eps^(1/3))
+        const double gsf = 6.0554544523933395e-06;
+        V.rInnerSq = pow2(H.radii.front() * (1 + gsf));
+        V.rOuterSq = pow2(H.radii.back() * (1 - gsf));
+        V.nr = static_cast<int>(H.lnr.size());
+        V.lnr = P->lnr.ptr;
+        V.nt = static_cast<int>(H.tau.size());
+        V.tau = P->tau.ptr;
+        for(int i = 0; i < 2 * LMAX_MAX + 1; i++) V.splSlot[i] = H.splSlot[i];
+        V.spl2d = P->spl2d.ptr;
+        V.spl1d = P->spl1d.ptr;
+        V.logScaling = H.logScaling;
+        V.invPhi0 = H.invPhi0;
+        V.inner.ind = H.inner.ind; V.inner.r0sq = H.inner.r0sq; V.inner.inner = 1; V.inner.Q = H.inner.Q;
+        V.inner.S = P->innerS.ptr; V.inner.U = P->innerU.ptr; V.inner.W = P->innerW.ptr;
+        V.outer.ind = H.outer.ind; V.outer.r0sq = H.outer.r0sq; V.outer.inner = 0; V.outer.Q = H.outer.Q;
+        V.outer.S = P->outerS.ptr; V.outer.U = P->outerU.ptr; V.outer.W = P->outerW.ptr;
+        P->axisymmetric = (H.ind.sym & SYM_AXISYMMETRIC) == SYM_AXISYMMETRIC;
+    } catch(...) {
+        delete P;
+        throw;
+    }
+    return P;
+}
+
+}  // namespace agb

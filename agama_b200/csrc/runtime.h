@@ -1,0 +1,62 @@
+// Host runtime shared by the C-ABI entry points: error reporting, CUDA checks and the
+// device-resident objects behind the opaque handles.
+#pragma once
+#include <string>
+#include <stdexcept>
+#include <vector>
+#include <cuda_runtime.h>
+#include "multipole.h"
+
+namespace agb {
+
+/// last error message of the calling thread (the reference keeps one global string,
+/// src/interface_c.cpp:5-7; a per-thread string keeps concurrent callers apart)
+void setError(const std::string& msg);
+const char* lastError();
+
+#define AGB_CUDA(call) do { cudaError_t e_ = (call); if(e_ != cudaSuccess) \
+    throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call); } while(0)
+
+/// throws if no CUDA device is usable: the engine has no CPU fallback
+void requireDevice();
+
+/// device buffer (RAII)
+template<typename T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { if(ptr) cudaFree(ptr); }
+    void alloc(size_t count) {
+        if(ptr) { cudaFree(ptr); ptr = nullptr; }
+        n = count;
+        if(count) AGB_CUDA(cudaMalloc(&ptr, count * sizeof(T)));
+    }
+    void upload(const std::vector<T>& v) {
+        alloc(v.size());
+        if(!v.empty()) AGB_CUDA(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+};
+
+/// a Multipole potential resident on one device
+struct DevicePotential {
+    int device = 0;
+    MultipoleHost host;
+    DevBuf<double> lnr, tau, spl2d, spl1d, innerS, innerU, innerW, outerS, outerU, outerW;
+    MultipoleView view;
+    /// the axisymmetric (m = 0) part, used by the action finder (same as the full potential
+    /// when the potential is axisymmetric)
+    bool axisymmetric = false;
+};
+
+DevicePotential* createDevicePotential(const std::vector<double>& radii,
+    const std::vector<std::vector<double>>& Phi, const std::vector<std::vector<double>>& dPhi);
+
+/// launch helpers (defined in the .cu files)
+void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
+    double* grad, double* hess, cudaStream_t stream);
+
+}  // namespace agb

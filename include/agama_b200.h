@@ -1,0 +1,77 @@
+/* C-ABI of the B200 engine for Agama's Multipole / DOP853 orbit / Staeckel-fudge action path.
+
+   The first group of entry points has exactly the names, argument meaning and error behaviour
+   of the reference's plain-C interface (src/interface_c.h), so a C/C++/Fortran/ctypes caller
+   of that interface can link this library instead for the supported subset.  The remaining
+   entry points are batched (many points per call) and device-pointer variants that the
+   reference interface does not have; their comments name the reference routine each one
+   replaces when applied point by point.
+
+   Conventions: opaque handles are created by agama_create* and freed by agama_delete*;
+   constructors return NULL on error and batched calls return 0 on success or -1 on error;
+   the text of the last error of the calling thread is returned by agama_getError().
+   Arrays are row-major, double precision: positions n x 3 (x,y,z), phase-space points
+   n x 6 (x,y,z,vx,vy,vz), gradients n x 3, Hessians n x 6 (xx,yy,zz,xy,yz,zx).
+   *Device variants take device pointers and a cudaStream_t (as void*; NULL = default stream),
+   and return after enqueueing the work. */
+#ifndef AGAMA_B200_H
+#define AGAMA_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct agama_Potential agama_Potential;
+typedef struct agama_ActionFinder agama_ActionFinder;
+
+/* ---------------------------------------------------------------------------------------
+   Entry points with the reference's names and signatures (src/interface_c.h).            */
+
+/* reference: agama_getError, src/interface_c.h:20 (src/interface_c.cpp:25-28) */
+const char* agama_getError(void);
+
+/* reference: agama_createPotential, src/interface_c.h:45 (src/interface_c.cpp:31-51).
+   Accepts "file=<coefficient file>" (optionally with "type=Multipole"): a Multipole potential
+   stored by the reference's writePotential (src/potential_factory.cpp:909-930). */
+agama_Potential* agama_createPotential(const char* params);
+
+/* reference: agama_deletePotential, src/interface_c.h:51 */
+void agama_deletePotential(agama_Potential* potential);
+
+/* reference: agama_evalPotential, src/interface_c.h:77 (src/interface_c.cpp:68-90):
+   potential at pos, gradient into deriv[3] and Hessian into deriv2[6] when not NULL. */
+double agama_evalPotential(const agama_Potential* potential, const double pos[3], double time,
+    double deriv[3], double deriv2[6]);
+
+/* ---------------------------------------------------------------------------------------
+   Construction from arrays (reference: potential::Multipole(gridRadii, Phi, dPhi),
+   src/potential_multipole.cpp:1491-1516, the constructor behind the coefficient file).
+   radii[gridSizeR] increasing; Phi and dPhi are numCoefs x gridSizeR with the coefficient
+   index c = l*(l+1)+m, numCoefs = (lmax+1)^2. */
+agama_Potential* agama_createMultipoleFromCoefs(int gridSizeR, const double* radii, int numCoefs,
+    const double* Phi, const double* dPhi);
+
+/* order, symmetry (coord::SymmetryType bit mask) and grid sizes of a Multipole potential */
+int agama_getPotentialInfo(const agama_Potential* potential, int* lmax, int* mmax, int* symmetry,
+    int* gridSizeR, int* gridSizeTau);
+
+/* Host-only check of a coefficient file: parses it and builds the tables without a device
+   (reference: the parsing half of createPotential for type=Multipole,
+   src/potential_factory.cpp:725-746).  Returns 0 and the order / symmetry / grid sizes. */
+int agama_inspectMultipoleFile(const char* file, int* lmax, int* mmax, int* symmetry,
+    int* gridSizeR, int* gridSizeTau);
+
+/* Batched potential / gradient / Hessian at n points, host buffers (any output may be NULL).
+   Replaces n calls of agama_evalPotential (src/interface_c.cpp:68-90); the reference batches
+   the same call in Python, BatchFunction over BasePotential::eval (src/interface_python.cpp:1405-1485,
+   :3077-3104). */
+int agama_evalPotentialMany(const agama_Potential* potential, long n, const double* pos, double time,
+    double* phi, double* deriv, double* deriv2);
+
+/* The same on device buffers, enqueued on the given stream. */
+int agama_evalPotentialManyDevice(const agama_Potential* potential, long n, const double* pos,
+    double* phi, double* deriv, double* deriv2, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,314 @@
+// Flat C API over the reference Agama library, compiled from the reference sources into
+// oracle/_ref/libagama_ref.so.  TEST INFRASTRUCTURE ONLY: used by tests/, by the fixture
+// generator and by the CPU reference arm of bench.py -- never by the engine itself.
+//
+// Each loop mirrors the way the reference's own Python binding drives the library:
+//   potential / force : OpenMP dynamic chunks of 1024 points  (interface_python.cpp:1405-1485)
+//   orbits            : OpenMP schedule(dynamic,1) over orbits (interface_python.cpp:8101)
+//   actions           : OpenMP dynamic chunks of 64 points     (interface_python.cpp:3791-3822)
+// and calls the same library entry points:
+//   BasePotential::eval(PosCar)                 potential_base.h:153-156
+//   orbit::OrbitIntegrator<Car>::init/run       orbit.cpp:52-117
+//   actions::ActionFinderAxisymFudge::eval      actions_staeckel.cpp:954-979
+//   actions::evalAxisymFudge (fixed Delta)      actions_staeckel.cpp:683-693
+// The table-export functions read private members of the action finder so that the exact
+// focal-distance table and L_circ(E) spline used by the reference can be handed to tests.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <omp.h>
+// expose the private interpolation tables of the action finder (test code only)
+#define private public
+#define protected public
+#include "actions_staeckel.h"
+#include "potential_utils.h"
+#include "math_spline.h"
+#undef private
+#undef protected
+#include "potential_factory.h"
+#include "potential_base.h"
+#include "orbit.h"
+#include "coord.h"
+#include "utils.h"
+
+namespace {
+
+std::string g_error;
+
+void setThreads(int nthreads) { if(nthreads > 0) omp_set_num_threads(nthreads); }
+
+/// forwarding potential that counts evaluations (pattern of SPotential in the reference's
+/// tests/test_potential_expansions.cpp:289-302)
+class CountingPotential: public potential::BasePotential {
+public:
+    potential::PtrPotential pot;
+    mutable std::atomic<long long> count;
+    explicit CountingPotential(const potential::PtrPotential& p) : pot(p), count(0) {}
+    virtual coord::SymmetryType symmetry() const { return pot->symmetry(); }
+    virtual std::string name() const { return pot->name(); }
+protected:
+    virtual void evalCar(const coord::PosCar &pos, double* p, coord::GradCar* g, coord::HessCar* h, double t) const
+    { ++count; pot->eval(pos, p, g, h, t); }
+    virtual void evalCyl(const coord::PosCyl &pos, double* p, coord::GradCyl* g, coord::HessCyl* h, double t) const
+    { ++count; pot->eval(pos, p, g, h, t); }
+    virtual void evalSph(const coord::PosSph &pos, double* p, coord::GradSph* g, coord::HessSph* h, double t) const
+    { ++count; pot->eval(pos, p, g, h, t); }
+    virtual double densityCar(const coord::PosCar &pos, double t) const { return pot->density(pos, t); }
+    virtual double densityCyl(const coord::PosCyl &pos, double t) const { return pot->density(pos, t); }
+    virtual double densitySph(const coord::PosSph &pos, double t) const { return pot->density(pos, t); }
+};
+
+struct PotHandle { potential::PtrPotential pot; };
+struct AfHandle  { std::shared_ptr<CountingPotential> cnt; std::shared_ptr<actions::ActionFinderAxisymFudge> af; };
+
+/// runtime function counting accepted DOP853 steps
+class StepCounter: public orbit::BaseRuntimeFnc {
+public:
+    long* counter;
+    StepCounter(orbit::BaseOrbitIntegrator& o, long* c) : orbit::BaseRuntimeFnc(o), counter(c) {}
+    virtual bool processTimestep(double, double) { ++*counter; return true; }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_error() { return g_error.c_str(); }
+
+/// load a potential from an INI file (e.g. a Multipole coefficient file written by writePotential)
+void* ref_load_potential(const char* iniFile) {
+    try {
+        PotHandle* h = new PotHandle;
+        h->pot = potential::readPotential(iniFile);
+        return h;
+    } catch(std::exception& e) { g_error = e.what(); return NULL; }
+}
+
+/// create a potential from key=value parameters (as agama_createPotential does)
+void* ref_create_potential(const char* params) {
+    try {
+        PotHandle* h = new PotHandle;
+        h->pot = potential::createPotential(utils::KeyValueMap(std::string(params)));
+        return h;
+    } catch(std::exception& e) { g_error = e.what(); return NULL; }
+}
+
+int ref_write_potential(void* pot, const char* file) {
+    try { return potential::writePotential(file, *static_cast<PotHandle*>(pot)->pot) ? 0 : -1; }
+    catch(std::exception& e) { g_error = e.what(); return -1; }
+}
+
+void ref_free_potential(void* pot) { delete static_cast<PotHandle*>(pot); }
+
+/// potential, gradient (dPhi/dx) and optional Hessian (xx,yy,zz,xy,yz,zx) at n Cartesian points
+int ref_eval_many(void* handle, long n, const double* pos, double* phi, double* grad, double* hess, int nthreads) {
+    const potential::BasePotential& pot = *static_cast<PotHandle*>(handle)->pot;
+    setThreads(nthreads);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 1024)
+    for(long i = 0; i < n; i++) {
+        try {
+            double p; coord::GradCar g; coord::HessCar h;
+            pot.eval(coord::PosCar(pos[3*i], pos[3*i+1], pos[3*i+2]), &p, grad ? &g : NULL, hess ? &h : NULL);
+            if(phi) phi[i] = p;
+            if(grad) { grad[3*i] = g.dx; grad[3*i+1] = g.dy; grad[3*i+2] = g.dz; }
+            if(hess) { hess[6*i] = h.dx2; hess[6*i+1] = h.dy2; hess[6*i+2] = h.dz2;
+                       hess[6*i+3] = h.dxdy; hess[6*i+4] = h.dydz; hess[6*i+5] = h.dxdz; }
+        } catch(std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
+/// potential + gradient in cylindrical coordinates (R,z,phi) -> (Phi, dR, dz, dphi) and Hessian
+int ref_eval_cyl_many(void* handle, long n, const double* pos, double* phi, double* grad, double* hess) {
+    const potential::BasePotential& pot = *static_cast<PotHandle*>(handle)->pot;
+    try {
+        for(long i = 0; i < n; i++) {
+            double p; coord::GradCyl g; coord::HessCyl h;
+            pot.eval(coord::PosCyl(pos[3*i], pos[3*i+1], pos[3*i+2]), &p, grad ? &g : NULL, hess ? &h : NULL);
+            if(phi) phi[i] = p;
+            if(grad) { grad[3*i] = g.dR; grad[3*i+1] = g.dz; grad[3*i+2] = g.dphi; }
+            if(hess) { hess[6*i] = h.dR2; hess[6*i+1] = h.dz2; hess[6*i+2] = h.dphi2;
+                       hess[6*i+3] = h.dRdz; hess[6*i+4] = h.dzdphi; hess[6*i+5] = h.dRdphi; }
+        }
+    } catch(std::exception& e) { g_error = e.what(); return -1; }
+    return 0;
+}
+
+/// integrate n orbits with DOP853 (accuracy acc) for times T[i] in a frame rotating with Omega;
+/// output the final phase-space point, the number of accepted steps and a status
+/// (0 = reached T, 1 = stopped early: zero/non-finite step or maxSteps)
+int ref_orbits_many(void* handle, long n, const double* ic, const double* T, double Omega,
+    double accuracy, long maxSteps, double* final, long* nsteps, int* status, int nthreads)
+{
+    const potential::BasePotential& pot = *static_cast<PotHandle*>(handle)->pot;
+    setThreads(nthreads);
+    orbit::OrbitIntParams params(accuracy, maxSteps > 0 ? (size_t)maxSteps : (size_t)1e8);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 1)
+    for(long i = 0; i < n; i++) {
+        try {
+            long cnt = 0;
+            orbit::OrbitIntegrator<coord::Car> orbint(pot, Omega, params);
+            orbint.addRuntimeFnc(orbit::PtrRuntimeFnc(new StepCounter(orbint, &cnt)));
+            orbint.init(coord::PosVelCar(ic + 6*i));
+            coord::PosVelCar end = orbint.run(T[i]);
+            end.unpack_to(final + 6*i);
+            if(nsteps) nsteps[i] = cnt;
+            if(status) status[i] = 0;
+        } catch(std::exception& e) {
+            if(status) status[i] = -1;
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
+/// Staeckel-fudge actions with a given focal distance per point (Cartesian posvel input);
+/// if countEvals is not NULL, it receives the number of potential evaluations per point
+int ref_actions_fd_many(void* handle, long n, const double* posvel, const double* fd, double* act,
+    long long* countEvals, int nthreads)
+{
+    potential::PtrPotential base = static_cast<PotHandle*>(handle)->pot;
+    setThreads(nthreads);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 64)
+    for(long i = 0; i < n; i++) {
+        try {
+            CountingPotential cnt(base);
+            actions::Actions a;
+            actions::evalAxisymFudge(cnt, coord::toPosVelCyl(coord::PosVelCar(posvel + 6*i)), &a, NULL, NULL, fd[i]);
+            act[3*i] = a.Jr; act[3*i+1] = a.Jz; act[3*i+2] = a.Jphi;
+            if(countEvals) countEvals[i] = cnt.count;
+        } catch(std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
+/// Staeckel-fudge actions, angles and frequencies with a given focal distance (f1 outputs)
+int ref_actions_angles_fd_many(void* handle, long n, const double* posvel, const double* fd,
+    double* act, double* ang, double* freq, int nthreads)
+{
+    potential::PtrPotential base = static_cast<PotHandle*>(handle)->pot;
+    setThreads(nthreads);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 64)
+    for(long i = 0; i < n; i++) {
+        try {
+            actions::Actions a; actions::Angles t; actions::Frequencies f;
+            actions::evalAxisymFudge(*base, coord::toPosVelCyl(coord::PosVelCar(posvel + 6*i)),
+                act ? &a : NULL, ang ? &t : NULL, freq ? &f : NULL, fd[i]);
+            if(act)  { act[3*i] = a.Jr; act[3*i+1] = a.Jz; act[3*i+2] = a.Jphi; }
+            if(ang)  { ang[3*i] = t.thetar; ang[3*i+1] = t.thetaz; ang[3*i+2] = t.thetaphi; }
+            if(freq) { freq[3*i] = f.Omegar; freq[3*i+1] = f.Omegaz; freq[3*i+2] = f.Omegaphi; }
+        } catch(std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
+void* ref_actionfinder_create(void* handle) {
+    try {
+        AfHandle* h = new AfHandle;
+        h->cnt.reset(new CountingPotential(static_cast<PotHandle*>(handle)->pot));
+        h->af.reset(new actions::ActionFinderAxisymFudge(h->cnt, false));
+        h->cnt->count = 0;
+        return h;
+    } catch(std::exception& e) { g_error = e.what(); return NULL; }
+}
+
+void ref_actionfinder_free(void* af) { delete static_cast<AfHandle*>(af); }
+
+/// total number of potential evaluations made through the action finder since creation / reset
+long long ref_actionfinder_evalcount(void* af, int reset) {
+    AfHandle* h = static_cast<AfHandle*>(af);
+    long long c = h->cnt->count;
+    if(reset) h->cnt->count = 0;
+    return c;
+}
+
+int ref_actionfinder_many(void* handle, long n, const double* posvel, double* act, double* fdOut, int nthreads) {
+    const actions::ActionFinderAxisymFudge& af = *static_cast<AfHandle*>(handle)->af;
+    setThreads(nthreads);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 64)
+    for(long i = 0; i < n; i++) {
+        try {
+            coord::PosVelCyl p = coord::toPosVelCyl(coord::PosVelCar(posvel + 6*i));
+            actions::Actions a;
+            af.eval(p, &a);
+            act[3*i] = a.Jr; act[3*i+1] = a.Jz; act[3*i+2] = a.Jphi;
+            if(fdOut) fdOut[i] = af.focalDistance(p);
+        } catch(std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
+/// sizes of the action finder's tables: [sizeE, sizeL, nLofE, nRofL, nPhiofR]
+int ref_actionfinder_table_sizes(void* handle, long* sizes) {
+    const actions::ActionFinderAxisymFudge& af = *static_cast<AfHandle*>(handle)->af;
+    sizes[0] = af.interpD.xval.size();
+    sizes[1] = af.interpD.yval.size();
+    sizes[2] = af.interp.LofE.xval.size();
+    sizes[3] = af.interp.RofL.xval.size();
+    sizes[4] = af.interp.PhiofR.xval.size();
+    return 0;
+}
+
+/// copy the focal-distance table (grids in scaled E and scaled Lz/Lcirc, values sizeE x sizeL)
+/// and the Interpolator's LofE / RofL / PhiofR quintic splines (x, f, f', f'') plus scalars
+/// [invPhi0(finder), invPhi0(interp), slopeOut, coefOut, massOut]
+int ref_actionfinder_tables(void* handle, double* gridE, double* gridL, double* delta,
+    double* lofe, double* rofl, double* phiofr, double* scalars)
+{
+    const actions::ActionFinderAxisymFudge& af = *static_cast<AfHandle*>(handle)->af;
+    std::copy(af.interpD.xval.begin(), af.interpD.xval.end(), gridE);
+    std::copy(af.interpD.yval.begin(), af.interpD.yval.end(), gridL);
+    std::copy(af.interpD.fval.begin(), af.interpD.fval.end(), delta);
+    const math::QuinticSpline* spl[3] = { &af.interp.LofE, &af.interp.RofL, &af.interp.PhiofR };
+    double* out[3] = { lofe, rofl, phiofr };
+    for(int s = 0; s < 3; s++) {
+        size_t m = spl[s]->xval.size();
+        std::copy(spl[s]->xval.begin(),  spl[s]->xval.end(),  out[s]);
+        std::copy(spl[s]->fval.begin(),  spl[s]->fval.end(),  out[s] + m);
+        std::copy(spl[s]->fder.begin(),  spl[s]->fder.end(),  out[s] + 2*m);
+        std::copy(spl[s]->fder2.begin(), spl[s]->fder2.end(), out[s] + 3*m);
+    }
+    scalars[0] = af.invPhi0;
+    scalars[1] = af.interp.invPhi0;
+    scalars[2] = af.interp.slopeOut;
+    scalars[3] = af.interp.coefOut;
+    scalars[4] = af.interp.massOut;
+    return 0;
+}
+
+/// L_circ(E) through the reference Interpolator of the action finder
+int ref_actionfinder_lcirc(void* handle, long n, const double* E, double* L) {
+    const actions::ActionFinderAxisymFudge& af = *static_cast<AfHandle*>(handle)->af;
+    for(long i = 0; i < n; i++) L[i] = af.interp.L_circ(E[i]);
+    return 0;
+}
+
+}  // extern "C"

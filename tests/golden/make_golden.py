@@ -1,0 +1,110 @@
+"""Generate the golden fixtures of the parity tests from the reference implementation.
+
+Run here, where the reference sources exist and the oracle has been built (make -C oracle):
+
+    python tests/golden/make_golden.py [potentials|orbits|actions|all]
+
+It writes, into tests/golden/:
+  <name>.coef            Multipole coefficient files written by the reference (writePotential)
+                         for the benchmark potentials and a few extra cases (1-D path, spherical);
+  potential_<name>.npz   evaluation points (incl. edge cases) with the reference's potential,
+                         gradient and Hessian at them;
+  orbits_<name>.npz      initial conditions, integration times and the reference's final
+                         phase-space points, accepted step counts and statuses;
+  actions_<name>.npz     phase-space points with the reference's Staeckel-fudge actions (fixed
+                         focal distance and through ActionFinderAxisymFudge), plus the finder's
+                         focal-distance table and L_circ(E) spline.
+All inputs are synthetic and seeded (agama_b200/workloads.py); no external dataset is involved.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+
+from agama_b200 import workloads  # noqa: E402
+from oracle import ref  # noqa: E402
+
+# extra potentials exercising the other evaluation paths
+EXTRA_POTENTIALS = {
+    # lmax <= 2: per-(l,m) 1-D splines with the closed-form l<=2 transform
+    "quad": dict(density=dict(type="Dehnen", mass=1, scaleRadius=1, gamma=1.5, axisRatioY=0.7, axisRatioZ=0.5),
+                 lmax=2, gridSizeR=30, symmetry="triaxial"),
+    # spherical: lmax = 0
+    "sph": dict(density=dict(type="Plummer", mass=2, scaleRadius=0.7), lmax=0, gridSizeR=25),
+    # odd harmonics and m < 0 terms (no reflection symmetry): general inverse transform
+    "lop": dict(density=dict(type="Dehnen", mass=1, scaleRadius=1, gamma=1, axisRatioY=0.8, axisRatioZ=0.6,
+                             orientation=[0.3, 0.5, 0.2], center=[0.05, -0.02, 0.03]),
+                lmax=5, gridSizeR=40, symmetry="none"),
+}
+
+
+def build_reference_potential(spec):
+    """construct a Multipole from a density with the reference's Python interface"""
+    import agama
+    spec = dict(spec)
+    d = spec.pop("density")
+    comps = []
+    for x in (d if isinstance(d, list) else [d]):
+        x = dict(x)
+        if x["type"] in ("MiyamotoNagai", "NFW"):
+            comps.append(agama.Potential(**x))
+        else:
+            comps.append(agama.Density(**x))
+    dens = comps[0] if len(comps) == 1 else agama.Density(*comps)
+    return agama.Potential(type="Multipole", density=dens, **spec)
+
+
+def coef_path(name):
+    return os.path.join(HERE, name + ".coef")
+
+
+def make_potentials():
+    specs = {"cfg%d" % k: v for k, v in workloads.CONFIG_POTENTIALS.items()}
+    specs.update(EXTRA_POTENTIALS)
+    for name, spec in specs.items():
+        pot = build_reference_potential(spec)
+        pot.export(coef_path(name))
+        print("wrote", coef_path(name))
+
+
+def eval_points(coef, seed, n=1500):
+    """points spanning the inner asymptote, the spline region and the outer asymptote,
+    plus edge cases: on the z axis, in the equatorial plane, at the grid radii, near r=0"""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    with open(coef) as f:
+        rows = f.read().split("#Phi")[1].split("\n")[2:]
+    radii = np.array([float(r.split("\t")[0]) for r in rows if r.strip() and not r.startswith("#")][:1000])
+    radii = radii[: np.argmax(np.diff(radii) <= 0) + 1] if np.any(np.diff(radii) <= 0) else radii
+    rmin, rmax = radii[0], radii[-1]
+    r = np.exp(rng.uniform(np.log(rmin / 30), np.log(rmax * 30), size=n))
+    x = rng.normal(size=(n, 3))
+    x *= (r / np.linalg.norm(x, axis=1))[:, None]
+    edge = []
+    for rr in [rmin * 0.5, rmin, rmin * (1 + 1e-5), radii[1], radii[len(radii) // 2], rmax * (1 - 1e-5), rmax, rmax * 2]:
+        edge += [[rr, 0, 0], [0, 0, rr], [0, 0, -rr], [0, rr, 0], [-rr / 2, rr / 2, rr / np.sqrt(2)],
+                 [rr * 0.6, -rr * 0.8, 0]]
+    edge += [[1e-7, 2e-7, -1e-7], [1e5, -2e5, 3e5], [0.3, 0, 0.4], [-0.3, 0, 0.4], [0, -0.5, 1e-12]]
+    return np.vstack([x, np.array(edge, dtype=float)])
+
+
+def make_potential_vectors():
+    names = ["cfg%d" % k for k in workloads.CONFIG_POTENTIALS] + list(EXTRA_POTENTIALS)
+    for i, name in enumerate(names):
+        pot = ref.Potential(file=coef_path(name))
+        pts = eval_points(coef_path(name), seed=100 + i)
+        phi, grad, hess = pot.eval(pts, hess=True)
+        out = os.path.join(HERE, "potential_%s.npz" % name)
+        np.savez_compressed(out, points=pts, phi=phi, grad=grad, hess=hess)
+        print("wrote", out, len(pts))
+
+
+if __name__ == "__main__":
+    what = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if what in ("potentials", "all"):
+        make_potentials()
+        make_potential_vectors()
