@@ -43,7 +43,9 @@ def _compile(src, newest_header, verbose):
     if src.endswith(".cu"):
         cmd += CUDA_FLAGS
     else:
-        cmd += ["-x", "c++"] + ARCH
+        # host construction code: FMA contraction on, as in the reference's own -march builds,
+        # so that the spline tables come out identical to the reference's
+        cmd += ["-x", "c++", "-Xcompiler", "-march=x86-64-v3"] + ARCH
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -21,6 +21,9 @@ constexpr int LMAX_MAX = 16;
 /// number of doubles stored per node of a 2-D quintic spline (9 used + 1 pad for 16-byte loads)
 constexpr int NODE_STRIDE = 10;
 
+/// sqrt(pi) to the digits the reference library uses (its M_SQRTPI)
+constexpr double SQRT_PI = 1.77245385090551602729816748334;
+
 AGB_HD double pow2(double x) { return x * x; }
 AGB_HD double signOf(double x) { return x > 0 ? 1. : x < 0 ? -1. : 0.; }
 AGB_HD bool isFinite(double x) { return x == x && x != INFINITY && x != -INFINITY; }

@@ -2,6 +2,7 @@
 // coefficient-file reader.  Runs once per potential; the evaluation itself is device code.
 #include "multipole.h"
 #include "sphharm.cuh"
+#include "ref_tables.h"
 #include <stdexcept>
 #include <fstream>
 #include <sstream>
@@ -16,6 +17,7 @@ const double SQRT_DBL_EPSILON = 1.4901161193847656e-08;
 const double ROOT3_DBL_EPSILON = 6.0554544523933395e-06;   // DBL_EPSILON^(1/3)
 const double GRID_SAFETY_FACTOR = ROOT3_DBL_EPSILON;        // reference src/potential_multipole.cpp:59
 const int LMAX_1D_SPLINE = 2;                               // reference src/potential_multipole.cpp:43
+
 
 inline bool isXRefl(int s) { return (s & SYM_XREFL) == SYM_XREFL; }
 inline bool isYRefl(int s) { return (s & SYM_YREFL) == SYM_YREFL; }
@@ -121,8 +123,14 @@ MultipoleHost::Asympt makeAsymptote(const std::vector<double>& radii,
 std::vector<double> gridInTau(int lmax)
 {
     const int ngl = lmax + 1;
-    std::vector<double> t(ngl + 2), w(ngl);
-    glNodesWeights(ngl, &t[1], &w[0]);
+    if(ngl > GL_HALF_MAXN)
+        throw std::invalid_argument("Multipole: lmax too large for the angular grid");
+    std::vector<double> t(ngl + 2);
+    const double* half = GL_HALF_NODES + GL_HALF_OFFSET[ngl];
+    for(int i = 0; i <= ngl / 2; i++) {         // nodes on [-1, 1] from the rule on [0, 1]
+        t[1 + i] = -1 + half[i] * 2;
+        t[ngl - i] = 1 - half[i] * 2;
+    }
     for(int i = 1; i <= ngl; i++)
         t[i] /= 1 + sqrt(1 - pow2(t[i]));
     t.front() = -1;
@@ -391,7 +399,7 @@ MultipoleHost buildMultipole(const std::vector<double>& radii,
             const int lmin = ind.lmin(m);
             if(lmin > ind.lmax) continue;
             const int absm = std::abs(m);
-            const double mul = m == 0 ? 2 * sqrt(M_PI) : 2 * sqrt(M_PI) * M_SQRT2;
+            const double mul = m == 0 ? 2 * SQRT_PI : 2 * SQRT_PI * M_SQRT2;
             for(size_t j = 0; j < nt; j++) {
                 legendreArray(ind.lmax, absm, M.tau[j], &P[0], &dP[0], nullptr);
                 for(size_t k = 0; k < nr; k++) {

@@ -111,7 +111,7 @@ __device__ void sphHarmInverse(const HarmIndices& ind, double R, double z, doubl
     for(int mm = 0; mm < nm; mm++) {
         const int m = mm + ind.mmin(), lmin = ind.lmin(m);
         if(lmin > ind.lmax) continue;
-        const double mul = m == 0 ? 3.5449077018110318 : 5.0132565492620005;  // 2 sqrt(pi), * sqrt(2)
+        const double mul = m == 0 ? 2 * SQRT_PI : 2 * SQRT_PI * M_SQRT2;
         for(int q = 0; q < NQ; q++) Cm[mm + q * nm] = 0;
         const int absm = m < 0 ? -m : m;
         legendreArray(ind.lmax, absm, tau, P, NQ >= 3 ? dP : nullptr, NQ == 6 ? d2P : nullptr);

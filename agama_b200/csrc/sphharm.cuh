@@ -1,6 +1,7 @@
 // Normalised associated Legendre functions and multiple-angle trigonometry, host and device.
 #pragma once
 #include "common.cuh"
+#include "ref_tables.h"
 
 namespace agb {
 
@@ -12,20 +13,31 @@ namespace agb {
 AGB_HD void legendreArray(int lmax, int m, double tau, double* P, double* dP, double* d2P)
 {
     if(lmax == 0) {
-        P[0] = 0.28209479177387814;   // 1 / (2 sqrt(pi))
+        P[0] = 0.5 / SQRT_PI;
         if(dP)  dP[0] = 0;
         if(d2P) d2P[0] = 0;
         return;
     }
     const double ct = 2 * tau / (1 + tau * tau);          // cos(theta)
     const double st = (1 - tau * tau) / (1 + tau * tau);  // sin(theta)
-    // P_m^m = (-1)^m (2m-1)!! sin^m(theta), normalised by sqrt((2m+1) / (4 pi (2m)!))
-    double prefact = 0.28209479177387814, dfact = 1;
-    for(int k = 1; k <= m; k++) {
-        prefact *= sqrt((2 * k + 1.) / ((2 * k - 1.) * (2 * k) * (2 * k - 1))) ;
-        dfact *= (2 * k - 1);
+    // P_m^m = (-1)^m (2m-1)!! sin^m(theta), normalised by sqrt((2m+1) / (4 pi (2m)!));
+    // the normalisations for m <= 16 come from the reference's 16-digit table
+    double prefact, coef;
+    if(m <= PMM_TABLE_MAX) {
+#ifdef __CUDA_ARCH__
+        prefact = PMM_NORM_DEV[m];
+        coef = PMM_COEF_DEV[m];
+#else
+        prefact = PMM_NORM[m];
+        coef = PMM_COEF[m];
+#endif
+    } else {
+        double f = 1, df = 1;
+        for(int k = 2; k <= 2 * m; k++) f *= k;
+        for(int k = 2 * m - 1; k > 1; k -= 2) df *= k;
+        prefact = 0.5 / SQRT_PI * sqrt((2 * m + 1) / f);
+        coef = prefact * df * (m % 2 == 1 ? -1 : 1);
     }
-    // note: the loop above accumulates sqrt((2m+1)/(2m)!) as a telescoping product
     if(m == 0) {
         P[0] = prefact;
         if(dP)  dP[0] = 0;
@@ -35,12 +47,17 @@ AGB_HD void legendreArray(int lmax, int m, double tau, double* P, double* dP, do
         if(dP)  dP[0] = -ct * prefact;
         if(d2P) d2P[0] = st * prefact;
     } else {
-        const double coef = prefact * dfact * (m % 2 == 1 ? -1 : 1);
-        double sinm2 = 1;
-        for(int k = 0; k < m - 2; k++) sinm2 *= st;
-        P[0] = coef * sinm2 * st * st;
+        // sin^(m-2) by binary exponentiation (same product order as the reference's math::pow)
+        double sinm2 = 1, base = st;
+        for(int e = m - 2; ; ) {
+            if(e % 2) sinm2 *= base;
+            e >>= 1;
+            base *= base;
+            if(!e) break;
+        }
+        P[0] = coef * sinm2 * (st * st);
         if(dP)  dP[0] = m * coef * sinm2 * st * ct;
-        if(d2P) d2P[0] = m * coef * sinm2 * (m * ct * ct - 1);
+        if(d2P) d2P[0] = m * coef * sinm2 * (m * (ct * ct) - 1);
     }
     if(lmax == m)
         return;

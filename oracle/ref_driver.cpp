@@ -158,11 +158,17 @@ int ref_orbits_many(void* handle, long n, const double* ic, const double* T, dou
     for(long i = 0; i < n; i++) {
         try {
             long cnt = 0;
+            orbit::Trajectory traj;
             orbit::OrbitIntegrator<coord::Car> orbint(pot, Omega, params);
             orbint.addRuntimeFnc(orbit::PtrRuntimeFnc(new StepCounter(orbint, &cnt)));
-            orbint.init(coord::PosVelCar(ic + 6*i));
-            coord::PosVelCar end = orbint.run(T[i]);
-            end.unpack_to(final + 6*i);
+            // final point recorded as the reference's Python orbit() does: a runtime trajectory
+            // with an infinite sampling interval (interface_python.cpp:8126-8127, orbit.cpp:19-25)
+            orbint.addRuntimeFnc(orbit::PtrRuntimeFnc(new orbit::RuntimeTrajectory(orbint, INFINITY, traj)));
+            coord::PosVelCar ic6(ic + 6*i);
+            orbint.init(ic6);
+            orbint.run(T[i]);
+            if(traj.empty()) ic6.unpack_to(final + 6*i);
+            else traj[0].first.unpack_to(final + 6*i);
             if(nsteps) nsteps[i] = cnt;
             if(status) status[i] = 0;
         } catch(std::exception& e) {
