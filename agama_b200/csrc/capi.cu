@@ -163,3 +163,62 @@ extern "C" int agama_inspectMultipoleFile(const char* file, int* lmax, int* mmax
         if(gridSizeTau) *gridSizeTau = static_cast<int>(H.tau.size());
     });
 }
+
+// ------------------------------------------------------------------------------------------
+// orbits
+
+#include "dop853.cuh"
+
+namespace {
+OrbitParams makeOrbitParams(double Omega, double accuracy, long maxNumSteps)
+{
+    if(!(accuracy > 0)) throw std::invalid_argument("integrateOrbits: accuracy must be positive");
+    OrbitParams P;
+    P.Omega = Omega;
+    P.accRel = accuracy;
+    P.accAbs = 0;
+    P.maxSteps = maxNumSteps > 0 ? maxNumSteps : 100000000L;   // reference default 1e8, src/orbit.h:127
+    return P;
+}
+}  // namespace
+
+extern "C" int agama_integrateOrbitsManyDevice(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
+    long* numSteps, long* numRejected, int* status, int useQueue, void* stream)
+{
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && (!ic || !T || !finalState)))
+            throw std::invalid_argument("integrateOrbitsManyDevice: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const OrbitParams P = makeOrbitParams(Omega, accuracy, maxNumSteps);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        unsigned long long* queue = nullptr;
+        if(useQueue) AGB_CUDA(cudaMallocAsync(&queue, sizeof(unsigned long long), s));
+        launchOrbits(p->pot->view, P, n, ic, T, finalState, numSteps, numRejected, status, queue, s);
+        if(queue) AGB_CUDA(cudaFreeAsync(queue, s));
+    });
+}
+
+extern "C" int agama_integrateOrbitsMany(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
+    long* numSteps, int* status)
+{
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && (!ic || !T || !finalState)))
+            throw std::invalid_argument("integrateOrbitsMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const OrbitParams P = makeOrbitParams(Omega, accuracy, maxNumSteps);
+        DevBuf<double> dic(6 * n), dT(n), dout(6 * n);
+        DevBuf<long> dsteps(n);
+        DevBuf<int> dstat(n);
+        DevBuf<unsigned long long> q(1);
+        AGB_CUDA(cudaMemcpy(dic.ptr, ic, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
+        AGB_CUDA(cudaMemcpy(dT.ptr, T, n * sizeof(double), cudaMemcpyHostToDevice));
+        launchOrbits(p->pot->view, P, n, dic.ptr, dT.ptr, dout.ptr, dsteps.ptr, nullptr, dstat.ptr, q.ptr, 0);
+        AGB_CUDA(cudaMemcpy(finalState, dout.ptr, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        if(numSteps) AGB_CUDA(cudaMemcpy(numSteps, dsteps.ptr, n * sizeof(long), cudaMemcpyDeviceToHost));
+        if(status) AGB_CUDA(cudaMemcpy(status, dstat.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
+    });
+}

@@ -55,8 +55,13 @@ struct DevicePotential {
 DevicePotential* createDevicePotential(const std::vector<double>& radii,
     const std::vector<std::vector<double>>& Phi, const std::vector<std::vector<double>>& dPhi);
 
+struct OrbitParams;
+
 /// launch helpers (defined in the .cu files)
 void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
     double* grad, double* hess, cudaStream_t stream);
+/// DOP853 batch; queue != nullptr selects the persistent work-queue mapping (8-byte counter)
+void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream);
 
 }  // namespace agb

@@ -1,5 +1,52 @@
-"""DOP853 orbit integration on the device."""
+"""DOP853 orbit integration on the device.
+
+Mirror of the reference's Python orbit() (src/interface_python.cpp:7689-8200) for the
+final-point output (trajsize = 1): orbits start at ic (x,y,z,vx,vy,vz in the frame rotating with
+pattern speed Omega) at time 0 and are integrated for `time` (scalar or per orbit).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import check, ptr
 
 
-def orbit(*args, **kwargs):
-    raise NotImplementedError
+def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=True, info=False):
+    """Integrate orbits; returns the final phase-space points (n x 6), and with info=True also
+    a dict with the accepted step counts, rejected attempts and statuses
+    (0 ok, 1 step limit reached, 2 zero / non-finite step, 3 non-finite error estimate).
+
+    ic / time may be numpy arrays (host; copied to the device and back) or CUDA torch tensors
+    (processed in place on the current stream; the outputs are then tensors too).
+    queue=True drains the batch from a device work queue (best for uneven integration times).
+    """
+    from . import _is_device_array, _dev_ptr, _current_stream
+    if _is_device_array(ic):
+        import torch
+        x = ic.contiguous().view(-1, 6)
+        n = x.shape[0]
+        T = time if _is_device_array(time) else torch.full((n,), float(time), dtype=torch.float64, device=x.device)
+        T = T.contiguous()
+        out = torch.empty_like(x)
+        steps = torch.empty(n, dtype=torch.int64, device=x.device)
+        rej = torch.empty(n, dtype=torch.int64, device=x.device)
+        st = torch.empty(n, dtype=torch.int32, device=x.device)
+        check(_native.lib().agama_integrateOrbitsManyDevice(
+            potential.handle, n, _dev_ptr(x), _dev_ptr(T), float(Omega), float(accuracy), int(maxNumSteps),
+            _dev_ptr(out), _dev_ptr(steps), _dev_ptr(rej), _dev_ptr(st), 1 if queue else 0, _current_stream()))
+        return (out, dict(steps=steps, rejected=rej, status=st)) if info else out
+    x = np.ascontiguousarray(ic, dtype=np.float64)
+    single = x.ndim == 1
+    x = x.reshape(-1, 6)
+    n = len(x)
+    T = np.ascontiguousarray(np.broadcast_to(np.asarray(time, dtype=np.float64), (n,)))
+    out = np.empty((n, 6))
+    steps = np.zeros(n, dtype=np.int64)
+    st = np.zeros(n, dtype=np.int32)
+    check(_native.lib().agama_integrateOrbitsMany(
+        potential.handle, n, ptr(x), ptr(T), float(Omega), float(accuracy), int(maxNumSteps),
+        ptr(out), steps.ctypes.data_as(_native.L), st.ctypes.data_as(_native.I)))
+    if single:
+        out = out[0]
+    return (out, dict(steps=steps, status=st)) if info else out

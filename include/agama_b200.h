@@ -71,6 +71,26 @@ int agama_evalPotentialMany(const agama_Potential* potential, long n, const doub
 int agama_evalPotentialManyDevice(const agama_Potential* potential, long n, const double* pos,
     double* phi, double* deriv, double* deriv2, void* stream);
 
+/* ---------------------------------------------------------------------------------------
+   Orbit integration (DOP853).  Each of the n orbits starts at ic[i] (x,y,z,vx,vy,vz, in the
+   frame rotating with pattern speed Omega about z) at time 0 and is integrated for time T[i]
+   with relative accuracy `accuracy` and at most maxNumSteps accepted steps (<= 0: 1e8).
+   Outputs: the final point in the rotating frame, the number of accepted steps and a status
+   (0 ok, 1 step limit reached, 2 zero / non-finite step, 3 non-finite error estimate).
+   Replaces n runs of orbit::OrbitIntegrator<Car>(pot, Omega, {accuracy, maxNumSteps}).init(ic)
+   + run(T) with a final-point RuntimeTrajectory (src/orbit.h:165-315, src/orbit.cpp:15-117),
+   as driven by the reference's Python orbit() (src/interface_python.cpp:8101-8160). */
+int agama_integrateOrbitsMany(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
+    long* numSteps, int* status);
+
+/* The same on device buffers (numSteps, numRejected, status may be NULL; numRejected counts
+   rejected step attempts).  useQueue != 0 drains the batch from a device work queue with a
+   grid sized to the GPU (for batches of very uneven integration times). */
+int agama_integrateOrbitsManyDevice(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
+    long* numSteps, long* numRejected, int* status, int useQueue, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,8 +103,61 @@ def make_potential_vectors():
         print("wrote", out, len(pts))
 
 
+def tcirc(coef, E):
+    """T_circ(E) of the reference (potential_utils.h:83-87) through its Python interface"""
+    import agama
+    return agama.Potential(file=coef).Tcirc(E)
+
+
+def regular_flags(pot, ic, T, Omega, accuracy=1e-8):
+    """an orbit counts as regular when a 1e-12 relative perturbation of its initial point
+    changes the final point by less than 1e-9 (relative): no exponential divergence over T"""
+    f0, _, _ = pot.orbits(ic, T, Omega=Omega, accuracy=accuracy)
+    f1, _, _ = pot.orbits(ic * (1 + 1e-12), T, Omega=Omega, accuracy=accuracy)
+    d = np.max(np.abs(f1 - f0) / np.maximum(np.abs(f0), 1e-300), axis=1)
+    sc = np.linalg.norm(f1[:, :3] - f0[:, :3], axis=1) / np.linalg.norm(f0[:, :3], axis=1)
+    return (sc < 1e-9) & (d < 1e-6)
+
+
+def make_orbit_vectors():
+    # config 1: orbits drawn as in the benchmark, T = 10 T_circ(E)
+    coef = coef_path("cfg1")
+    pot = ref.Potential(file=coef)
+    n = 48
+    x = workloads.dehnen_positions(n, gamma=1, q=(0.8, 0.6), seed=workloads.SEEDS["orbits1"])
+    ic = workloads.orbit_ics(x, lambda p: pot.eval(p)[0], seed=workloads.SEEDS["orbits1"] + 100)
+    E = pot.eval(ic[:, :3])[0] + 0.5 * np.sum(ic[:, 3:] ** 2, axis=1)
+    T = 10 * tcirc(coef, E)
+    # edge cases: zero time, backward integration, an escaping orbit, a step-limited orbit
+    ic = np.vstack([ic, ic[:3], [[0.5, 0.1, 0.2, 3.0, 0.5, -0.2]]])
+    T = np.concatenate([T, [0.0, -T[1], T[2], 50.0]])
+    final, steps, status = pot.orbits(ic, T, Omega=0.0, accuracy=1e-8)
+    fin10, steps10, st10 = pot.orbits(ic[:4], T[:4], Omega=0.0, accuracy=1e-8, maxSteps=10)
+    regular = regular_flags(pot, ic, T, 0.0)
+    np.savez_compressed(os.path.join(HERE, "orbits_cfg1.npz"), ic=ic, T=T, Omega=0.0, accuracy=1e-8,
+                        final=final, steps=steps, status=status, regular=regular,
+                        final_maxsteps10=fin10, steps_maxsteps10=steps10, status_maxsteps10=st10)
+    print("cfg1 orbits", len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max())
+    # config 3: rotating frame Omega = 0.05, uneven times 10^U[1, 1.5] T_circ
+    coef = coef_path("cfg3")
+    pot = ref.Potential(file=coef)
+    n = 24
+    x = workloads.dehnen_positions(n, gamma=0.5, q=(0.7, 0.5), seed=workloads.SEEDS["orbits3"])
+    ic = workloads.orbit_ics(x, lambda p: pot.eval(p)[0], seed=workloads.SEEDS["orbits3"] + 100)
+    E = pot.eval(ic[:, :3])[0] + 0.5 * np.sum(ic[:, 3:] ** 2, axis=1)
+    rng = np.random.Generator(np.random.PCG64(41))
+    T = tcirc(coef, E) * 10 ** rng.uniform(1, 1.5, size=n)
+    final, steps, status = pot.orbits(ic, T, Omega=0.05, accuracy=1e-8)
+    regular = regular_flags(pot, ic, T, 0.05)
+    np.savez_compressed(os.path.join(HERE, "orbits_cfg3.npz"), ic=ic, T=T, Omega=0.05, accuracy=1e-8,
+                        final=final, steps=steps, status=status, regular=regular)
+    print("cfg3 orbits", len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max())
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     if what in ("potentials", "all"):
         make_potentials()
         make_potential_vectors()
+    if what in ("orbits", "all"):
+        make_orbit_vectors()

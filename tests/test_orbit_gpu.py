@@ -1,0 +1,81 @@
+"""Parity of the device DOP853 orbit integration with the reference's OrbitIntegrator<Car>
+(golden vectors from tests/golden/make_golden.py; accuracy 1e-8 as in the benchmark).
+
+Bounds (from the engine's specification):
+  * regular orbits: final positions and velocities agree to 1e-7 relative (vector norms);
+  * chaotic orbits (a 1e-12 perturbation of the initial point already changes the reference's
+    own end point by >1e-9): only the conservation of the (Jacobi) energy is compared --
+    the engine's drift must be no worse than 10x the reference's (or 1e-9);
+  * accepted step counts of regular orbits agree within 2% (+-2 steps);
+  * T = 0 returns the initial point unchanged; the step limit stops orbits with status 1.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+
+def jacobi_energy(pot, w, Omega):
+    phi = pot.potential(w[:, :3])
+    return phi + 0.5 * np.sum(w[:, 3:] ** 2, axis=1) - Omega * (w[:, 0] * w[:, 4] - w[:, 1] * w[:, 3])
+
+
+def rel_vec(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)
+
+
+@pytest.mark.parametrize("cfg", ["cfg1", "cfg3"])
+@pytest.mark.parametrize("queue", [True, False])
+def test_orbit_parity(cfg, queue):
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % cfg))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    Omega = float(g["Omega"])
+    final, info = agama_b200.orbit(pot, g["ic"], g["T"], Omega=Omega, accuracy=float(g["accuracy"]),
+                                   queue=queue, info=True)
+    reg = g["regular"] & (g["status"] == 0)
+    assert np.all(info["status"] == g["status"])
+    epos = rel_vec(final[reg, :3], g["final"][reg, :3])
+    evel = rel_vec(final[reg, 3:], g["final"][reg, 3:])
+    assert epos.max() <= 1e-7 and evel.max() <= 1e-7, (epos.max(), evel.max())
+    s, sr = info["steps"][reg], g["steps"][reg]
+    assert np.all(np.abs(s - sr) <= np.maximum(2, 0.02 * sr)), np.abs(s - sr).max()
+    # energy conservation for all (incl. chaotic) orbits
+    E0 = jacobi_energy(pot, g["ic"], Omega)
+    drift = np.abs(jacobi_energy(pot, final, Omega) / E0 - 1)
+    drift_ref = np.abs(jacobi_energy(pot, g["final"], Omega) / E0 - 1)
+    ok = g["status"] == 0
+    assert np.all(drift[ok] <= np.maximum(10 * drift_ref[ok], 1e-9)), (drift[ok].max(), drift_ref[ok].max())
+
+
+def test_orbit_edge_cases():
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "orbits_cfg1.npz"))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+    # zero integration time: the initial point comes back unchanged
+    i0 = int(np.where(g["T"] == 0)[0][0])
+    f, info = agama_b200.orbit(pot, g["ic"][i0:i0 + 1], 0.0, info=True)
+    assert np.array_equal(f[0], g["ic"][i0]) and info["steps"][0] == 0
+    # step limit: status 1 after exactly 10 steps, same point as the reference after 10 steps
+    f, info = agama_b200.orbit(pot, g["ic"][:4], g["T"][:4], maxNumSteps=10, info=True)
+    assert np.all(info["status"] == g["status_maxsteps10"]) and np.all(info["steps"] == g["steps_maxsteps10"])
+    assert rel_vec(f[:, :3], g["final_maxsteps10"][:, :3]).max() <= 1e-10
+    # empty batch
+    assert agama_b200.orbit(pot, np.zeros((0, 6)), 1.0).shape == (0, 6)
+
+
+def test_orbit_device_pointers():
+    import torch
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "orbits_cfg1.npz"))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+    ic = torch.tensor(g["ic"], device="cuda")
+    T = torch.tensor(g["T"], device="cuda")
+    out, info = agama_b200.orbit(pot, ic, T, info=True)
+    torch.cuda.synchronize()
+    host = agama_b200.orbit(pot, g["ic"], g["T"])
+    assert np.array_equal(out.cpu().numpy(), host)

@@ -3,7 +3,15 @@ reference's own BasePotential::eval, tests/golden/make_golden.py).
 
 Tolerances: potential and force (gradient) relative error <= 1e-12; Hessian <= 1e-10 (second
 derivatives of the quintic splines amplify round-off; the Hessian is used by the fudge's root
-bracketing, not by forces)."""
+bracketing, not by forces).
+
+Beyond the radial grid (r > r_max) the potential is the reference's outer power-law pair
+U (r/r_max)^s + W (r/r_max)^(-l-1).  For a halo whose enclosed mass grows almost
+logarithmically (the NFW component of config 2) the fitted slope is s = -0.99999 against
+v = -1, so U = -W = 0.0516 while U + W = -6e-6: the expression has condition number ~1e4,
+and the one-ulp difference between the device's and the host libm's exp/log becomes a
+~2e-12 relative difference (the reference's own value carries the same round-off).  Points
+in that region are held to 1e-11; everywhere else the bound is 1e-12."""
 import os
 
 import numpy as np
@@ -23,6 +31,12 @@ def rel_err_vec(a, b):
     return num / den
 
 
+def grid_radii(name):
+    with open(os.path.join(GOLDEN, name + ".coef")) as f:
+        block = f.read().split("#Phi")[1].split("#dPhi/dr")[0].strip().split("\n")[1:]
+    return np.array([float(line.split()[0]) for line in block if line.strip()])
+
+
 @pytest.fixture(scope="module")
 def potentials():
     import agama_b200
@@ -38,8 +52,10 @@ def test_potential_force_parity(potentials, name):
     egrad = rel_err_vec(-acc, g["grad"])
     ehess = rel_err_vec(hess, g["hess"])
     assert np.all(np.isfinite(phi)) and np.all(np.isfinite(acc))
-    assert ephi.max() <= 1e-12, (ephi.max(), g["points"][ephi.argmax()])
-    assert egrad.max() <= 1e-12, (egrad.max(), g["points"][egrad.argmax()])
+    r = np.linalg.norm(g["points"], axis=1)
+    tol = np.where(r > grid_radii(name)[-1], 1e-11, 1e-12)
+    assert np.all(ephi <= tol), (ephi.max(), g["points"][np.argmax(ephi / tol)])
+    assert np.all(egrad <= tol), (egrad.max(), g["points"][np.argmax(egrad / tol)])
     assert ehess.max() <= 1e-10, (ehess.max(), g["points"][ehess.argmax()])
 
 
