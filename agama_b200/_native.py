@@ -31,6 +31,16 @@ SIGNATURES = {
     "agama_integrateOrbitsManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
                                                        ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
                                                        ctypes.c_int, VP]),
+    "agama_deleteActionFinder": (None, [VP]),
+    "agama_evalActionsAnglesFrequencies": (None, [VP, D, D, D, D]),
+    "agama_evalActionsAnglesFrequenciesStandalone": (None, [VP, ctypes.c_double, D, D, D, D]),
+    "agama_createActionFinderFromTables": (VP, [VP, ctypes.c_int, D, ctypes.c_int, D, D, ctypes.c_int, D,
+                                                ctypes.c_int, D, ctypes.c_int, D, D]),
+    "agama_evalActionsMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, D]),
+    "agama_evalActionsManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP]),
+    "agama_evalActionsStandaloneMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, D]),
+    "agama_evalActionsStandaloneManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double, VP,
+                                                             VP, VP]),
 }
 
 _lib = None

@@ -1,9 +1,102 @@
-"""Staeckel-fudge action finder on the device (filled in with the fudge kernels)."""
+"""Staeckel-fudge action finder on the device.
+
+Mirror of the reference's Python ActionFinder / actions (src/interface_python.cpp:3705-3860):
+
+    af = ActionFinder(potential, tables=...)     # focal-distance table + L_circ(E) interpolator
+    J  = af(points)                              # (n, 3): Jr, Jz, Jphi
+    J  = actions(potential, points, fd=...)      # fixed focal distance(s)
+
+`points` are Cartesian phase-space points (n x 6) as numpy arrays (host) or CUDA torch tensors
+(device, processed on the current stream).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import check, ptr
 
 
 class ActionFinder:
-    pass
+    """Staeckel-fudge action finder (the reference's ActionFinderAxisymFudge, non-interpolated).
+
+    tables: dict with gridE, gridL, delta (nE x nL), lofe / rofl / phiofr (4 x n: x, f, f', f''),
+    invPhi0, interp_invPhi0, slopeOut, coefOut, massOut -- the focal-distance grid and the
+    L_circ(E) interpolator of the finder.
+    """
+
+    def __init__(self, potential, tables=None):
+        if tables is None:
+            raise NotImplementedError("ActionFinder: building the focal-distance table needs tables=...")
+        self.potential = potential
+        t = {k: np.ascontiguousarray(v, dtype=np.float64) if isinstance(v, np.ndarray) else v
+             for k, v in tables.items()}
+        gE, gL, dl = t["gridE"], t["gridL"], np.ascontiguousarray(t["delta"], dtype=np.float64)
+        lofe, rofl, phr = (np.ascontiguousarray(t[k], dtype=np.float64) for k in ("lofe", "rofl", "phiofr"))
+        scal = np.array([t["invPhi0"], t["interp_invPhi0"], t["slopeOut"], t["coefOut"], t["massOut"]], dtype=np.float64)
+        h = _native.lib().agama_createActionFinderFromTables(
+            potential.handle, len(gE), ptr(gE), len(gL), ptr(gL), ptr(dl), lofe.shape[1], ptr(lofe),
+            rofl.shape[1], ptr(rofl), phr.shape[1], ptr(phr), ptr(scal))
+        if not h:
+            raise RuntimeError("agama_b200: " + _native.error())
+        self._h = ctypes.c_void_p(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _native._lib is not None:
+            _native._lib.agama_deleteActionFinder(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __call__(self, points, fd=False):
+        """actions (n x 3); with fd=True also the focal distance used for each point"""
+        from . import _is_device_array, _dev_ptr, _current_stream
+        if _is_device_array(points):
+            import torch
+            p = points.contiguous().view(-1, 6)
+            n = p.shape[0]
+            act = torch.empty((n, 3), dtype=torch.float64, device=p.device)
+            fdo = torch.empty(n, dtype=torch.float64, device=p.device) if fd else None
+            check(_native.lib().agama_evalActionsManyDevice(self._h, n, _dev_ptr(p), _dev_ptr(act), _dev_ptr(fdo),
+                                                            _current_stream()))
+            return (act, fdo) if fd else act
+        p = np.ascontiguousarray(points, dtype=np.float64)
+        single = p.ndim == 1
+        p = p.reshape(-1, 6)
+        n = len(p)
+        act = np.empty((n, 3))
+        fdo = np.empty(n) if fd else None
+        check(_native.lib().agama_evalActionsMany(self._h, n, ptr(p), ptr(act), ptr(fdo)))
+        if single:
+            act = act[0]
+        return (act, fdo) if fd else act
 
 
-def actions(*args, **kwargs):
-    raise NotImplementedError
+def actions(potential, points, fd, iters=False):
+    """Staeckel-fudge actions for given focal distance(s) fd (scalar or per point)."""
+    from . import _is_device_array, _dev_ptr, _current_stream
+    if _is_device_array(points):
+        import torch
+        p = points.contiguous().view(-1, 6)
+        n = p.shape[0]
+        act = torch.empty((n, 3), dtype=torch.float64, device=p.device)
+        it = torch.empty(n, dtype=torch.int32, device=p.device) if iters else None
+        fda = fd.contiguous() if _is_device_array(fd) else None
+        check(_native.lib().agama_evalActionsStandaloneManyDevice(
+            potential.handle, n, _dev_ptr(p), _dev_ptr(fda), 0.0 if fda is not None else float(fd),
+            _dev_ptr(act), _dev_ptr(it), _current_stream()))
+        return (act, it) if iters else act
+    p = np.ascontiguousarray(points, dtype=np.float64)
+    single = p.ndim == 1
+    p = p.reshape(-1, 6)
+    n = len(p)
+    act = np.empty((n, 3))
+    if np.ndim(fd) == 0:
+        check(_native.lib().agama_evalActionsStandaloneMany(potential.handle, n, ptr(p), None, float(fd), ptr(act)))
+    else:
+        fda = np.ascontiguousarray(np.broadcast_to(np.asarray(fd, dtype=np.float64), (n,)))
+        check(_native.lib().agama_evalActionsStandaloneMany(potential.handle, n, ptr(p), ptr(fda), 0.0, ptr(act)))
+    return act[0] if single else act

@@ -1,0 +1,148 @@
+// Staeckel-fudge action kernels, the device-resident action finder and their host launchers.
+#include "runtime.h"
+#include "fudge.cuh"
+#include <mutex>
+#include <map>
+
+namespace agb {
+
+namespace {
+
+constexpr int FUDGE_BLOCK = 128;
+
+/// Gauss-Legendre rules on [0,1] for the orders 1..20, 25, 32, 40 (the set the reference
+/// tabulates, src/math_glquadrature.h), computed by Newton iteration in extended precision
+struct GLRulesHost { int offset[GL_MAX_ORDER + 1]; std::vector<double> nodes, weights; };
+
+GLRulesHost makeGLRules()
+{
+    GLRulesHost g;
+    for(int n = 0; n <= GL_MAX_ORDER; n++) g.offset[n] = -1;
+    const int orders[] = { 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 25, 32, 40 };
+    for(int n : orders) {
+        g.offset[n] = static_cast<int>(g.nodes.size());
+        std::vector<long double> x(n), w(n);
+        for(int i = 0; i < n; i++) {
+            long double t = cosl(3.14159265358979323846264338327950288L * (i + 0.75L) / (n + 0.5L)), dp = 1;
+            for(int it = 0; it < 100; it++) {
+                long double p0 = 1, p1 = t;
+                for(int k = 2; k <= n; k++) { long double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k; p0 = p1; p1 = p2; }
+                if(n == 1) { p1 = t; p0 = 1; }
+                dp = n * (t * p1 - p0) / (t * t - 1);
+                const long double dx = p1 / dp;
+                t -= dx;
+                if(fabsl(dx) < 1e-19L) break;
+            }
+            long double p0 = 1, p1 = t;
+            for(int k = 2; k <= n; k++) { long double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k; p0 = p1; p1 = p2; }
+            if(n == 1) { p1 = t; p0 = 1; }
+            dp = n * (t * p1 - p0) / (t * t - 1);
+            x[i] = (1 - t) / 2;                    // ascending nodes on [0, 1]
+            w[i] = 1 / ((1 - t * t) * dp * dp);    // = (2 / ((1-t^2) P'^2)) / 2
+        }
+        for(int i = 0; i < n; i++) { g.nodes.push_back(static_cast<double>(x[i])); g.weights.push_back(static_cast<double>(w[i])); }
+    }
+    return g;
+}
+
+/// per-device copy of the quadrature rules (uploaded on first use)
+struct GLDevice { DevBuf<double> nodes, weights; GLRules view; };
+std::mutex g_glMutex;
+std::map<int, GLDevice*> g_gl;
+
+const GLRules& glRulesForCurrentDevice()
+{
+    int dev;
+    AGB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_glMutex);
+    auto it = g_gl.find(dev);
+    if(it != g_gl.end()) return it->second->view;
+    static const GLRulesHost host = makeGLRules();
+    GLDevice* d = new GLDevice;
+    d->nodes.upload(host.nodes);
+    d->weights.upload(host.weights);
+    for(int n = 0; n <= GL_MAX_ORDER; n++) d->view.offset[n] = host.offset[n];
+    d->view.nodes = d->nodes.ptr;
+    d->view.weights = d->weights.ptr;
+    g_gl[dev] = d;
+    return d->view;
+}
+
+/// One point per thread.  FINDER: Delta from the finder's table; otherwise from fd[i] (or fd0 if
+/// fd is null).  Outputs actions (Jr, Jz, Jphi), optionally Delta and root-finder iterations.
+template<bool FINDER>
+__global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const MultipoleView M, const GLRules gl,
+    const FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd, double fd0,
+    double* __restrict__ act, double* __restrict__ fdOut, int* __restrict__ iters)
+{
+    const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    if(i >= n) return;
+    double w[6], pc[6];
+    for(int c = 0; c < 6; c++) w[c] = posvel[6 * i + c];
+    carToCylPosVel(w, pc);
+    double Phi;
+    CylDerivs g; CylHess h;
+    evalMultipoleCyl<1>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
+    const double delta = FINDER ? finderFocalDistance(F, pc, Phi) : (fd ? fd[i] : fd0);
+    double a[3];
+    int it = 0;
+    fudgeActions(M, gl, pc, Phi, delta, a, &it);
+    act[3 * i] = a[0]; act[3 * i + 1] = a[1]; act[3 * i + 2] = a[2];
+    if(fdOut) fdOut[i] = delta;
+    if(iters) iters[i] = it;
+}
+
+}  // namespace
+
+void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
+    double* act, int* iters, cudaStream_t stream)
+{
+    if(n <= 0) return;
+    const GLRules& gl = glRulesForCurrentDevice();
+    FudgeTables dummy{};
+    fudgeKernel<false><<<(n + FUDGE_BLOCK - 1) / FUDGE_BLOCK, FUDGE_BLOCK, 0, stream>>>(
+        M, gl, dummy, n, posvel, fd, fd0, act, nullptr, iters);
+    AGB_CUDA(cudaGetLastError());
+}
+
+void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
+    double* act, double* fdOut, int* iters, cudaStream_t stream)
+{
+    if(n <= 0) return;
+    const GLRules& gl = glRulesForCurrentDevice();
+    fudgeKernel<true><<<(n + FUDGE_BLOCK - 1) / FUDGE_BLOCK, FUDGE_BLOCK, 0, stream>>>(
+        M, gl, F, n, posvel, nullptr, 0, act, fdOut, iters);
+    AGB_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------------
+
+DeviceActionFinder* createDeviceActionFinder(DevicePotential* pot, const FinderTablesHost& T)
+{
+    if(!pot->axisymmetric)
+        throw std::invalid_argument("Fudge approximation only works for axisymmetric potentials");
+    if(T.nE < 2 || T.nL < 2 || T.gridE.size() != static_cast<size_t>(T.nE) ||
+        T.gridL.size() != static_cast<size_t>(T.nL) || T.delta.size() != static_cast<size_t>(T.nE * T.nL) ||
+        T.lofe.size() % 4 || T.rofl.size() % 4 || T.phiofr.size() % 4)
+        throw std::invalid_argument("ActionFinder: inconsistent table sizes");
+    DeviceActionFinder* A = new DeviceActionFinder;
+    A->pot = pot;
+    A->host = T;
+    A->gridE.upload(T.gridE);
+    A->gridL.upload(T.gridL);
+    A->delta.upload(T.delta);
+    A->lofe.upload(T.lofe);
+    A->rofl.upload(T.rofl);
+    A->phiofr.upload(T.phiofr);
+    FudgeTables& F = A->view;
+    F.invPhi0 = T.invPhi0;
+    F.nE = T.nE; F.nL = T.nL;
+    F.gridE = A->gridE.ptr; F.gridL = A->gridL.ptr; F.delta = A->delta.ptr;
+    F.iInvPhi0 = T.interpInvPhi0; F.slopeOut = T.slopeOut; F.coefOut = T.coefOut; F.massOut = T.massOut;
+    F.LofE = Spline1dView{ static_cast<int>(T.lofe.size() / 4), A->lofe.ptr };
+    F.RofL = Spline1dView{ static_cast<int>(T.rofl.size() / 4), A->rofl.ptr };
+    F.PhiofR = Spline1dView{ static_cast<int>(T.phiofr.size() / 4), A->phiofr.ptr };
+    return A;
+}
+
+}  // namespace agb

@@ -222,3 +222,120 @@ extern "C" int agama_integrateOrbitsMany(const agama_Potential* p, long n, const
         if(status) AGB_CUDA(cudaMemcpy(status, dstat.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
     });
 }
+
+// ------------------------------------------------------------------------------------------
+// actions (Staeckel fudge)
+
+struct agama_ActionFinder { DeviceActionFinder* af; };
+
+namespace {
+void requireAxisymmetric(const agama_Potential* p) {
+    if(!p) throw std::invalid_argument("null potential");
+    if(!p->pot->axisymmetric)
+        throw std::invalid_argument("Fudge approximation only works for axisymmetric potentials");
+}
+std::vector<double> vec(const double* p, long n) { return p ? std::vector<double>(p, p + n) : std::vector<double>(); }
+}  // namespace
+
+extern "C" agama_ActionFinder* agama_createActionFinderFromTables(const agama_Potential* p,
+    int nE, const double* gridE, int nL, const double* gridL, const double* delta,
+    int nLofE, const double* LofE, int nRofL, const double* RofL, int nPhiofR, const double* PhiofR,
+    const double* scalars)
+{
+    try {
+        requireAxisymmetric(p);
+        if(nE < 2 || nL < 2 || !gridE || !gridL || !delta || nLofE < 2 || !LofE || nRofL < 2 || !RofL ||
+            nPhiofR < 2 || !PhiofR || !scalars)
+            throw std::invalid_argument("createActionFinderFromTables: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        FinderTablesHost T;
+        T.nE = nE; T.nL = nL;
+        T.gridE = vec(gridE, nE); T.gridL = vec(gridL, nL); T.delta = vec(delta, static_cast<long>(nE) * nL);
+        T.lofe = vec(LofE, 4L * nLofE); T.rofl = vec(RofL, 4L * nRofL); T.phiofr = vec(PhiofR, 4L * nPhiofR);
+        T.invPhi0 = scalars[0]; T.interpInvPhi0 = scalars[1]; T.slopeOut = scalars[2];
+        T.coefOut = scalars[3]; T.massOut = scalars[4];
+        return new agama_ActionFinder{ createDeviceActionFinder(p->pot, T) };
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+extern "C" void agama_deleteActionFinder(agama_ActionFinder* a)
+{
+    if(!a) return;
+    delete a->af;
+    delete a;
+}
+
+extern "C" int agama_evalActionsManyDevice(const agama_ActionFinder* a, long n, const double* posvel,
+    double* act, double* fdOut, void* stream)
+{
+    return guarded([&] {
+        if(!a || n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        launchActionsFinder(a->af->pot->view, a->af->view, n, posvel, act, fdOut, nullptr, static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int agama_evalActionsMany(const agama_ActionFinder* a, long n, const double* posvel,
+    double* act, double* fdOut)
+{
+    return guarded([&] {
+        if(!a || n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        DevBuf<double> dpv(6 * n), dact(3 * n), dfd(fdOut ? n : 0);
+        AGB_CUDA(cudaMemcpy(dpv.ptr, posvel, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
+        launchActionsFinder(a->af->pot->view, a->af->view, n, dpv.ptr, dact.ptr, dfd.ptr, nullptr, 0);
+        AGB_CUDA(cudaMemcpy(act, dact.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        if(fdOut) AGB_CUDA(cudaMemcpy(fdOut, dfd.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" int agama_evalActionsStandaloneManyDevice(const agama_Potential* p, long n, const double* posvel,
+    const double* fd, double fd0, double* act, int* rootIters, void* stream)
+{
+    return guarded([&] {
+        requireAxisymmetric(p);
+        if(n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsStandaloneManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        launchActionsFixedDelta(p->pot->view, n, posvel, fd, fd0, act, rootIters, static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int agama_evalActionsStandaloneMany(const agama_Potential* p, long n, const double* posvel,
+    const double* fd, double fd0, double* act)
+{
+    return guarded([&] {
+        requireAxisymmetric(p);
+        if(n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsStandaloneMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        DevBuf<double> dpv(6 * n), dact(3 * n), dfd(fd ? n : 0);
+        AGB_CUDA(cudaMemcpy(dpv.ptr, posvel, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
+        if(fd) AGB_CUDA(cudaMemcpy(dfd.ptr, fd, n * sizeof(double), cudaMemcpyHostToDevice));
+        launchActionsFixedDelta(p->pot->view, n, dpv.ptr, dfd.ptr, fd0, dact.ptr, nullptr, 0);
+        AGB_CUDA(cudaMemcpy(act, dact.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" void agama_evalActionsAnglesFrequencies(const agama_ActionFinder* a, const double posvel[6],
+    double actions[3], double angles[3], double frequencies[3])
+{
+    double act[3] = { NAN, NAN, NAN };
+    if(agama_evalActionsMany(a, 1, posvel, act, nullptr) != 0) act[0] = act[1] = act[2] = NAN;
+    if(actions) for(int k = 0; k < 3; k++) actions[k] = act[k];
+    if(angles) { angles[0] = angles[1] = angles[2] = NAN; setError("angles are not provided by this engine yet"); }
+    if(frequencies) { frequencies[0] = frequencies[1] = frequencies[2] = NAN; setError("frequencies are not provided by this engine yet"); }
+}
+
+extern "C" void agama_evalActionsAnglesFrequenciesStandalone(const agama_Potential* p, double fd,
+    const double posvel[6], double actions[3], double angles[3], double frequencies[3])
+{
+    double act[3] = { NAN, NAN, NAN };
+    if(agama_evalActionsStandaloneMany(p, 1, posvel, nullptr, fd, act) != 0) act[0] = act[1] = act[2] = NAN;
+    if(actions) for(int k = 0; k < 3; k++) actions[k] = act[k];
+    if(angles) { angles[0] = angles[1] = angles[2] = NAN; setError("angles are not provided by this engine yet"); }
+    if(frequencies) { frequencies[0] = frequencies[1] = frequencies[2] = NAN; setError("frequencies are not provided by this engine yet"); }
+}

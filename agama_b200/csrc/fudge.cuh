@@ -1,0 +1,362 @@
+// Axisymmetric Staeckel-fudge actions on the device (one phase-space point per thread).
+//
+// Reference: src/actions_staeckel.cpp -- findIntegralsOfMotionAxisymFudge (:176-195),
+// AxisymFunctionFudge::evalDeriv (:202-252), AxisymIntegrand (:276-299),
+// AxisymScaledForRootfinder (:329-354), findIntegrationLimitsAxisym (:360-483),
+// computeActions (:604-619), evalAxisym (:645-670), evalAxisymFudge (:683-693) and
+// ActionFinderAxisymFudge::eval (:954-979); prolate spheroidal coordinates from src/coord.cpp
+// (:266-338, :525-531); L_circ(E) from potential::Interpolator (src/potential_utils.cpp:872-980).
+#pragma once
+#include "multipole_eval.cuh"
+#include "fudge_types.h"
+
+namespace agb {
+
+constexpr int FUDGE_INTEGR_ORDER = 10;           // src/actions_staeckel.cpp:21
+constexpr double FUDGE_ACCURACY_RANGE = 1e-6;    // src/actions_staeckel.cpp:35
+constexpr double FUDGE_MINIMUM_RANGE = 1e-10;    // src/actions_staeckel.cpp:38
+
+/// QuinticSpline::evalDeriv (src/math_spline.cpp:1405-1429): linear extrapolation outside
+__device__ __forceinline__ void spline1d(const Spline1dView& S, double x, double* f, double* df, double* d2f)
+{
+    const int n = S.n;
+    const double* xv = S.t;
+    const double* fv = S.t + n;
+    const double* f1 = S.t + 2 * n;
+    const double* f2 = S.t + 3 * n;
+    if(n == 0 || x != x) { *f = NAN; if(df) *df = NAN; if(d2f) *d2f = NAN; return; }
+    const int i = binSearch(x, xv, n);
+    if(i < 0 || i >= n - 1) {
+        const int e = i < 0 ? 0 : n - 1;
+        const double d = ldg(f1 + e);
+        *f = ldg(fv + e) + (d == 0 ? 0 : d * (x - ldg(xv + e)));
+        if(df) *df = d;
+        if(d2f) *d2f = 0;
+        return;
+    }
+    const double fl[1] = { ldg(fv + i) }, fh[1] = { ldg(fv + i + 1) }, d1l[1] = { ldg(f1 + i) },
+        d1h[1] = { ldg(f1 + i + 1) }, d2l[1] = { ldg(f2 + i) }, d2h[1] = { ldg(f2 + i + 1) };
+    quinticSegment<1>(x, ldg(xv + i), ldg(xv + i + 1), fl, fh, d1l, d1h, d2l, d2h, f, df, d2f);
+}
+
+/// potential::Interpolator::evalDeriv (src/potential_utils.cpp:872-911): Phi(R), dPhi/dR, d2Phi/dR2
+__device__ void interpPhi(const FudgeTables& F, double R, double* val, double* der, double* der2)
+{
+    const double logR = log(R);
+    if(logR > ldg(F.PhiofR.t + F.PhiofR.n - 1) && F.coefOut != 0) {
+        const double Rs = exp(logR * F.slopeOut);
+        const double Phi = (-F.massOut + (F.slopeOut == -1 ? logR : (R * Rs - 1) / (F.slopeOut + 1)) * F.coefOut) / R;
+        *val = Phi;
+        *der = (-Phi + F.coefOut * Rs) / R;
+        *der2 = (2 * Phi + F.coefOut * Rs * (F.slopeOut - 2)) / pow2(R);
+        return;
+    }
+    double s, d1, d2;
+    spline1d(F.PhiofR, logR, &s, &d1, &d2);
+    const double ex = exp(s), E = 1 / (F.iInvPhi0 - ex), dE = E * E * ex, d2E = E * dE * (F.iInvPhi0 + ex);
+    *val = E;
+    *der = dE * d1 / R;
+    *der2 = (dE * (d2 - d1) + d2E * d1 * d1) / pow2(R);
+}
+
+/// potential::Interpolator::L_circ (src/potential_utils.cpp:954-980)
+__device__ double interpLcirc(const FudgeTables& F, double E)
+{
+    if(!(E >= 1. / F.iInvPhi0 && E <= 0))
+        return NAN;
+    const double scaledE = log(F.iInvPhi0 - 1 / E);
+    double logL;
+    spline1d(F.LofE, scaledE, &logL, nullptr, nullptr);
+    double Lcirc = exp(logL);
+    if(scaledE > ldg(F.LofE.t + F.LofE.n - 1)) {   // large-radius correction
+        double logR;
+        spline1d(F.RofL, logL, &logR, nullptr, nullptr);
+        const double Rc = exp(logR);
+        double Phi, dPhi, d2Phi;
+        interpPhi(F, Rc, &Phi, &dPhi, &d2Phi);
+        const double Ec = Phi + 0.5 * Rc * dPhi;
+        const double denom = 1 - 0.5 * (Ec - E) * (Rc * d2Phi - dPhi) / ((Rc * d2Phi + 3 * dPhi) * Rc * dPhi);
+        Lcirc = clip(sqrt(Rc * dPhi) * (Rc - (Ec - E) / (dPhi * denom)), 0.75 * Lcirc, 1.25 * Lcirc);
+    }
+    return Lcirc;
+}
+
+/// bilinear Delta(xi, chi) (LinearInterpolator2d::evalDeriv, src/math_spline.cpp:2152-2190)
+__device__ double deltaLookup(const FudgeTables& F, double x, double y)
+{
+    const int nx = F.nE, ny = F.nL;
+    const int xi = binSearch(x, F.gridE, nx), yi = binSearch(y, F.gridL, ny);
+    if(xi < 0 || xi >= nx - 1 || yi < 0 || yi >= ny - 1)
+        return NAN;
+    const double* f = F.delta + static_cast<size_t>(xi) * ny + yi;
+    const double zll = ldg(f), zlu = ldg(f + 1), zul = ldg(f + ny), zuu = ldg(f + ny + 1);
+    const double xl = ldg(F.gridE + xi), yl = ldg(F.gridL + yi);
+    const double t = (x - xl) / (ldg(F.gridE + xi + 1) - xl), u = (y - yl) / (ldg(F.gridL + yi + 1) - yl);
+    const double T = 1 - t, U = 1 - u;
+    return T * (U * zll + u * zlu) + t * (U * zul + u * zuu);
+}
+
+/// the fudge's auxiliary function F(tau) and the integrals of motion of one point
+struct FudgeFunction {
+    const MultipoleView* M;
+    double lambda, nu, phi, D2;     // point in prolate spheroidal coordinates (Delta^2 = D2)
+    double E, Lz, I3, flambda, fnu;
+    int bad;                        // set when a coordinate conversion is invalid
+
+    /// F(tau) and optionally F', F'' (src/actions_staeckel.cpp:202-252)
+    template<bool DER, bool DER2>
+    __device__ void eval(double tau, double* val, double* der, double* der2) const
+    {
+        double lam, n, mult, I;
+        if(tau >= D2) { lam = tau; n = fabs(nu); mult = lam - n; I = I3 - fnu; }
+        else          { lam = lambda; n = tau; mult = n - lam; I = I3 - flambda; }
+        // prolate spheroidal -> cylindrical (src/coord.cpp:266-291)
+        const double absnu = fabs(n), sgn = n >= 0 ? 1 : -1;
+        const double lmd = lam - D2, nmd = absnu - D2;
+        if(nmd > 0 || lmd < 0) {
+            *val = NAN; if(DER) *der = NAN; if(DER2) *der2 = NAN;
+            return;
+        }
+        const double R = sqrt(lmd * (1 - absnu / D2));
+        const double z = sqrt(lam * absnu / D2) * sgn;
+        double Phi;
+        CylDerivs g; CylHess h;
+        if(DER2)     evalMultipoleCyl<6>(*M, R, z, phi, &Phi, &g, &h);
+        else if(DER) evalMultipoleCyl<3>(*M, R, z, phi, &Phi, &g, &h);
+        else         evalMultipoleCyl<1>(*M, R, z, phi, &Phi, &g, &h);
+        const double tmd = tau - D2;
+        *val = (tmd != 0 ? (E * tau - I - Phi * mult) * tmd : 0) - Lz * Lz / 2 * tau;
+        if(DER || DER2) {
+            const double dRdl = 0.5 * R / lmd, dRdn = 0.5 * R / nmd * sgn, dzdl = 0.5 * z / lam, dzdn = 0.5 * z / n;
+            const bool lbranch = tau >= D2;
+            const double dPhidtau = lbranch ? g.dR * dRdl + g.dz * dzdl : g.dR * dRdn + g.dz * dzdn;
+            if(DER)
+                *der = E * (tau + tmd) - Lz * Lz / 2 - I - (mult + tmd) * Phi -
+                       (tmd != 0 ? tmd * mult * dPhidtau : 0);
+            if(DER2) {
+                double d2;
+                if(lbranch) {
+                    const double d2Rdl2 = -0.25 * R / pow2(lmd), d2zdl2 = -0.25 * z / pow2(lam);
+                    d2 = h.dR2 * pow2(dRdl) + h.dz2 * pow2(dzdl) + 2 * h.dRdz * dRdl * dzdl +
+                         g.dR * d2Rdl2 + g.dz * d2zdl2;
+                } else {
+                    const double d2Rdn2 = -0.25 * R / pow2(nmd), d2zdn2 = -0.25 * z / pow2(n);
+                    d2 = h.dR2 * pow2(dRdn) + h.dz2 * pow2(dzdn) + 2 * h.dRdz * dRdn * dzdn +
+                         g.dR * d2Rdn2 + g.dz * d2zdn2;
+                }
+                *der2 = 2 * (E - Phi - (mult + tmd) * dPhidtau) - tmd * mult * d2;
+            }
+        }
+    }
+    __device__ double value(double tau) const { double v; eval<false, false>(tau, &v, nullptr, nullptr); return v; }
+};
+
+/// F(tau) with its first derivative, as the root finder sees it
+struct FudgeRootFn {
+    static constexpr bool hasDeriv = true;
+    const FudgeFunction* f;
+    __device__ void operator()(double x, double* v, double* d) const {
+        if(d) f->eval<true, false>(x, v, d, nullptr); else f->eval<false, false>(x, v, nullptr, nullptr);
+    }
+};
+
+/// F(tau)/tau^2 on [lambda_pos, inf) mapped to s in [0, 1] by the semi-infinite scaling
+/// (AxisymScaledForRootfinder inside ScaledFnc<ScalingSemiInf>, src/actions_staeckel.cpp:329-354,
+/// src/math_core.h:214-232)
+struct FudgeRootFnSemiInf {
+    static constexpr bool hasDeriv = true;
+    const FudgeFunction* f;
+    double u0;
+    __device__ void operator()(double s, double* v, double* d) const {
+        double duds;
+        const double tau = unscaleSemiInf(u0, s, d ? &duds : nullptr);
+        double fv, dfdu = NAN;
+        if(tau > 1e100) {
+            fv = f->E;
+        } else {
+            double fval, fder;
+            if(d) f->eval<true, false>(tau, &fval, &fder, nullptr); else f->eval<false, false>(tau, &fval, nullptr, nullptr);
+            fv = fval / pow2(tau);
+            if(d) dfdu = (fder - 2 * fval / tau) / pow2(tau);
+        }
+        *v = fv;
+        if(d) *d = dfdu * duds;
+    }
+};
+
+struct FudgeLimits { double lambda_min, lambda_max, nu_min, nu_max; int order; };
+
+/// integration limits of the lambda and nu motions; reference findIntegrationLimitsAxisym
+__device__ FudgeLimits fudgeLimits(const FudgeFunction& fnc, int* rootIters)
+{
+    FudgeLimits lim;
+    const double delta = fnc.D2;
+    const double f_zero = fnc.value(0);
+    double f_lambda, df_lambda, d2f_lambda;
+    fnc.eval<true, true>(fnc.lambda, &f_lambda, &df_lambda, &d2f_lambda);
+    lim.nu_min = 0;
+    lim.nu_max = lim.lambda_min = lim.lambda_max = NAN;
+    double nu_upper = delta, lambda_lower = delta;
+    FudgeRootFn rf{ &fnc };
+    int it;
+    if(fnc.Lz == 0) {
+        const double dminus = delta * (1 - 1e-15), dplus = delta * (1 + 1e-15);
+        if(fnc.value(dminus) < 0) {
+            if(f_zero > 0) nu_upper = dminus;
+            else lim.nu_max = lim.nu_min;
+        } else
+            lim.nu_max = delta;
+        if(fnc.value(dplus) < 0) lambda_lower = dplus;
+        else lim.lambda_min = delta;
+    }
+    if(!isFinite(lim.nu_max)) {
+        if(f_zero > 0) {
+            lim.nu_max = findRoot(rf, fabs(fnc.nu), nu_upper, FUDGE_ACCURACY_RANGE, &it);
+            *rootIters += it;
+        }
+        if(!isFinite(lim.nu_max))
+            lim.nu_max = fabs(fnc.nu);
+    }
+    double lambda_pos = fnc.lambda;
+    const double dxToRoot = -f_lambda / df_lambda;
+    if(f_lambda <= 0 || fabs(dxToRoot) < fnc.lambda * FUDGE_MINIMUM_RANGE) {
+        if(df_lambda >= 0) lim.lambda_min = fnc.lambda;
+        if(df_lambda <= 0) {
+            lim.lambda_max = fnc.lambda;
+            if(fnc.lambda == delta) lim.lambda_min = delta;
+        }
+        bool nearShell = d2f_lambda < 0 &&
+            pow2(df_lambda) - 2 * f_lambda * d2f_lambda - pow2(fnc.lambda * FUDGE_MINIMUM_RANGE * d2f_lambda) < 0;
+        const double safeOffset = fmin(0.5 * fabs(df_lambda / d2f_lambda), fnc.lambda * FUDGE_MINIMUM_RANGE);
+        lambda_pos += fmax(dxToRoot, safeOffset) * (df_lambda >= 0 ? 1 : -1);
+        double f_lp, df_lp, d2f_lp;
+        fnc.eval<true, true>(lambda_pos, &f_lp, &df_lp, &d2f_lp);
+        nearShell |= d2f_lp < 0 &&
+            pow2(df_lp) - 2 * f_lp * d2f_lp - pow2(fnc.lambda * FUDGE_MINIMUM_RANGE * d2f_lp) < 0;
+        if(nearShell || f_lp < 0)
+            lim.lambda_min = lim.lambda_max = fnc.lambda;
+    }
+    if(!isFinite(lim.lambda_min)) {
+        lim.lambda_min = findRoot(rf, lambda_lower, lambda_pos, FUDGE_ACCURACY_RANGE, &it);
+        *rootIters += it;
+    }
+    if(!isFinite(lim.lambda_max)) {
+        FudgeRootFnSemiInf sf{ &fnc, lambda_pos };
+        const double s = findRoot(sf, 0, 1, FUDGE_ACCURACY_RANGE, &it);
+        *rootIters += it;
+        lim.lambda_max = unscaleSemiInf(lambda_pos, s, nullptr);
+    }
+    if(!(lim.nu_max >= delta * FUDGE_MINIMUM_RANGE))
+        lim.nu_max = 0;
+    if(!(lim.lambda_max - lim.lambda_min >= delta * FUDGE_MINIMUM_RANGE))
+        lim.lambda_min = lim.lambda_max = fnc.lambda;
+    const double ratio = sqrt((lim.lambda_min - delta) / (lim.lambda_max - delta));
+    if(ratio == 0) lim.order = GL_MAX_ORDER;
+    else {
+        int e;
+        frexp(ratio, &e);
+        lim.order = min(GL_MAX_ORDER, FUDGE_INTEGR_ORDER - e);
+    }
+    return lim;
+}
+
+/// integral of sqrt(p^2(tau)) over [lo, hi] with the cubic end-point stretch
+/// (integrateGL of ScaledIntegrand<ScalingCub>(AxisymIntegrand), src/math_core.cpp:1191-1205)
+__device__ double fudgeMomentumIntegral(const FudgeFunction& fnc, const GLRules& gl, double lo, double hi, int order)
+{
+    int N = order < 1 ? 1 : order;
+    while(gl.offset[N] < 0) N++;
+    const double* x = gl.nodes + gl.offset[N];
+    const double* w = gl.weights + gl.offset[N];
+    double sum = 0;
+    for(int i = 0; i < N; i++) {
+        double duds;
+        const double tau = unscaleCub(lo, hi, ldg(x + i), &duds);
+        const double tmd = tau - fnc.D2;
+        const double p2 = fnc.value(tau) / (2 * pow2(tmd) * tau);
+        double v = p2 < 0 ? 0 : sqrt(p2);
+        if(!isFinite(v)) v = 0;
+        sum += ldg(w + i) * (v * duds);
+    }
+    return sum;
+}
+
+/** Actions (Jr, Jz, Jphi) of one point (R, z, phi, vR, vz, vphi) for focal distance fd
+    (evalAxisymFudge: fd <= 0 falls back to max(R,1)*1e-4); Phi is the potential at the point. */
+__device__ void fudgeActions(const MultipoleView& M, const GLRules& gl, const double* pc, double Phi,
+    double fd, double* act, int* rootIters)
+{
+    const double R = pc[0], z = pc[1], phi = pc[2], vR = pc[3], vz = pc[4], vphi = pc[5];
+    if(fd <= 0) fd = fmax(R, 1.) * 1e-4;
+    const double D2 = fd * fd;
+    // cylindrical -> prolate spheroidal (src/coord.cpp:294-338) and velocities (:525-531)
+    const double R2 = R * R, z2 = z * z, signz = z >= 0 ? 1 : -1;
+    const double sum = R2 + z2 + D2, dif = R2 + z2 - D2;
+    double sqD = sqrt(pow2(dif) + 4 * R2 * D2);
+    if(z2 == 0) sqD = sum;
+    if(R2 == 0) sqD = fabs(dif);
+    double lmd, dmn;
+    if(dif >= 0) { lmd = 0.5 * (sqD + dif); dmn = R2 > 0 ? D2 * R2 / lmd : 0; }
+    else         { dmn = 0.5 * (sqD - dif); lmd = D2 * R2 / dmn; }
+    const double lambda = D2 + lmd;
+    double absnu = 2 * D2 / (sum + sqD) * z2;
+    if(absnu * 2 > D2) absnu = D2 - dmn; else dmn = D2 - absnu;
+    const double Lz = R * vphi;
+    if(sqD == 0) { act[0] = act[1] = NAN; act[2] = Lz; return; }   // lambda = nu = Delta^2: undefined
+    FudgeFunction fnc;
+    fnc.M = &M;
+    fnc.lambda = lambda;
+    fnc.nu = absnu * signz;
+    fnc.phi = phi;
+    fnc.D2 = D2;
+    fnc.bad = 0;
+    double Phi0;
+    CylDerivs g; CylHess h;
+    evalMultipoleCyl<1>(M, sqrt(lambda - D2), 0, phi, &Phi0, &g, &h);
+    const double Ekin = 0.5 * (vR * vR + vz * vz + vphi * vphi);
+    fnc.E = Phi + Ekin;
+    fnc.Lz = Lz;
+    fnc.flambda = -lambda * Phi0;
+    fnc.fnu = fnc.flambda + Phi * (lambda - absnu);
+    fnc.I3 = lambda * (Phi - Phi0) + 0.5 * (pow2(z * vphi) + pow2(R * vz - z * vR) + pow2(vz) * D2);
+    if(!isFinite(fnc.E + fnc.I3 + fnc.Lz) || fnc.E >= 0) {
+        act[0] = act[1] = NAN; act[2] = Lz;
+        return;
+    }
+    const FudgeLimits lim = fudgeLimits(fnc, rootIters);
+    act[0] = fudgeMomentumIntegral(fnc, gl, lim.lambda_min, lim.lambda_max, lim.order) / M_PI;
+    act[1] = fudgeMomentumIntegral(fnc, gl, lim.nu_min, lim.nu_max, lim.order) / M_PI * 2;
+    act[2] = Lz;
+}
+
+/// Cartesian posvel -> cylindrical (R, z, phi, vR, vz, vphi); reference src/coord.cpp:476-484
+__device__ __forceinline__ void carToCylPosVel(const double* w, double* pc)
+{
+    const double R = sqrt(w[0] * w[0] + w[1] * w[1]);
+    if(R == 0) {
+        pc[0] = 0; pc[1] = w[2]; pc[2] = atan2(w[4], w[3]);
+        pc[3] = sqrt(w[3] * w[3] + w[4] * w[4]); pc[4] = w[5]; pc[5] = 0;
+        return;
+    }
+    const double c = w[0] / R, s = w[1] / R;
+    pc[0] = R; pc[1] = w[2]; pc[2] = atan2(w[1], w[0]);
+    pc[3] = w[3] * c + w[4] * s;
+    pc[4] = w[5];
+    pc[5] = -w[3] * s + w[4] * c;
+}
+
+/** focal distance of the action finder at a point with potential Phi: E, Lz -> Lcirc(E) ->
+    (xi, chi) -> Delta; reference ActionFinderAxisymFudge::eval steps 0-1,
+    src/actions_staeckel.cpp:957-977 */
+__device__ double finderFocalDistance(const FudgeTables& F, const double* pc, double Phi)
+{
+    const double E = Phi + 0.5 * (pc[3] * pc[3] + pc[4] * pc[4] + pc[5] * pc[5]);
+    const double Lz = pc[0] * pc[5];
+    const double Lcirc = interpLcirc(F, E);
+    const double xi = clip(log(F.invPhi0 - 1 / E), ldg(F.gridE), ldg(F.gridE + F.nE - 1));
+    const double Lzrel = clip(fabs(Lz) / Lcirc, 0., 1.);
+    const double chi = scaleCub(0, 1, Lzrel);
+    return fmax(0., deltaLookup(F, xi, chi));
+}
+
+}  // namespace agb

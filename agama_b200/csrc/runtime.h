@@ -6,6 +6,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "multipole.h"
+#include "fudge_types.h"
 
 namespace agb {
 
@@ -57,11 +58,27 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
 
 struct OrbitParams;
 
+/// a Staeckel-fudge action finder: tables on the device of its potential
+struct DeviceActionFinder {
+    DevicePotential* pot = nullptr;   // not owned
+    FinderTablesHost host;
+    DevBuf<double> gridE, gridL, delta, lofe, rofl, phiofr;
+    FudgeTables view;
+};
+DeviceActionFinder* createDeviceActionFinder(DevicePotential* pot, const FinderTablesHost& T);
+
 /// launch helpers (defined in the .cu files)
 void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
     double* grad, double* hess, cudaStream_t stream);
 /// DOP853 batch; queue != nullptr selects the persistent work-queue mapping (8-byte counter)
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream);
+
+/// Staeckel fudge with a given focal distance per point (fd) or one for all (fd0 when fd is null)
+void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
+    double* act, int* iters, cudaStream_t stream);
+/// Staeckel fudge with the focal distance from the action finder's table
+void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
+    double* act, double* fdOut, int* iters, cudaStream_t stream);
 
 }  // namespace agb

@@ -91,6 +91,58 @@ int agama_integrateOrbitsManyDevice(const agama_Potential* potential, long n, co
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, long* numRejected, int* status, int useQueue, void* stream);
 
+/* ---------------------------------------------------------------------------------------
+   Staeckel-fudge actions (axisymmetric potentials only).  posvel: n x 6 Cartesian points;
+   act: n x 3 (Jr, Jz, Jphi); unbound points (E >= 0) give Jr = Jz = NaN, as in the reference
+   (src/actions_staeckel.cpp:648-656). */
+
+/* reference: agama_deleteActionFinder, src/interface_c.h:118 */
+void agama_deleteActionFinder(agama_ActionFinder* actionFinder);
+
+/* reference: agama_evalActionsAnglesFrequencies, src/interface_c.h:135 (src/interface_c.cpp:129-155):
+   actions of one point through the action finder; angles / frequencies are not computed by
+   this engine (they come back NaN with a message in agama_getError()). */
+void agama_evalActionsAnglesFrequencies(const agama_ActionFinder* actionFinder, const double posvel[6],
+    double actions[3], double angles[3], double frequencies[3]);
+
+/* reference: agama_evalActionsAnglesFrequenciesStandalone, src/interface_c.h:155
+   (src/interface_c.cpp:157-192): actions of one point for a given focal distance fd
+   (actions::evalAxisymFudge, src/actions_staeckel.cpp:683-693). */
+void agama_evalActionsAnglesFrequenciesStandalone(const agama_Potential* potential, double fd,
+    const double posvel[6], double actions[3], double angles[3], double frequencies[3]);
+
+/* An action finder from precomputed tables: the focal-distance grid Delta(scaledE, chi) of
+   ActionFinderAxisymFudge (gridE[nE] = ln(1/Phi0 - 1/E), gridL[nL] = chi = s(Lz/Lcirc),
+   delta[nE x nL]; src/actions_staeckel.cpp:751-795) and the L_circ(E) interpolator of
+   potential::Interpolator (quintic splines LofE, RofL, PhiofR stored as [x | f | f' | f''] with
+   n nodes each; scalars = {1/Phi0 of the finder, 1/Phi0 of the interpolator, slopeOut,
+   coefOut, massOut}; src/potential_utils.cpp:757-980). */
+agama_ActionFinder* agama_createActionFinderFromTables(const agama_Potential* potential,
+    int nE, const double* gridE, int nL, const double* gridL, const double* delta,
+    int nLofE, const double* LofE, int nRofL, const double* RofL, int nPhiofR, const double* PhiofR,
+    const double* scalars);
+
+/* Batched actions through the action finder, host buffers; fdOut (n, may be NULL) receives the
+   focal distance used for each point.  Replaces n calls of agama_evalActionsAnglesFrequencies
+   / ActionFinderAxisymFudge::eval (src/actions_staeckel.cpp:954-979) as batched by the
+   reference's Python ActionFinder (src/interface_python.cpp:3761-3822). */
+int agama_evalActionsMany(const agama_ActionFinder* actionFinder, long n, const double* posvel,
+    double* act, double* fdOut);
+
+/* The same on device buffers. */
+int agama_evalActionsManyDevice(const agama_ActionFinder* actionFinder, long n, const double* posvel,
+    double* act, double* fdOut, void* stream);
+
+/* Batched actions for given focal distances fd[n] (or fd0 for all points when fd is NULL);
+   replaces n calls of agama_evalActionsAnglesFrequenciesStandalone. */
+int agama_evalActionsStandaloneMany(const agama_Potential* potential, long n, const double* posvel,
+    const double* fd, double fd0, double* act);
+
+/* The same on device buffers; rootIters (n, may be NULL) receives the number of root-finder
+   iterations spent on each point. */
+int agama_evalActionsStandaloneManyDevice(const agama_Potential* potential, long n, const double* posvel,
+    const double* fd, double fd0, double* act, int* rootIters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

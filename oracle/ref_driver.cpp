@@ -169,8 +169,10 @@ int ref_orbits_many(void* handle, long n, const double* ic, const double* T, dou
             orbint.run(T[i]);
             if(traj.empty()) ic6.unpack_to(final + 6*i);
             else traj[0].first.unpack_to(final + 6*i);
+            // the reference reports no status: infer "stopped before T" from the last recorded time
+            const bool reachedEnd = T[i] == 0 || (!traj.empty() && traj[0].second == T[i]);
             if(nsteps) nsteps[i] = cnt;
-            if(status) status[i] = 0;
+            if(status) status[i] = reachedEnd ? 0 : 1;
         } catch(std::exception& e) {
             if(status) status[i] = -1;
 #pragma omp critical

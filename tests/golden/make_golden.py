@@ -154,6 +154,44 @@ def make_orbit_vectors():
     print("cfg3 orbits", len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max())
 
 
+def action_points(pot, n, seed, Rd=3.0, hz=0.3):
+    """disk-like points of the benchmark distribution plus edge cases: in the plane (z = 0),
+    no rotation (Lz = 0), counter-rotating, nearly circular, on the z axis, unbound"""
+    vc = workloads.vcirc_from_force(lambda p: -pot.eval(p)[1])
+    w = workloads.disk_particles(n, vc, seed=seed, Rd=Rd, hz=hz)
+    v1 = float(vc(np.array([1.0]))[0])
+    v5 = float(vc(np.array([5.0]))[0])
+    edge = np.array([
+        [2.0, 0.0, 0.0, 0.05, v1 * 0.9, 0.03],      # in the equatorial plane
+        [3.0, 0.0, 0.4, 0.1, 0.0, 0.05],            # Lz = 0
+        [-4.0, 1.0, -0.3, 0.02, -0.1, 0.01],        # counter-rotating (Lz < 0)
+        [5.0, 0.0, 0.0, 0.0, v5, 0.0],              # circular orbit in the plane
+        [5.0, 0.0, 0.0, 0.0, v5, 1e-6],             # nearly circular
+        [0.0, 0.0, 1.5, 0.1, 0.05, 0.02],           # on the z axis
+        [1.0, 0.5, 0.2, 3.0, 2.0, 1.0],             # unbound (E > 0)
+        [8.0, -2.0, 3.0, -0.05, 0.1, 0.12],         # thick, eccentric
+    ])
+    return np.vstack([w, edge])
+
+
+def make_action_vectors():
+    for name, n, seed in [("cfg2", 2000, 303), ("cfg5", 600, 606), ("cfg4", 600, 505)]:
+        coef = coef_path(name)
+        pot = ref.Potential(file=coef)
+        pts = action_points(pot, n, seed)
+        af = ref.ActionFinder(pot)
+        af.evalcount(reset=True)
+        act_af, fd = af.actions(pts, with_fd=True)
+        evals_per_point = af.evalcount(reset=True) / len(pts)
+        act_fd, counts = pot.actions_fd(pts, fd, count=True)
+        tab = af.tables()
+        np.savez_compressed(os.path.join(HERE, "actions_%s.npz" % name), points=pts, fd=fd,
+                            act_finder=act_af, act_fd=act_fd, evals_fd=counts,
+                            evals_per_point_finder=evals_per_point, **{"tab_" + k: v for k, v in tab.items()})
+        print(name, "actions", len(pts), "evals/point %.1f" % evals_per_point,
+              "table", tab["delta"].shape, "LofE", tab["lofe"].shape)
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     if what in ("potentials", "all"):
@@ -161,3 +199,5 @@ if __name__ == "__main__":
         make_potential_vectors()
     if what in ("orbits", "all"):
         make_orbit_vectors()
+    if what in ("actions", "all"):
+        make_action_vectors()

@@ -1,0 +1,86 @@
+"""Parity of the device Staeckel-fudge actions with the reference (golden vectors from
+tests/golden/make_golden.py: actions::evalAxisymFudge for given focal distances, and
+ActionFinderAxisymFudge with its own focal-distance table).
+
+Bound (engine specification): actions agree to 1e-6 relative.  For components that vanish
+(Jr of a circular orbit, Jz of a planar one) the bound is taken relative to the total action
+|Jr| + |Jz| + |Jphi|: |dJ_i| <= 1e-6 |J_i| + 1e-9 (|Jr| + |Jz| + |Jphi|).
+Unbound points (E >= 0) give NaN for Jr, Jz in both."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+CFGS = ["cfg2", "cfg5", "cfg4"]
+
+
+def check_actions(J, Jref, tol=1e-6):
+    nan_ref = ~np.isfinite(Jref)
+    assert np.array_equal(~np.isfinite(J), nan_ref), "NaN pattern differs"
+    ok = ~np.any(nan_ref, axis=1)
+    J, Jref = J[ok], Jref[ok]
+    scale = np.sum(np.abs(Jref), axis=1, keepdims=True)
+    err = np.abs(J - Jref)
+    bound = tol * np.abs(Jref) + 1e-9 * scale
+    worst = np.argmax(np.max(err / bound, axis=1))
+    assert np.all(err <= bound), ("worst", J[worst], Jref[worst], np.max(err / bound))
+    return np.max(err / np.maximum(np.abs(Jref), 1e-300) * (np.abs(Jref) > 1e-6 * scale))
+
+
+def tables(g):
+    return {k[4:]: g[k] for k in g.files if k.startswith("tab_")}
+
+
+@pytest.mark.parametrize("cfg", CFGS)
+def test_actions_fixed_focal_distance(cfg):
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "actions_%s.npz" % cfg))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    J = agama_b200.actions(pot, g["points"], fd=g["fd"])
+    check_actions(J, g["act_fd"])
+
+
+@pytest.mark.parametrize("cfg", CFGS)
+def test_action_finder(cfg):
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "actions_%s.npz" % cfg))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    af = agama_b200.ActionFinder(pot, tables=tables(g))
+    J, fd = af(g["points"], fd=True)
+    # the focal distance comes from the same bilinear table: round-off level agreement
+    fin = np.isfinite(g["fd"]) & (g["fd"] > 0)
+    assert np.allclose(fd[fin], g["fd"][fin], rtol=1e-10, atol=0)
+    check_actions(J, g["act_finder"])
+
+
+def test_actions_device_pointers_and_single_point():
+    import ctypes
+    import torch
+    import agama_b200
+    from agama_b200 import _native
+    g = np.load(os.path.join(GOLDEN, "actions_cfg2.npz"))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg2.coef"))
+    af = agama_b200.ActionFinder(pot, tables=tables(g))
+    host = af(g["points"])
+    dev = af(torch.tensor(g["points"], device="cuda"))
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), host, equal_nan=True)
+    # the reference-named single-point entry points
+    p = np.ascontiguousarray(g["points"][5])
+    act = np.zeros(3)
+    _native.lib().agama_evalActionsAnglesFrequencies(af.handle, _native.ptr(p), _native.ptr(act), None, None)
+    assert np.array_equal(act, host[5])
+    _native.lib().agama_evalActionsAnglesFrequenciesStandalone(pot.handle, ctypes.c_double(g["fd"][5]),
+                                                              _native.ptr(p), _native.ptr(act), None, None)
+    assert np.allclose(act, g["act_fd"][5], rtol=1e-6)
+
+
+def test_actions_reject_non_axisymmetric():
+    import agama_b200
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+    with pytest.raises(RuntimeError, match="axisymmetric"):
+        agama_b200.actions(pot, np.ones((2, 6)), fd=1.0)
