@@ -339,3 +339,51 @@ extern "C" void agama_evalActionsAnglesFrequenciesStandalone(const agama_Potenti
     if(angles) { angles[0] = angles[1] = angles[2] = NAN; setError("angles are not provided by this engine yet"); }
     if(frequencies) { frequencies[0] = frequencies[1] = frequencies[2] = NAN; setError("frequencies are not provided by this engine yet"); }
 }
+
+// ------------------------------------------------------------------------------------------
+// device FP64 throughput probe (the roofline denominator for the FP64-bound kernels)
+
+namespace {
+__global__ void fp64FmaProbe(double* out, int iters)
+{
+    // 8 independent FMA chains per thread keep the FP64 pipe busy
+    double a[8];
+    const double b = 1.0000001, c = 1e-9;
+    for(int k = 0; k < 8; k++) a[k] = threadIdx.x * 1e-7 + k;
+    for(int i = 0; i < iters; i++)
+#pragma unroll
+        for(int k = 0; k < 8; k++) a[k] = fma(a[k], b, c);
+    double s = 0;
+    for(int k = 0; k < 8; k++) s += a[k];
+    if(s == 12345.678) out[0] = s;   // keeps the chains live
+}
+}  // namespace
+
+extern "C" int agama_measureFP64Throughput(double* tflops)
+{
+    return guarded([&] {
+        requireDevice();
+        int dev, sms;
+        AGB_CUDA(cudaGetDevice(&dev));
+        AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        DevBuf<double> out(1);
+        const int block = 256, grid = sms * 8, iters = 4096;
+        cudaEvent_t e0, e1;
+        AGB_CUDA(cudaEventCreate(&e0));
+        AGB_CUDA(cudaEventCreate(&e1));
+        fp64FmaProbe<<<grid, block>>>(out.ptr, iters);   // warm-up
+        float best = 1e30f;
+        for(int rep = 0; rep < 5; rep++) {
+            AGB_CUDA(cudaEventRecord(e0));
+            fp64FmaProbe<<<grid, block>>>(out.ptr, iters);
+            AGB_CUDA(cudaEventRecord(e1));
+            AGB_CUDA(cudaEventSynchronize(e1));
+            float ms;
+            AGB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, ms);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *tflops = 2.0 * 8 * iters * static_cast<double>(grid) * block / (best * 1e-3) / 1e12;
+    });
+}

@@ -143,6 +143,12 @@ int agama_evalActionsStandaloneMany(const agama_Potential* potential, long n, co
 int agama_evalActionsStandaloneManyDevice(const agama_Potential* potential, long n, const double* posvel,
     const double* fd, double fd0, double* act, int* rootIters, void* stream);
 
+/* ---------------------------------------------------------------------------------------
+   Measurement helper (no reference counterpart): FP64 fused-multiply-add throughput of the
+   current device in TFLOP/s, measured with independent FMA chains; the roofline denominator
+   of the FP64-bound kernels above. */
+int agama_measureFP64Throughput(double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

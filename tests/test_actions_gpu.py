@@ -51,9 +51,10 @@ def test_action_finder(cfg):
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
     af = agama_b200.ActionFinder(pot, tables=tables(g))
     J, fd = af(g["points"], fd=True)
-    # the focal distance comes from the same bilinear table: round-off level agreement
-    fin = np.isfinite(g["fd"]) & (g["fd"] > 0)
-    assert np.allclose(fd[fin], g["fd"][fin], rtol=1e-10, atol=0)
+    # the focal distance comes from the same bilinear table: round-off level agreement (where
+    # the table is ~0 the sign of the round-off decides between a tiny Delta and max(0, .) = 0)
+    fin = np.isfinite(g["fd"])
+    assert np.allclose(fd[fin], g["fd"][fin], rtol=1e-10, atol=1e-8 * np.max(g["fd"][fin]))
     check_actions(J, g["act_finder"])
 
 
