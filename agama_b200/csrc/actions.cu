@@ -71,8 +71,8 @@ const GLRules& glRulesForCurrentDevice()
 /// One point per thread.  FINDER: Delta from the finder's table; otherwise from fd[i] (or fd0 if
 /// fd is null).  Outputs actions (Jr, Jz, Jphi), optionally Delta and root-finder iterations.
 template<bool FINDER>
-__global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const MultipoleView M, const GLRules gl,
-    const FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd, double fd0,
+__global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const __grid_constant__ MultipoleView M, const GLRules gl,
+    const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd, double fd0,
     double* __restrict__ act, double* __restrict__ fdOut, int* __restrict__ iters)
 {
     const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const MultipoleView M
     carToCylPosVel(w, pc);
     double Phi;
     CylDerivs g; CylHess h;
-    evalMultipoleCyl<1>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
+    evalMultipoleCylCall<1, EVAL_AXI>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
     const double delta = FINDER ? finderFocalDistance(F, pc, Phi) : (fd ? fd[i] : fd0);
     double a[3];
     int it = 0;

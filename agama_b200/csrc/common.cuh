@@ -20,6 +20,8 @@ namespace agb {
 constexpr int LMAX_MAX = 16;
 /// number of doubles stored per node of a 2-D quintic spline (9 used + 1 pad for 16-byte loads)
 constexpr int NODE_STRIDE = 10;
+/// most azimuthal harmonics the register-resident spline evaluator handles
+constexpr int FAST_MAX_HARMONICS = 8;
 
 /// sqrt(pi) to the digits the reference library uses (its M_SQRTPI)
 constexpr double SQRT_PI = 1.77245385090551602729816748334;
@@ -27,7 +29,8 @@ constexpr double SQRT_PI = 1.77245385090551602729816748334;
 AGB_HD double pow2(double x) { return x * x; }
 AGB_HD double signOf(double x) { return x > 0 ? 1. : x < 0 ? -1. : 0.; }
 AGB_HD bool isFinite(double x) { return x == x && x != INFINITY && x != -INFINITY; }
-AGB_HD double clip(double x, double lo, double hi) { return x < lo ? lo : x > hi ? hi : x; }
+/// clamp to [lo, hi]; NaN maps to lo (as math::clip, reference src/math_core.h:29)
+AGB_HD double clip(double x, double lo, double hi) { return x > hi ? hi : x > lo ? x : lo; }
 AGB_HD bool signBit(double x) {
 #ifdef __CUDA_ARCH__
     return signbit(x);

@@ -121,9 +121,9 @@ struct FudgeFunction {
         const double z = sqrt(lam * absnu / D2) * sgn;
         double Phi;
         CylDerivs g; CylHess h;
-        if(DER2)     evalMultipoleCyl<6>(*M, R, z, phi, &Phi, &g, &h);
-        else if(DER) evalMultipoleCyl<3>(*M, R, z, phi, &Phi, &g, &h);
-        else         evalMultipoleCyl<1>(*M, R, z, phi, &Phi, &g, &h);
+        if(DER2)     evalMultipoleCylCall<6, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
+        else if(DER) evalMultipoleCylCall<3, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
+        else         evalMultipoleCylCall<1, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         const double tmd = tau - D2;
         *val = (tmd != 0 ? (E * tau - I - Phi * mult) * tmd : 0) - Lz * Lz / 2 * tau;
         if(DER || DER2) {
@@ -312,7 +312,7 @@ __device__ void fudgeActions(const MultipoleView& M, const GLRules& gl, const do
     fnc.bad = 0;
     double Phi0;
     CylDerivs g; CylHess h;
-    evalMultipoleCyl<1>(M, sqrt(lambda - D2), 0, phi, &Phi0, &g, &h);
+    evalMultipoleCylCall<1, EVAL_AXI>(M, sqrt(lambda - D2), 0, phi, &Phi0, &g, &h);
     const double Ekin = 0.5 * (vR * vR + vz * vz + vphi * vphi);
     fnc.E = Phi + Ekin;
     fnc.Lz = Lz;

@@ -54,6 +54,11 @@ struct MultipoleView {
     int logScaling;
     double invPhi0;
     PowerLawView inner, outer;
+    /// the non-empty harmonics for the register-resident evaluator: m = 0 first, then the others
+    /// by ascending m; nFast = 0 when there are more than FAST_MAX_HARMONICS of them
+    int nFast;
+    int fastM[FAST_MAX_HARMONICS];
+    int fastSlot[FAST_MAX_HARMONICS];
 };
 
 /** Host-side Multipole: owns the tables built from the radial grid and the coefficients

@@ -385,10 +385,143 @@ __device__ void evalInterp2d(const MultipoleView& M, double R, double z, double 
     }
 }
 
+/** The same 2-D spline evaluation with the harmonics held in registers: at most MAXS non-empty
+    azimuthal harmonics, listed in M.fastM / M.fastSlot with m = 0 first and the others in
+    ascending m (the order in which the reference sums them), so every array index is a
+    compile-time constant after unrolling and nothing goes to local memory.  cos/sin(|m| phi)
+    come from the same multiple-angle recurrence as trigMultiAngle. */
+template<int NQ, int MAXS>
+__device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double R, double z, double phi,
+    double* pot, CylDerivs* g, CylHess* h)
+{
+    const double r = sqrt(R * R + z * z), logr = log(r), rpRinv = 1. / (r + fabs(R));
+    const double tau = R == 0 ? signOf(z) : z * rpRinv;
+    const int xi = binSearch(logr, M.lnr, M.nr), yi = binSearch(tau, M.tau, M.nt);
+    const bool inside = !(xi < 0 || xi >= M.nr - 1 || yi < 0 || yi >= M.nt - 1);
+    const int xs = inside ? xi : 0, ys = inside ? yi : 0;
+    const double xl = M.lnr[xs], xh = M.lnr[xs + 1], yl = M.tau[ys], yh = M.tau[ys + 1];
+    const size_t slotStride = static_cast<size_t>(M.nr) * M.nt * NODE_STRIDE;
+    double P[MAXS], Dr[MAXS], Dt[MAXS], Drr[MAXS], Drt[MAXS], Dtt[MAXS];
+#pragma unroll
+    for(int s = 0; s < MAXS; s++) {
+        if(s < M.nFast) {
+            spline2dCell<NQ>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
+                &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
+            if(!inside) P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = NAN;
+        }
+    }
+    if(M.logScaling) {
+        const double ex = exp(P[0]), val = 1 / (M.invPhi0 - ex);
+        P[0] = val;
+        if(NQ >= 3) {
+            const double dPdX = val * val * ex;
+            if(NQ == 6) {
+                const double d2PdX2 = dPdX * val * (M.invPhi0 + ex);
+                Drr[0] = dPdX * Drr[0] + d2PdX2 * Dr[0] * Dr[0];
+                Dtt[0] = dPdX * Dtt[0] + d2PdX2 * Dt[0] * Dt[0];
+                Drt[0] = dPdX * Drt[0] + d2PdX2 * Dr[0] * Dt[0];
+            }
+            Dr[0] *= dPdX;
+            Dt[0] *= dPdX;
+        }
+#pragma unroll
+        for(int s = 1; s < MAXS; s++) {
+            if(s < M.nFast) {
+                if(NQ == 6) {
+                    Drr[s] = Drr[s] * P[0] + P[s] * Drr[0] + 2 * Dr[s] * Dr[0];
+                    Dtt[s] = Dtt[s] * P[0] + P[s] * Dtt[0] + 2 * Dt[s] * Dt[0];
+                    Drt[s] = Drt[s] * P[0] + P[s] * Drt[0] + Dr[s] * Dt[0] + Dt[s] * Dr[0];
+                }
+                if(NQ >= 3) {
+                    Dr[s] = Dr[s] * P[0] + P[s] * Dr[0];
+                    Dt[s] = Dt[s] * P[0] + P[s] * Dt[0];
+                }
+                P[s] *= P[0];
+            }
+        }
+    }
+    // Fourier synthesis in the reference's order: m = 0, then the others by ascending m
+    SphDerivs gs; SphHess hs;
+    *pot = P[0];
+    if(NQ >= 3) { gs.dr = Dr[0]; gs.dt = Dt[0]; gs.dphi = 0; }
+    if(NQ == 6) { hs.dr2 = Drr[0]; hs.drdt = Drt[0]; hs.dt2 = Dtt[0]; hs.drdphi = hs.dtdphi = hs.dphi2 = 0; }
+    if(MAXS > 1 && M.nFast > 1) {
+        double cm[MAXS], sm[MAXS];
+        double s1, c1, sh, ch;
+        sincos(phi, &s1, &c1);
+        sincos(0.5 * phi, &sh, &ch);
+        const double alpha = 2 * sh * sh, beta = s1;
+        double cp = 1, sp = 0;
+#pragma unroll
+        for(int k = 1; k <= LMAX_MAX; k++) {
+            if(k <= M.ind.mmax) {
+                const double c = cp - (alpha * cp + beta * sp), sv = sp - (alpha * sp - beta * cp);
+#pragma unroll
+                for(int s = 1; s < MAXS; s++)
+                    if(M.fastM[s] == k || M.fastM[s] == -k) { cm[s] = c; sm[s] = sv; }
+                cp = c;
+                sp = sv;
+            }
+        }
+#pragma unroll
+        for(int s = 1; s < MAXS; s++) {
+            if(s < M.nFast) {
+                const int m = M.fastM[s];
+                const double tr = m > 0 ? cm[s] : sm[s];
+                const double dtr = m > 0 ? -m * sm[s] : -m * cm[s];
+                const double d2tr = -m * m * tr;
+                *pot += P[s] * tr;
+                if(NQ >= 3) {
+                    gs.dr += Dr[s] * tr;
+                    gs.dt += Dt[s] * tr;
+                    gs.dphi += P[s] * dtr;
+                }
+                if(NQ == 6) {
+                    hs.dr2 += Drr[s] * tr;
+                    hs.drdt += Drt[s] * tr;
+                    hs.dt2 += Dtt[s] * tr;
+                    hs.drdphi += Dr[s] * dtr;
+                    hs.dtdphi += Dt[s] * dtr;
+                    hs.dphi2 += P[s] * d2tr;
+                }
+            }
+        }
+    }
+    if(NQ == 1) return;
+    const double rinv = 1 / r, r2inv = rinv * rinv;
+    const double drdR = R * r2inv, drdz = z * r2inv, dtdR = -tau * rinv, dtdz = rinv - rpRinv;
+    g->dR = gs.dr * drdR + gs.dt * dtdR;
+    g->dz = gs.dr * drdz + gs.dt * dtdz;
+    g->dphi = gs.dphi;
+    if(NQ == 6) {
+        const double d2rdR2 = drdz * drdz - drdR * drdR, d2rdRdz = -2 * drdR * drdz, d2rdz2 = -d2rdR2;
+        const double d2tdR2 = z * r2inv * rinv;
+        const double d2tdRdz = dtdR * dtdR - drdR * drdR * r * rpRinv;
+        const double d2tdz2 = -d2tdR2 - dtdR * rpRinv;
+        h->dR2 = (hs.dr2 * drdR + hs.drdt * dtdR) * drdR + (hs.drdt * drdR + hs.dt2 * dtdR) * dtdR +
+                 gs.dr * d2rdR2 + gs.dt * d2tdR2;
+        h->dRdz = (hs.dr2 * drdz + hs.drdt * dtdz) * drdR + (hs.drdt * drdz + hs.dt2 * dtdz) * dtdR +
+                  gs.dr * d2rdRdz + gs.dt * d2tdRdz;
+        h->dz2 = (hs.dr2 * drdz + hs.drdt * dtdz) * drdz + (hs.drdt * drdz + hs.dt2 * dtdz) * dtdz +
+                 gs.dr * d2rdz2 + gs.dt * d2tdz2;
+        h->dRdphi = hs.drdphi * drdR + hs.dtdphi * dtdR;
+        h->dzdphi = hs.drdphi * drdz + hs.dtdphi * dtdz;
+        h->dphi2 = hs.dphi2;
+    }
+}
+
+/// which spline evaluators a kernel instantiation includes
+enum EvalKind {
+    EVAL_GENERAL = 0,   ///< any Multipole (runtime dispatch, local-memory harmonic arrays)
+    EVAL_AXI = 1,       ///< axisymmetric: a single (m = 0) harmonic in registers
+    EVAL_FAST = 2       ///< up to FAST_MAX_HARMONICS harmonics in registers
+};
+
 /** Multipole::evalCyl: pick the inner asymptote, the spline interpolator or the outer
     asymptote by radius (reference src/potential_multipole.cpp:1538-1548).
-    NQ = 1 (value), 3 (+ gradient) or 6 (+ Hessian). */
-template<int NQ>
+    NQ = 1 (value), 3 (+ gradient) or 6 (+ Hessian); KIND selects the spline evaluator
+    (the host picks the instantiation that matches the potential). */
+template<int NQ, int KIND = EVAL_GENERAL>
 __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
@@ -397,16 +530,37 @@ __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double 
         evalPowerLaw<NQ>(M.inner, R, z, phi, pot, g, h);
     else if(rsq > M.rOuterSq)
         evalPowerLaw<NQ>(M.outer, R, z, phi, pot, g, h);
-    else if(M.is2d)
-        evalInterp2d<NQ>(M, R, z, phi, pot, g, h);
-    else
+    else if(M.is2d) {
+        if(KIND == EVAL_AXI)
+            evalInterp2dFast<NQ, 1>(M, R, z, phi, pot, g, h);
+        else if(KIND == EVAL_FAST)
+            evalInterp2dFast<NQ, FAST_MAX_HARMONICS>(M, R, z, phi, pot, g, h);
+        else
+            evalInterp2d<NQ>(M, R, z, phi, pot, g, h);
+    } else
         evalInterp1d<NQ>(M, R, z, phi, pot, g, h);
+}
+
+/// out-of-line copy of evalMultipoleCyl: callers with many call sites (root finders, stage
+/// loops) share one body instead of inlining it at every site
+template<int NQ, int KIND>
+__device__ __noinline__ void evalMultipoleCylCall(const MultipoleView& M, double R, double z, double phi,
+    double* pot, CylDerivs* g, CylHess* h)
+{
+    evalMultipoleCyl<NQ, KIND>(M, R, z, phi, pot, g, h);
+}
+
+/// the evaluator kind matching a potential (host side)
+inline int evalKindOf(const MultipoleView& M)
+{
+    if(!M.is2d || M.nFast == 0) return EVAL_GENERAL;
+    return M.nFast == 1 ? EVAL_AXI : EVAL_FAST;
 }
 
 /** Evaluation at a Cartesian point with gradient (and Hessian xx,yy,zz,xy,yz,zx) in Cartesian
     coordinates: Car -> Cyl -> evaluate -> back (reference coord::evalAndConvert,
     src/coord.h:831-856, with the Car<->Cyl derivatives of src/coord.cpp:94-123, 608-719). */
-template<int NQ>
+template<int NQ, int KIND = EVAL_GENERAL>
 __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double x, double y, double z,
     double* pot, double* grad, double* hess)
 {
@@ -422,7 +576,7 @@ __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double 
         phi = atan2(y, x);
     }
     CylDerivs g; CylHess h;
-    evalMultipoleCyl<NQ>(M, R, z, phi, pot, &g, &h);
+    evalMultipoleCyl<NQ, KIND>(M, R, z, phi, pot, &g, &h);
     if(NQ >= 3) {
         grad[0] = g.dR * dRdx + g.dphi * dphidx;
         grad[1] = g.dR * dRdy + g.dphi * dphidy;

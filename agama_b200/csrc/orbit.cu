@@ -25,6 +25,7 @@ struct StageStore {
 };
 
 /// integrate one orbit; writes the final point (rotating frame), counters and status
+template<int KIND>
 __device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, const double* ic,
     double tEnd, const StageStore& S, double* out, long* nAccepted, long* nRejected, int* status)
 {
@@ -37,7 +38,7 @@ __device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, con
     int st = ORBIT_OK;
     // --- init: derivatives at the start and the initial step (OdeStepperDOP853::init)
     double accFac = 1;
-    orbitRHS<3>(M, Om, t, x, k1, &accFac);
+    orbitRHS<3, KIND>(M, Om, t, x, k1, &accFac);
     double hNext;
     {
         // initTimeStep (src/math_ode.cpp:35-91): Euler + Heun probes, Aarseth-like estimate
@@ -46,9 +47,9 @@ __device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, con
         const double h1 = fmax(HMIN, fmin(HMAX, sqrt(nx / nd) * 0.01));
         double k2[6], k3[6];
         for(int c = 0; c < 6; c++) xt[c] = x[c] + h1 * k1[c];
-        orbitRHS<3>(M, Om, t + h1, xt, k2, nullptr);
+        orbitRHS<3, KIND>(M, Om, t + h1, xt, k2, nullptr);
         for(int c = 0; c < 6; c++) xt[c] = x[c] + 0.5 * h1 * (k1[c] + k2[c]);
-        orbitRHS<3>(M, Om, t + h1, xt, k3, nullptr);
+        orbitRHS<3, KIND>(M, Om, t + h1, xt, k3, nullptr);
         double h2 = INFINITY;
         for(int c = 0; c < 6; c++) {
             const double d0 = fmax(P.accAbs, fmax(fabs(x[c]), fabs(xt[c])));
@@ -72,40 +73,40 @@ __device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, con
                 if(h == 0 || !isFinite(h) || ++attempts > MAX_ATTEMPTS_PER_STEP) { st = ORBIT_BAD_STEP; break; }
                 // ---- the twelve stages (xt = x + h * sum a_ij k_j), then k13 at the end point
                 for(int c = 0; c < 6; c++) xt[c] = x[c] + h * a21 * k1[c];
-                { double k[6]; orbitRHS<3>(M, Om, t + c2 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(0, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c2 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(0, c) = k[c]; }
                 for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a31 * k1[c] + a32 * S.at(0, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c3 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(1, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c3 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(1, c) = k[c]; }
                 for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a41 * k1[c] + a43 * S.at(1, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c4 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(2, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c4 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(2, c) = k[c]; }
                 for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a51 * k1[c] + a53 * S.at(1, c) + a54 * S.at(2, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c5 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(3, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c5 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(3, c) = k[c]; }
                 for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a61 * k1[c] + a64 * S.at(2, c) + a65 * S.at(3, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c6 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(4, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c6 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(4, c) = k[c]; }
                 for(int c = 0; c < 6; c++)
                     xt[c] = x[c] + h * (a71 * k1[c] + a74 * S.at(2, c) + a75 * S.at(3, c) + a76 * S.at(4, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c7 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(5, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c7 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(5, c) = k[c]; }
                 for(int c = 0; c < 6; c++)
                     xt[c] = x[c] + h * (a81 * k1[c] + a84 * S.at(2, c) + a85 * S.at(3, c) + a86 * S.at(4, c) +
                         a87 * S.at(5, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c8 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(6, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c8 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(6, c) = k[c]; }
                 for(int c = 0; c < 6; c++)
                     xt[c] = x[c] + h * (a91 * k1[c] + a94 * S.at(2, c) + a95 * S.at(3, c) + a96 * S.at(4, c) +
                         a97 * S.at(5, c) + a98 * S.at(6, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c9 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(7, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c9 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(7, c) = k[c]; }
                 for(int c = 0; c < 6; c++)
                     xt[c] = x[c] + h * (a101 * k1[c] + a104 * S.at(2, c) + a105 * S.at(3, c) + a106 * S.at(4, c) +
                         a107 * S.at(5, c) + a108 * S.at(6, c) + a109 * S.at(7, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c10 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(8, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c10 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(8, c) = k[c]; }
                 // stage 11 -> slot of k2, stage 12 -> slot of k3
                 for(int c = 0; c < 6; c++)
                     xt[c] = x[c] + h * (a111 * k1[c] + a114 * S.at(2, c) + a115 * S.at(3, c) + a116 * S.at(4, c) +
                         a117 * S.at(5, c) + a118 * S.at(6, c) + a119 * S.at(7, c) + a1110 * S.at(8, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + c11 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(0, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c11 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(0, c) = k[c]; }
                 for(int c = 0; c < 6; c++)
                     xt[c] = x[c] + h * (a121 * k1[c] + a124 * S.at(2, c) + a125 * S.at(3, c) + a126 * S.at(4, c) +
                         a127 * S.at(5, c) + a128 * S.at(6, c) + a129 * S.at(7, c) + a1210 * S.at(8, c) +
                         a1211 * S.at(0, c));
-                { double k[6]; orbitRHS<3>(M, Om, t + h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(1, c) = k[c]; }
+                { double k[6]; orbitRHS<3, KIND>(M, Om, t + h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(1, c) = k[c]; }
                 double k1b[6];
                 for(int c = 0; c < 6; c++) {
                     k1b[c] = b1 * k1[c] + b6 * S.at(4, c) + b7 * S.at(5, c) + b8 * S.at(6, c) + b9 * S.at(7, c) +
@@ -113,7 +114,7 @@ __device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, con
                     xt[c] = x[c] + h * k1b[c];
                 }
                 double af = 1;
-                orbitRHS<3>(M, Om, t + h, xt, k13, &af);
+                orbitRHS<3, KIND>(M, Om, t + h, xt, k13, &af);
                 // ---- error estimate (3rd and 5th order embedded solutions)
                 double err5 = 0, err3 = 0;
                 for(int c = 0; c < 6; c++) {
@@ -167,7 +168,8 @@ __device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, con
 }
 
 /// one orbit per thread (queue == nullptr) or a persistent grid draining a work queue
-__global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const MultipoleView M, const OrbitParams P,
+template<int KIND>
+__global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constant__ MultipoleView M, const OrbitParams P,
     long n, const double* __restrict__ ic, const double* __restrict__ T, double* __restrict__ out,
     long* __restrict__ nsteps, long* __restrict__ nrej, int* __restrict__ status,
     unsigned long long* queue)
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const MultipoleView 
         double o[6];
         long na, nr;
         int s;
-        integrateOrbit(M, P, ic + 6 * i, T[i], S, o, &na, &nr, &s);
+        integrateOrbit<KIND>(M, P, ic + 6 * i, T[i], S, o, &na, &nr, &s);
         for(int c = 0; c < 6; c++) out[6 * i + c] = o[c];
         if(nsteps) nsteps[i] = na;
         if(nrej) nrej[i] = nr;
@@ -199,12 +201,15 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
     if(n <= 0) return;
     const int block = ORBIT_BLOCK;
     const size_t shmem = orbitSharedBytes(block);
+    const int kind = evalKindOf(M);
+    auto kernel = kind == EVAL_AXI ? dop853Kernel<EVAL_AXI> : kind == EVAL_FAST ? dop853Kernel<EVAL_FAST>
+                                                                              : dop853Kernel<EVAL_GENERAL>;
     long grid;
     if(queue) {
         int dev, sms, perSM = 0;
         AGB_CUDA(cudaGetDevice(&dev));
         AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, dop853Kernel, block, shmem));
+        AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, block, shmem));
         grid = static_cast<long>(sms) * (perSM > 0 ? perSM : 1);
         const long needed = (n + block - 1) / block;
         if(grid > needed) grid = needed;
@@ -212,7 +217,7 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
     } else {
         grid = (n + block - 1) / block;
     }
-    dop853Kernel<<<grid, block, shmem, stream>>>(M, P, n, ic, T, out, nsteps, nrej, status, queue);
+    kernel<<<grid, block, shmem, stream>>>(M, P, n, ic, T, out, nsteps, nrej, status, queue);
     AGB_CUDA(cudaGetLastError());
 }
 

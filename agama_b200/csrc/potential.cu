@@ -7,8 +7,9 @@ namespace agb {
 namespace {
 thread_local std::string g_error;
 
-/// One point per thread; 256 threads per block.  NQ = 1 (potential), 3 (+gradient), 6 (+Hessian).
-template<int NQ>
+/// One point per thread; 256 threads per block.  NQ = 1 (potential), 3 (+gradient), 6 (+Hessian);
+/// KIND = spline evaluator matching the potential (EvalKind).
+template<int NQ, int KIND>
 __global__ void __launch_bounds__(256) evalPotentialKernel(const MultipoleView M, long n,
     const double* __restrict__ pos, double* __restrict__ phi, double* __restrict__ grad,
     double* __restrict__ hess)
@@ -17,7 +18,7 @@ __global__ void __launch_bounds__(256) evalPotentialKernel(const MultipoleView M
     if(i >= n) return;
     const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
     double p, g[3], h[6];
-    evalMultipoleCar<NQ>(M, x, y, z, &p, g, h);
+    evalMultipoleCar<NQ, KIND>(M, x, y, z, &p, g, h);
     if(phi) phi[i] = p;
     if(NQ >= 3 && grad) { grad[3 * i] = g[0]; grad[3 * i + 1] = g[1]; grad[3 * i + 2] = g[2]; }
     if(NQ == 6 && hess)
@@ -42,12 +43,12 @@ void launchEvalPotential(const MultipoleView& M, long n, const double* pos, doub
     if(n <= 0) return;
     const int block = 256;
     const long grid = (n + block - 1) / block;
-    if(hess)
-        evalPotentialKernel<6><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess);
-    else if(grad)
-        evalPotentialKernel<3><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess);
-    else
-        evalPotentialKernel<1><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess);
+    const int nq = hess ? 6 : grad ? 3 : 1, kind = evalKindOf(M);
+#define AGB_LAUNCH(NQ_, K_) evalPotentialKernel<NQ_, K_><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess)
+    if(kind == EVAL_AXI)       { if(nq == 6) AGB_LAUNCH(6, EVAL_AXI);     else if(nq == 3) AGB_LAUNCH(3, EVAL_AXI);     else AGB_LAUNCH(1, EVAL_AXI); }
+    else if(kind == EVAL_FAST) { if(nq == 6) AGB_LAUNCH(6, EVAL_FAST);    else if(nq == 3) AGB_LAUNCH(3, EVAL_FAST);    else AGB_LAUNCH(1, EVAL_FAST); }
+    else                       { if(nq == 6) AGB_LAUNCH(6, EVAL_GENERAL); else if(nq == 3) AGB_LAUNCH(3, EVAL_GENERAL); else AGB_LAUNCH(1, EVAL_GENERAL); }
+#undef AGB_LAUNCH
     AGB_CUDA(cudaGetLastError());
 }
 
@@ -87,6 +88,18 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
         V.outer.ind = H.outer.ind; V.outer.r0sq = H.outer.r0sq; V.outer.inner = 0; V.outer.Q = H.outer.Q;
         V.outer.S = P->outerS.ptr; V.outer.U = P->outerU.ptr; V.outer.W = P->outerW.ptr;
         P->axisymmetric = (H.ind.sym & SYM_AXISYMMETRIC) == SYM_AXISYMMETRIC;
+        // register-resident evaluator: m = 0 first, then ascending m
+        V.nFast = 0;
+        if(H.is2d && H.splSlot[H.ind.mmax] >= 0) {
+            std::vector<int> ms(1, 0);
+            for(int m = -H.ind.mmax; m <= H.ind.mmax; m++)
+                if(m != 0 && H.splSlot[m + H.ind.mmax] >= 0) ms.push_back(m);
+            if(static_cast<int>(ms.size()) <= FAST_MAX_HARMONICS) {
+                V.nFast = static_cast<int>(ms.size());
+                for(int s = 0; s < V.nFast; s++) { V.fastM[s] = ms[s]; V.fastSlot[s] = H.splSlot[ms[s] + H.ind.mmax]; }
+            }
+        }
+        for(int s = V.nFast; s < FAST_MAX_HARMONICS; s++) { V.fastM[s] = 0; V.fastSlot[s] = 0; }
     } catch(...) {
         delete P;
         throw;
