@@ -274,8 +274,9 @@ def run_engine(args):
 
 # executed FP64 flops per action (dadd + dmul + 2 dfma, ncu, config-2 workload) and DRAM bytes per
 # launch of the fudge kernel for 1e6 particles; see profiles/fudge_actions_cfg2.md
-FLOPS_PER_ACTION_CFG2 = 20000.0
-TRAFFIC_PER_LAUNCH_CFG2 = None
+FLOPS_PER_ACTION_CFG2 = 26206.0
+# dram read + write of one 200 000-particle launch (9.89 MB + 0.22 MB), scaled to 1e6 particles
+TRAFFIC_PER_LAUNCH_CFG2 = 5 * (9.888256e6 + 0.220416e6)
 
 
 def ctypes_stream(stream):
