@@ -31,6 +31,9 @@ SIGNATURES = {
     "agama_integrateOrbitsManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
                                                        ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
                                                        ctypes.c_int, VP]),
+    "agama_integrateOrbitsManyDeviceNoAlloc": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
+                                                              ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
+                                                              ctypes.c_int, VP]),
     "agama_measureFP64Throughput": (ctypes.c_int, [D]),
     "agama_deleteActionFinder": (None, [VP]),
     "agama_evalActionsAnglesFrequencies": (None, [VP, D, D, D, D]),

@@ -223,6 +223,26 @@ extern "C" int agama_integrateOrbitsMany(const agama_Potential* p, long n, const
     });
 }
 
+extern "C" int agama_integrateOrbitsManyDeviceNoAlloc(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
+    long* numSteps, long* numRejected, int* status, int queueSlot, void* stream)
+{
+    // no cudaMalloc / cudaFree / allocating library call on this path: the work-queue counter is
+    // a slot of the library's static device array (launchOrbitsNoAlloc, orbit.cu)
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && (!ic || !T || !finalState)))
+            throw std::invalid_argument("integrateOrbitsManyDeviceNoAlloc: invalid arguments");
+        if(queueSlot < 0 || queueSlot >= noallocQueueSlots())
+            throw std::invalid_argument("integrateOrbitsManyDeviceNoAlloc: queueSlot " + std::to_string(queueSlot) +
+                " out of range 0.." + std::to_string(noallocQueueSlots() - 1));
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const OrbitParams P = makeOrbitParams(Omega, accuracy, maxNumSteps);
+        launchOrbitsNoAlloc(p->pot->view, P, n, ic, T, finalState, numSteps, numRejected, status, queueSlot,
+            static_cast<cudaStream_t>(stream));
+    });
+}
+
 // ------------------------------------------------------------------------------------------
 // actions (Staeckel fudge)
 

@@ -8,6 +8,8 @@
 // atomic counter) by a grid sized to the GPU, which balances orbits of very different length.
 #include "runtime.h"
 #include "dop853.cuh"
+#include <map>
+#include <mutex>
 
 namespace agb {
 
@@ -219,6 +221,55 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
     }
     kernel<<<grid, block, shmem, stream>>>(M, P, n, ic, T, out, nsteps, nrej, status, queue);
     AGB_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------------
+// Work-queue orbit integration without any allocation by the library.
+//
+// Some callers cannot have a library allocate device memory: applications whose own memory
+// manager has reserved (nearly) all of the GPU's memory up front, so a cudaMalloc fails or
+// fragments their pool; latency-critical loops in which cudaMalloc / cudaFree would synchronise
+// the device and stall the caller's other streams; and plugin hosts that account for all device
+// memory and forbid libraries from allocating behind their back.  For them the work-queue
+// counters live in a fixed static array in device memory, loaded with the library (every GPU
+// that loads it holds these 256 bytes until the process exits).
+
+/// number of independent work-queue counters (one per batch that may run at the same time)
+constexpr int NOALLOC_QUEUE_SLOTS = 32;
+
+/// the counters; each call clears its own slot on its stream before the launch
+static __device__ __align__(256) unsigned long long g_noallocQueue[NOALLOC_QUEUE_SLOTS];
+
+namespace {
+std::mutex g_noallocMutex;
+std::map<int, unsigned long long*> g_noallocAddress;   // device address of the array, per device
+}
+
+int noallocQueueSlots() { return NOALLOC_QUEUE_SLOTS; }
+
+void launchOrbitsNoAlloc(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    double* out, long* nsteps, long* nrej, int* status, int slot, cudaStream_t stream)
+{
+    if(slot < 0 || slot >= NOALLOC_QUEUE_SLOTS)
+        throw std::invalid_argument("integrateOrbitsManyDeviceNoAlloc: queueSlot must be in 0.." +
+            std::to_string(NOALLOC_QUEUE_SLOTS - 1) + " (the static work-queue array has " +
+            std::to_string(NOALLOC_QUEUE_SLOTS) + " counters)");
+    int dev;
+    AGB_CUDA(cudaGetDevice(&dev));
+    unsigned long long* base = nullptr;
+    {
+        // one-time set-up per device, with that device current: the host-side name of a
+        // __device__ array is not a device address, so look the address up once and cache it
+        std::lock_guard<std::mutex> lock(g_noallocMutex);
+        auto it = g_noallocAddress.find(dev);
+        if(it == g_noallocAddress.end()) {
+            AGB_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&base), g_noallocQueue));
+            g_noallocAddress[dev] = base;
+        } else
+            base = it->second;
+    }
+    // launchOrbits clears the counter (cudaMemsetAsync on the stream) before the kernel runs
+    launchOrbits(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, stream);
 }
 
 }  // namespace agb

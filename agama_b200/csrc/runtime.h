@@ -74,6 +74,11 @@ void launchEvalPotential(const MultipoleView& M, long n, const double* pos, doub
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream);
 
+/// the same work-queue batch with its counter in the library's static device array (slot 0..31),
+/// allocating nothing
+void launchOrbitsNoAlloc(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    double* out, long* nsteps, long* nrej, int* status, int slot, cudaStream_t stream);
+int noallocQueueSlots();
 /// Staeckel fudge with a given focal distance per point (fd) or one for all (fd0 when fd is null)
 void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
     double* act, int* iters, cudaStream_t stream);

@@ -91,6 +91,23 @@ int agama_integrateOrbitsManyDevice(const agama_Potential* potential, long n, co
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, long* numRejected, int* status, int useQueue, void* stream);
 
+/* The same work-queue batch (as agama_integrateOrbitsManyDevice with useQueue != 0), but the
+   library allocates nothing: no cudaMalloc, cudaFree or allocating library routine runs.  It is
+   for callers that cannot let a library allocate device memory -- applications whose memory
+   manager has reserved (nearly) all of the GPU's memory up front, latency-critical loops in which
+   an allocation would synchronise the device and stall other streams, and plugin hosts that
+   account for every byte of device memory.  This entry point has no counterpart in the reference.
+   The queue counter lives in a static array of 32 counters (256 bytes) in device memory, held by
+   every GPU that loads the library until the process exits; queueSlot (0..31) selects one, and a
+   value outside that range is rejected with an error.  Each call clears its counter on `stream`
+   before the launch; the array keeps the last call's values.  Calls that overlap on the GPU and
+   use the same slot race (orbits may be skipped or integrated twice): give batches that may run
+   at the same time different slots.  The first call on each device looks up the array's device
+   address (cudaGetSymbolAddress) -- make that first call before any stream capture. */
+int agama_integrateOrbitsManyDeviceNoAlloc(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
+    long* numSteps, long* numRejected, int* status, int queueSlot, void* stream);
+
 /* ---------------------------------------------------------------------------------------
    Staeckel-fudge actions (axisymmetric potentials only).  posvel: n x 6 Cartesian points;
    act: n x 3 (Jr, Jz, Jphi); unbound points (E >= 0) give Jr = Jz = NaN, as in the reference
