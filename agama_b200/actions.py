@@ -26,9 +26,14 @@ class ActionFinder:
     """
 
     def __init__(self, potential, tables=None):
-        if tables is None:
-            raise NotImplementedError("ActionFinder: building the focal-distance table needs tables=...")
         self.potential = potential
+        if tables is None:
+            # build the focal-distance table (shell orbits on the device) and L_circ(E)
+            h = _native.lib().agama_createActionFinder(potential.handle)
+            if not h:
+                raise RuntimeError("agama_b200: " + _native.error())
+            self._h = ctypes.c_void_p(h)
+            return
         t = {k: np.ascontiguousarray(v, dtype=np.float64) if isinstance(v, np.ndarray) else v
              for k, v in tables.items()}
         gE, gL, dl = t["gridE"], t["gridL"], np.ascontiguousarray(t["delta"], dtype=np.float64)
@@ -50,6 +55,19 @@ class ActionFinder:
     @property
     def handle(self):
         return self._h
+
+    def tables(self):
+        """the finder's tables, in the layout accepted by ActionFinder(potential, tables=...)"""
+        L = _native.lib()
+        sz = [ctypes.c_int() for _ in range(5)]
+        check(L.agama_getActionFinderTableSizes(self._h, *[ctypes.byref(x) for x in sz]))
+        nE, nL, n1, n2, n3 = (x.value for x in sz)
+        gE, gL, dl = np.empty(nE), np.empty(nL), np.empty((nE, nL))
+        lofe, rofl, phr, scal = np.empty((4, n1)), np.empty((4, n2)), np.empty((4, n3)), np.empty(5)
+        check(L.agama_getActionFinderTables(self._h, ptr(gE), ptr(gL), ptr(dl), ptr(lofe), ptr(rofl), ptr(phr),
+                                            ptr(scal)))
+        return dict(gridE=gE, gridL=gL, delta=dl, lofe=lofe, rofl=rofl, phiofr=phr, invPhi0=scal[0],
+                    interp_invPhi0=scal[1], slopeOut=scal[2], coefOut=scal[3], massOut=scal[4])
 
     def __call__(self, points, fd=False):
         """actions (n x 3); with fd=True also the focal distance used for each point"""

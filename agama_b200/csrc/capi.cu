@@ -281,6 +281,48 @@ extern "C" agama_ActionFinder* agama_createActionFinderFromTables(const agama_Po
     }
 }
 
+extern "C" agama_ActionFinder* agama_createActionFinder(const agama_Potential* p)
+{
+    try {
+        requireAxisymmetric(p);
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        return new agama_ActionFinder{ createDeviceActionFinder(p->pot, buildFinderTables(*p->pot)) };
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+extern "C" int agama_getActionFinderTableSizes(const agama_ActionFinder* a, int* nE, int* nL, int* nLofE,
+    int* nRofL, int* nPhiofR)
+{
+    return guarded([&] {
+        if(!a) throw std::invalid_argument("null action finder");
+        const FinderTablesHost& T = a->af->host;
+        if(nE) *nE = T.nE;
+        if(nL) *nL = T.nL;
+        if(nLofE) *nLofE = static_cast<int>(T.lofe.size() / 4);
+        if(nRofL) *nRofL = static_cast<int>(T.rofl.size() / 4);
+        if(nPhiofR) *nPhiofR = static_cast<int>(T.phiofr.size() / 4);
+    });
+}
+
+extern "C" int agama_getActionFinderTables(const agama_ActionFinder* a, double* gridE, double* gridL,
+    double* delta, double* LofE, double* RofL, double* PhiofR, double* scalars)
+{
+    return guarded([&] {
+        if(!a) throw std::invalid_argument("null action finder");
+        const FinderTablesHost& T = a->af->host;
+        auto put = [](const std::vector<double>& v, double* out) { if(out) std::copy(v.begin(), v.end(), out); };
+        put(T.gridE, gridE); put(T.gridL, gridL); put(T.delta, delta);
+        put(T.lofe, LofE); put(T.rofl, RofL); put(T.phiofr, PhiofR);
+        if(scalars) {
+            scalars[0] = T.invPhi0; scalars[1] = T.interpInvPhi0; scalars[2] = T.slopeOut;
+            scalars[3] = T.coefOut; scalars[4] = T.massOut;
+        }
+    });
+}
+
 extern "C" void agama_deleteActionFinder(agama_ActionFinder* a)
 {
     if(!a) return;

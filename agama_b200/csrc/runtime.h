@@ -66,6 +66,8 @@ struct DeviceActionFinder {
     FudgeTables view;
 };
 DeviceActionFinder* createDeviceActionFinder(DevicePotential* pot, const FinderTablesHost& T);
+/// build the focal-distance table and the L_circ interpolator of a potential (finder_build.cu)
+FinderTablesHost buildFinderTables(const DevicePotential& P);
 
 /// launch helpers (defined in the .cu files)
 void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,

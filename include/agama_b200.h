@@ -113,6 +113,19 @@ int agama_integrateOrbitsManyDeviceNoAlloc(const agama_Potential* potential, lon
    act: n x 3 (Jr, Jz, Jphi); unbound points (E >= 0) give Jr = Jz = NaN, as in the reference
    (src/actions_staeckel.cpp:648-656). */
 
+/* reference: agama_createActionFinder, src/interface_c.h:113 (src/interface_c.cpp:113-123):
+   the Staeckel-fudge action finder of an axisymmetric potential, with its focal-distance table
+   built from shell orbits on the device (ActionFinderAxisymFudge constructor,
+   src/actions_staeckel.cpp:751-795) and its L_circ(E) interpolator (potential::Interpolator,
+   src/potential_utils.cpp:757-870).  NULL (with agama_getError) for non-axisymmetric potentials. */
+agama_ActionFinder* agama_createActionFinder(const agama_Potential* potential);
+
+/* sizes and contents of an action finder's tables (layout as agama_createActionFinderFromTables) */
+int agama_getActionFinderTableSizes(const agama_ActionFinder* actionFinder, int* nE, int* nL, int* nLofE,
+    int* nRofL, int* nPhiofR);
+int agama_getActionFinderTables(const agama_ActionFinder* actionFinder, double* gridE, double* gridL,
+    double* delta, double* LofE, double* RofL, double* PhiofR, double* scalars);
+
 /* reference: agama_deleteActionFinder, src/interface_c.h:118 */
 void agama_deleteActionFinder(agama_ActionFinder* actionFinder);
 

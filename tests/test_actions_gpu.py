@@ -58,6 +58,26 @@ def test_action_finder(cfg):
     check_actions(J, g["act_finder"])
 
 
+@pytest.mark.parametrize("cfg", CFGS)
+def test_action_finder_builds_own_tables(cfg):
+    """agama_createActionFinder: the engine builds the focal-distance table from shell orbits on
+    the device and the L_circ(E) interpolator itself; the grids must equal the reference's, the
+    focal distances agree to the shell-orbit root tolerance, and the actions to 1e-6."""
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "actions_%s.npz" % cfg))
+    ref_tab = tables(g)
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    af = agama_b200.ActionFinder(pot)
+    tab = af.tables()
+    assert tab["gridE"].shape == ref_tab["gridE"].shape and tab["lofe"].shape == ref_tab["lofe"].shape
+    assert np.allclose(tab["gridE"], ref_tab["gridE"], rtol=1e-12, atol=0)
+    assert np.allclose(tab["gridL"], ref_tab["gridL"], rtol=1e-15, atol=0)
+    assert np.allclose(tab["lofe"], ref_tab["lofe"], rtol=1e-10, atol=1e-14)
+    scale = np.max(ref_tab["delta"])
+    assert np.max(np.abs(tab["delta"] - ref_tab["delta"])) <= 1e-5 * scale
+    check_actions(af(g["points"]), g["act_finder"])
+
+
 def test_actions_device_pointers_and_single_point():
     import ctypes
     import torch
