@@ -108,11 +108,6 @@ def make_particles(n, seed, vcirc):
     return workloads.disk_particles(n, vcirc, seed=seed)
 
 
-def finder_tables():
-    g = np.load(os.path.join(GOLDEN, "actions_cfg2.npz"))
-    return {k[4:]: g[k] for k in g.files if k.startswith("tab_")}
-
-
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -182,7 +177,7 @@ def run_engine(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg2.coef"))
-    af = agama_b200.ActionFinder(pot, tables=finder_tables())
+    af = agama_b200.ActionFinder(pot)          # focal-distance table built on the device
     vc = lambda R: np.sqrt(-R * pot.force(np.column_stack([R, 0 * R, 0 * R]))[:, 0])
     n = args.particles
     pts = make_particles(n, 3 + rank, vc)
