@@ -74,21 +74,29 @@ def test_action_finder_builds_own_tables(cfg):
     report["gridE"] = np.max(np.abs(tab["gridE"] / ref_tab["gridE"] - 1))
     for k in ("lofe", "rofl", "phiofr"):
         report[k] = np.max(np.abs(tab[k][:3] - ref_tab[k][:3]) / np.maximum(np.abs(ref_tab[k][:3]), 1e-300))
-    # Delta per node, relative to the table's typical value.  Excluded: the two outermost energy
-    # rows (E -> 0, shell orbits at r ~ 1e10 and beyond, where both tables hold meaningless values
-    # up to 1e36).  The shell radius is a root located to 1e-6 of its bracket and near circular
-    # orbits the focal-distance formula divides two vanishing quantities, so single nodes move by
-    # up to ~1e-3.
-    dref, dnew = ref_tab["delta"][:-2], tab["delta"][:-2]
-    typical = np.median(dref[dref > 0])
-    report["delta"] = np.max(np.abs(dnew - dref) / np.maximum(dref, typical))
+    # Delta per node over the energy rows that the test points use (one row of margin each side),
+    # relative to the row's typical value.  Rows far outside (E -> 0: shell orbits at r ~ 1e10 and
+    # beyond) hold meaningless values up to 1e36 in both tables.  Within the rows used the nodes
+    # agree to ~5e-7 (the shell radius is a root located to 1e-6 of its bracket; near circular
+    # orbits the focal-distance formula divides two vanishing quantities).
+    pts = g["points"]
+    E = pot.potential(pts[:, :3]) + 0.5 * np.sum(pts[:, 3:] ** 2, axis=1)
+    xi = np.log(ref_tab["invPhi0"] - 1 / E[E < 0])
+    r0 = max(0, np.searchsorted(ref_tab["gridE"], np.min(xi)) - 2)
+    r1 = min(len(ref_tab["gridE"]), np.searchsorted(ref_tab["gridE"], np.max(xi)) + 1)
+    dref, dnew = ref_tab["delta"][r0:r1], tab["delta"][r0:r1]
+    typical = np.array([np.median(row[row > 0]) if np.any(row > 0) else 1.0 for row in dref])[:, None]
+    rel = np.abs(dnew - dref) / np.maximum(dref, typical)
+    report["rows"] = (r0, r1)
+    report["delta"] = np.max(rel)
+    report["delta_node"] = np.unravel_index(np.argmax(rel), rel.shape)
     print(cfg, report)
     check_actions(J, g["act_finder"])
     assert tab["gridE"].shape == ref_tab["gridE"].shape and tab["lofe"].shape == ref_tab["lofe"].shape
     # grids to round-off (the L_circ grid of config 2 ends in the NFW outer asymptote whose
     # condition number ~1e4 moves a few single-precision grid steps by one float ulp: 1e-8)
     assert report["gridE"] <= 1e-12 and report["lofe"] <= 1e-7
-    assert report["delta"] <= 1e-2
+    assert report["delta"] <= 1e-5
 
 
 def test_actions_device_pointers_and_single_point():
