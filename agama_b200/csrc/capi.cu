@@ -3,6 +3,7 @@
 // device-pointer variants.  No exception crosses this boundary: constructors return NULL and
 // batched calls return a non-zero status, with the message in agama_getError().
 #include "runtime.h"
+#include "host_pipeline.h"
 #include "../../include/agama_b200.h"
 #include <cstring>
 #include <sstream>
@@ -126,13 +127,13 @@ int agama_evalPotentialMany(const agama_Potential* p, long n, const double* pos,
         if(!p || n < 0 || (n > 0 && !pos)) throw std::invalid_argument("evalPotentialMany: invalid arguments");
         if(n == 0) return;
         AGB_CUDA(cudaSetDevice(p->pot->device));
-        DevBuf<double> dpos(3 * n), dphi(n), dg(deriv ? 3 * n : 0), dh(deriv2 ? 6 * n : 0);
-        AGB_CUDA(cudaMemcpy(dpos.ptr, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice));
-        launchEvalPotential(p->pot->view, n, dpos.ptr, dphi.ptr, dg.ptr, dh.ptr, 0);
-        if(phi) AGB_CUDA(cudaMemcpy(phi, dphi.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
-        if(deriv) AGB_CUDA(cudaMemcpy(deriv, dg.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
-        if(deriv2) AGB_CUDA(cudaMemcpy(deriv2, dh.ptr, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
-        AGB_CUDA(cudaDeviceSynchronize());
+        const MultipoleView& M = p->pot->view;
+        runChunked(n, { { pos, 3 * sizeof(double) } },
+            { { phi, sizeof(double) }, { deriv, 3 * sizeof(double) }, { deriv2, 6 * sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchEvalPotential(M, count, static_cast<const double*>(in[0]), static_cast<double*>(out[0]),
+                    static_cast<double*>(out[1]), static_cast<double*>(out[2]), s);
+            });
     });
 }
 
@@ -347,11 +348,12 @@ extern "C" int agama_evalActionsMany(const agama_ActionFinder* a, long n, const 
         if(!a || n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsMany: invalid arguments");
         if(n == 0) return;
         AGB_CUDA(cudaSetDevice(a->af->pot->device));
-        DevBuf<double> dpv(6 * n), dact(3 * n), dfd(fdOut ? n : 0);
-        AGB_CUDA(cudaMemcpy(dpv.ptr, posvel, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
-        launchActionsFinder(a->af->pot->view, a->af->view, n, dpv.ptr, dact.ptr, dfd.ptr, nullptr, 0);
-        AGB_CUDA(cudaMemcpy(act, dact.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
-        if(fdOut) AGB_CUDA(cudaMemcpy(fdOut, dfd.ptr, n * sizeof(double), cudaMemcpyDeviceToHost));
+        const DeviceActionFinder& F = *a->af;
+        runChunked(n, { { posvel, 6 * sizeof(double) } }, { { act, 3 * sizeof(double) }, { fdOut, sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchActionsFinder(F.pot->view, F.view, count, static_cast<const double*>(in[0]),
+                    static_cast<double*>(out[0]), static_cast<double*>(out[1]), nullptr, s);
+            });
     });
 }
 
@@ -374,11 +376,12 @@ extern "C" int agama_evalActionsStandaloneMany(const agama_Potential* p, long n,
         if(n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsStandaloneMany: invalid arguments");
         if(n == 0) return;
         AGB_CUDA(cudaSetDevice(p->pot->device));
-        DevBuf<double> dpv(6 * n), dact(3 * n), dfd(fd ? n : 0);
-        AGB_CUDA(cudaMemcpy(dpv.ptr, posvel, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
-        if(fd) AGB_CUDA(cudaMemcpy(dfd.ptr, fd, n * sizeof(double), cudaMemcpyHostToDevice));
-        launchActionsFixedDelta(p->pot->view, n, dpv.ptr, dfd.ptr, fd0, dact.ptr, nullptr, 0);
-        AGB_CUDA(cudaMemcpy(act, dact.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        const MultipoleView& M = p->pot->view;
+        runChunked(n, { { posvel, 6 * sizeof(double) }, { fd, sizeof(double) } }, { { act, 3 * sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchActionsFixedDelta(M, count, static_cast<const double*>(in[0]), static_cast<const double*>(in[1]),
+                    fd0, static_cast<double*>(out[0]), nullptr, s);
+            });
     });
 }
 
