@@ -1,14 +1,15 @@
 // Staeckel-fudge action kernels, the device-resident action finder and their host launchers.
 #include "runtime.h"
 #include "fudge.cuh"
+#include "host_pipeline.h"
+#include "fudge_phases.h"
+#include <algorithm>
 #include <mutex>
 #include <map>
 
 namespace agb {
 
 namespace {
-
-constexpr int FUDGE_BLOCK = 128;
 
 /// Gauss-Legendre rules on [0,1] for the orders 1..20, 25, 32, 40 (the set the reference
 /// tabulates, src/math_glquadrature.h), computed by Newton iteration in extended precision
@@ -68,12 +69,19 @@ const GLRules& glRulesForCurrentDevice()
     return d->view;
 }
 
-/// One point per thread.  FINDER: Delta from the finder's table; otherwise from fd[i] (or fd0 if
-/// fd is null).  Outputs actions (Jr, Jz, Jphi), optionally Delta and root-finder iterations.
+constexpr int PREPARE_BLOCK = 128;
+constexpr long POINTS_PER_PASS = 1L << 20;     // records of one pass: 128 MB of scratch
+
+/// Phase 1, one point per thread: cylindrical coordinates, potential, focal distance (FINDER:
+/// from the finder's table; otherwise fd[i], or fd0 if fd is null), integrals of motion, the
+/// limits that need no root search and the brackets of those that do -> one record per point.
+/// Jphi (and NaN Jr, Jz of points without actions) are written directly.  Optional outputs:
+/// Delta used, root-finder iterations (zeroed here, counted by phase 2).
 template<bool FINDER>
-__global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const __grid_constant__ MultipoleView M, const GLRules gl,
-    const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd, double fd0,
-    double* __restrict__ act, double* __restrict__ fdOut, int* __restrict__ iters)
+__global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __grid_constant__ MultipoleView M,
+    const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd,
+    double fd0, FudgeRecord* __restrict__ rec, double* __restrict__ act, double* __restrict__ fdOut,
+    int* __restrict__ iters)
 {
     const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
     if(i >= n) return;
@@ -84,12 +92,36 @@ __global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const __grid_constant
     CylDerivs g; CylHess h;
     evalMultipoleCylCall<1, EVAL_AXI>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
     const double delta = FINDER ? finderFocalDistance(F, pc, Phi) : (fd ? fd[i] : fd0);
+    FudgeRecord r;
     double a[3];
-    int it = 0;
-    fudgeActions(M, gl, pc, Phi, delta, a, &it);
-    act[3 * i] = a[0]; act[3 * i + 1] = a[1]; act[3 * i + 2] = a[2];
+    fudgePrepare(M, pc, Phi, delta, r, a);
+    rec[i] = r;
+    act[3 * i + 2] = a[2];
+    if(!r.valid) { act[3 * i] = a[0]; act[3 * i + 1] = a[1]; }
     if(fdOut) fdOut[i] = delta;
-    if(iters) iters[i] = it;
+    if(iters) iters[i] = 0;
+}
+
+/// the three phases over passes of at most POINTS_PER_PASS points (bounded scratch)
+template<bool FINDER>
+void runActions(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel, const double* fd,
+    double fd0, double* act, double* fdOut, int* iters, cudaStream_t stream)
+{
+    if(n <= 0) return;
+    const GLRules& gl = glRulesForCurrentDevice();
+    const long pass = std::min(n, POINTS_PER_PASS);
+    Scratch recs(pass * sizeof(FudgeRecord), stream);
+    FudgeRecord* rec = static_cast<FudgeRecord*>(recs.ptr);
+    for(long first = 0; first < n; first += pass) {
+        const long count = std::min(pass, n - first);
+        int* it = iters ? iters + first : nullptr;
+        fudgePrepareKernel<FINDER><<<(count + PREPARE_BLOCK - 1) / PREPARE_BLOCK, PREPARE_BLOCK, 0, stream>>>(
+            M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, act + 3 * first,
+            fdOut ? fdOut + first : nullptr, it);
+        AGB_CUDA(cudaGetLastError());
+        launchFudgeRoots(M, count, rec, it, stream);
+        launchFudgeIntegrals(M, gl, count, rec, act + 3 * first, stream);
+    }
 }
 
 }  // namespace
@@ -97,22 +129,14 @@ __global__ void __launch_bounds__(FUDGE_BLOCK) fudgeKernel(const __grid_constant
 void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
     double* act, int* iters, cudaStream_t stream)
 {
-    if(n <= 0) return;
-    const GLRules& gl = glRulesForCurrentDevice();
     FudgeTables dummy{};
-    fudgeKernel<false><<<(n + FUDGE_BLOCK - 1) / FUDGE_BLOCK, FUDGE_BLOCK, 0, stream>>>(
-        M, gl, dummy, n, posvel, fd, fd0, act, nullptr, iters);
-    AGB_CUDA(cudaGetLastError());
+    runActions<false>(M, dummy, n, posvel, fd, fd0, act, nullptr, iters, stream);
 }
 
 void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
     double* act, double* fdOut, int* iters, cudaStream_t stream)
 {
-    if(n <= 0) return;
-    const GLRules& gl = glRulesForCurrentDevice();
-    fudgeKernel<true><<<(n + FUDGE_BLOCK - 1) / FUDGE_BLOCK, FUDGE_BLOCK, 0, stream>>>(
-        M, gl, F, n, posvel, nullptr, 0, act, fdOut, iters);
-    AGB_CUDA(cudaGetLastError());
+    runActions<true>(M, F, n, posvel, nullptr, 0, act, fdOut, iters, stream);
 }
 
 // ------------------------------------------------------------------------------------------

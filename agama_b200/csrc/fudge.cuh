@@ -40,7 +40,7 @@ __device__ __forceinline__ void spline1d(const Spline1dView& S, double x, double
 }
 
 /// potential::Interpolator::evalDeriv (src/potential_utils.cpp:872-911): Phi(R), dPhi/dR, d2Phi/dR2
-__device__ void interpPhi(const FudgeTables& F, double R, double* val, double* der, double* der2)
+static __device__ void interpPhi(const FudgeTables& F, double R, double* val, double* der, double* der2)
 {
     const double logR = log(R);
     if(logR > ldg(F.PhiofR.t + F.PhiofR.n - 1) && F.coefOut != 0) {
@@ -60,7 +60,7 @@ __device__ void interpPhi(const FudgeTables& F, double R, double* val, double* d
 }
 
 /// potential::Interpolator::L_circ (src/potential_utils.cpp:954-980)
-__device__ double interpLcirc(const FudgeTables& F, double E)
+static __device__ double interpLcirc(const FudgeTables& F, double E)
 {
     if(!(E >= 1. / F.iInvPhi0 && E <= 0))
         return NAN;
@@ -82,7 +82,7 @@ __device__ double interpLcirc(const FudgeTables& F, double E)
 }
 
 /// bilinear Delta(xi, chi) (LinearInterpolator2d::evalDeriv, src/math_spline.cpp:2152-2190)
-__device__ double deltaLookup(const FudgeTables& F, double x, double y)
+static __device__ double deltaLookup(const FudgeTables& F, double x, double y)
 {
     const int nx = F.nE, ny = F.nL;
     const int xi = binSearch(x, F.gridE, nx), yi = binSearch(y, F.gridL, ny);
@@ -184,46 +184,63 @@ struct FudgeRootFnSemiInf {
     }
 };
 
-struct FudgeLimits { double lambda_min, lambda_max, nu_min, nu_max; int order; };
+/// State of one point between the phases of the action computation: the point in prolate
+/// spheroidal coordinates, its integrals of motion, the integration limits known so far and the
+/// brackets of the roots still to be found.  One 128-byte record per point.
+struct __align__(16) FudgeRecord {
+    double lambda, nu, D2, E, Lz, I3, flambda, fnu, phi;
+    double lambdaMin, lambdaMax, nuMax;     // nu_min is always 0
+    double nuUpper;                         // nu_max root bracket: [|nu|, nuUpper]
+    double lambdaLower, lambdaPos;          // lambda_min root in [lambdaLower, lambdaPos];
+                                            // lambda_max root in [lambdaPos, inf)
+    int roots;                              // ROOT_* bits of the roots still to be found
+    int valid;                              // 0: the point has no integrals to do
+};
+static_assert(sizeof(FudgeRecord) == 128, "FudgeRecord is one 128-byte line");
 
-/// integration limits of the lambda and nu motions; reference findIntegrationLimitsAxisym
-__device__ FudgeLimits fudgeLimits(const FudgeFunction& fnc, int* rootIters)
+enum { ROOT_NU_MAX = 1, ROOT_LAMBDA_MIN = 2, ROOT_LAMBDA_MAX = 4 };
+
+__device__ __forceinline__ void loadFudgeFunction(const MultipoleView& M, const FudgeRecord& r, FudgeFunction& f)
 {
-    FudgeLimits lim;
+    f.M = &M;
+    f.lambda = r.lambda; f.nu = r.nu; f.phi = r.phi; f.D2 = r.D2;
+    f.E = r.E; f.Lz = r.Lz; f.I3 = r.I3; f.flambda = r.flambda; f.fnu = r.fnu;
+    f.bad = 0;
+}
+
+/** Integration limits of the lambda and nu motions (findIntegrationLimitsAxisym,
+    src/actions_staeckel.cpp:360-483), part 1: every decision up to the three root searches, whose
+    brackets go into the record; limits that need no root are stored directly (NaN otherwise). */
+static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& rec)
+{
     const double delta = fnc.D2;
     const double f_zero = fnc.value(0);
     double f_lambda, df_lambda, d2f_lambda;
     fnc.eval<true, true>(fnc.lambda, &f_lambda, &df_lambda, &d2f_lambda);
-    lim.nu_min = 0;
-    lim.nu_max = lim.lambda_min = lim.lambda_max = NAN;
+    double nu_max = NAN, lambda_min = NAN, lambda_max = NAN;
     double nu_upper = delta, lambda_lower = delta;
-    FudgeRootFn rf{ &fnc };
-    int it;
+    int roots = 0;
     if(fnc.Lz == 0) {
         const double dminus = delta * (1 - 1e-15), dplus = delta * (1 + 1e-15);
         if(fnc.value(dminus) < 0) {
             if(f_zero > 0) nu_upper = dminus;
-            else lim.nu_max = lim.nu_min;
+            else nu_max = 0;
         } else
-            lim.nu_max = delta;
+            nu_max = delta;
         if(fnc.value(dplus) < 0) lambda_lower = dplus;
-        else lim.lambda_min = delta;
+        else lambda_min = delta;
     }
-    if(!isFinite(lim.nu_max)) {
-        if(f_zero > 0) {
-            lim.nu_max = findRoot(rf, fabs(fnc.nu), nu_upper, FUDGE_ACCURACY_RANGE, &it);
-            *rootIters += it;
-        }
-        if(!isFinite(lim.nu_max))
-            lim.nu_max = fabs(fnc.nu);
+    if(!isFinite(nu_max)) {
+        if(f_zero > 0) roots |= ROOT_NU_MAX;           // falls back to |nu| if no root is found
+        else nu_max = fabs(fnc.nu);
     }
     double lambda_pos = fnc.lambda;
     const double dxToRoot = -f_lambda / df_lambda;
     if(f_lambda <= 0 || fabs(dxToRoot) < fnc.lambda * FUDGE_MINIMUM_RANGE) {
-        if(df_lambda >= 0) lim.lambda_min = fnc.lambda;
+        if(df_lambda >= 0) lambda_min = fnc.lambda;
         if(df_lambda <= 0) {
-            lim.lambda_max = fnc.lambda;
-            if(fnc.lambda == delta) lim.lambda_min = delta;
+            lambda_max = fnc.lambda;
+            if(fnc.lambda == delta) lambda_min = delta;
         }
         bool nearShell = d2f_lambda < 0 &&
             pow2(df_lambda) - 2 * f_lambda * d2f_lambda - pow2(fnc.lambda * FUDGE_MINIMUM_RANGE * d2f_lambda) < 0;
@@ -234,22 +251,45 @@ __device__ FudgeLimits fudgeLimits(const FudgeFunction& fnc, int* rootIters)
         nearShell |= d2f_lp < 0 &&
             pow2(df_lp) - 2 * f_lp * d2f_lp - pow2(fnc.lambda * FUDGE_MINIMUM_RANGE * d2f_lp) < 0;
         if(nearShell || f_lp < 0)
-            lim.lambda_min = lim.lambda_max = fnc.lambda;
+            lambda_min = lambda_max = fnc.lambda;
     }
-    if(!isFinite(lim.lambda_min)) {
-        lim.lambda_min = findRoot(rf, lambda_lower, lambda_pos, FUDGE_ACCURACY_RANGE, &it);
-        *rootIters += it;
+    if(!isFinite(lambda_min)) roots |= ROOT_LAMBDA_MIN;
+    if(!isFinite(lambda_max)) roots |= ROOT_LAMBDA_MAX;
+    rec.nuMax = nu_max; rec.lambdaMin = lambda_min; rec.lambdaMax = lambda_max;
+    rec.nuUpper = nu_upper; rec.lambdaLower = lambda_lower; rec.lambdaPos = lambda_pos;
+    rec.roots = roots;
+}
+
+/** Part 2: one of the root searches of part 1 (ROOT_* kind); returns the limit. */
+static __device__ double fudgeLimitRoot(const FudgeFunction& fnc, const FudgeRecord& rec, int kind, int* rootIters)
+{
+    int it = 0;
+    double x;
+    if(kind == ROOT_NU_MAX) {
+        x = findRoot(FudgeRootFn{ &fnc }, fabs(fnc.nu), rec.nuUpper, FUDGE_ACCURACY_RANGE, &it);
+        if(!isFinite(x)) x = fabs(fnc.nu);
+    } else if(kind == ROOT_LAMBDA_MIN) {
+        x = findRoot(FudgeRootFn{ &fnc }, rec.lambdaLower, rec.lambdaPos, FUDGE_ACCURACY_RANGE, &it);
+    } else {
+        FudgeRootFnSemiInf sf{ &fnc, rec.lambdaPos };
+        const double sroot = findRoot(sf, 0, 1, FUDGE_ACCURACY_RANGE, &it);
+        x = unscaleSemiInf(rec.lambdaPos, sroot, nullptr);
     }
-    if(!isFinite(lim.lambda_max)) {
-        FudgeRootFnSemiInf sf{ &fnc, lambda_pos };
-        const double s = findRoot(sf, 0, 1, FUDGE_ACCURACY_RANGE, &it);
-        *rootIters += it;
-        lim.lambda_max = unscaleSemiInf(lambda_pos, s, nullptr);
-    }
+    *rootIters += it;
+    return x;
+}
+
+struct FudgeLimits { double lambda_min, lambda_max, nu_max; int order; };
+
+/** Part 3: the final checks of the limits and the Gauss-Legendre order of both integrals. */
+static __device__ FudgeLimits fudgeLimitsFinish(const FudgeRecord& rec)
+{
+    const double delta = rec.D2;
+    FudgeLimits lim{ rec.lambdaMin, rec.lambdaMax, rec.nuMax, 0 };
     if(!(lim.nu_max >= delta * FUDGE_MINIMUM_RANGE))
         lim.nu_max = 0;
     if(!(lim.lambda_max - lim.lambda_min >= delta * FUDGE_MINIMUM_RANGE))
-        lim.lambda_min = lim.lambda_max = fnc.lambda;
+        lim.lambda_min = lim.lambda_max = rec.lambda;
     const double ratio = sqrt((lim.lambda_min - delta) / (lim.lambda_max - delta));
     if(ratio == 0) lim.order = GL_MAX_ORDER;
     else {
@@ -262,7 +302,7 @@ __device__ FudgeLimits fudgeLimits(const FudgeFunction& fnc, int* rootIters)
 
 /// integral of sqrt(p^2(tau)) over [lo, hi] with the cubic end-point stretch
 /// (integrateGL of ScaledIntegrand<ScalingCub>(AxisymIntegrand), src/math_core.cpp:1191-1205)
-__device__ double fudgeMomentumIntegral(const FudgeFunction& fnc, const GLRules& gl, double lo, double hi, int order)
+static __device__ double fudgeMomentumIntegral(const FudgeFunction& fnc, const GLRules& gl, double lo, double hi, int order)
 {
     int N = order < 1 ? 1 : order;
     while(gl.offset[N] < 0) N++;
@@ -281,14 +321,22 @@ __device__ double fudgeMomentumIntegral(const FudgeFunction& fnc, const GLRules&
     return sum;
 }
 
-/** Actions (Jr, Jz, Jphi) of one point (R, z, phi, vR, vz, vphi) for focal distance fd
-    (evalAxisymFudge: fd <= 0 falls back to max(R,1)*1e-4); Phi is the potential at the point. */
-__device__ void fudgeActions(const MultipoleView& M, const GLRules& gl, const double* pc, double Phi,
-    double fd, double* act, int* rootIters)
+/** Phase 1 of the actions of one point (R, z, phi, vR, vz, vphi) for focal distance fd
+    (evalAxisymFudge, src/actions_staeckel.cpp:683-693: fd <= 0 falls back to max(R,1)*1e-4);
+    Phi is the potential at the point.  Writes Jphi into act[2]; for a point without actions
+    (unbound, or lambda = nu = Delta^2) also NaN into act[0..1] and marks the record invalid.
+    Otherwise the record holds the integrals of motion (findIntegralsOfMotionAxisymFudge,
+    :176-195) and the limits and root brackets of fudgeLimitsSetup. */
+static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, double Phi, double fd,
+    FudgeRecord& rec, double* act)
 {
     const double R = pc[0], z = pc[1], phi = pc[2], vR = pc[3], vz = pc[4], vphi = pc[5];
     if(fd <= 0) fd = fmax(R, 1.) * 1e-4;
     const double D2 = fd * fd;
+    const double Lz = R * vphi;
+    act[2] = Lz;
+    rec.valid = 0;
+    rec.roots = 0;
     // cylindrical -> prolate spheroidal (src/coord.cpp:294-338) and velocities (:525-531)
     const double R2 = R * R, z2 = z * z, signz = z >= 0 ? 1 : -1;
     const double sum = R2 + z2 + D2, dif = R2 + z2 - D2;
@@ -301,8 +349,7 @@ __device__ void fudgeActions(const MultipoleView& M, const GLRules& gl, const do
     const double lambda = D2 + lmd;
     double absnu = 2 * D2 / (sum + sqD) * z2;
     if(absnu * 2 > D2) absnu = D2 - dmn; else dmn = D2 - absnu;
-    const double Lz = R * vphi;
-    if(sqD == 0) { act[0] = act[1] = NAN; act[2] = Lz; return; }   // lambda = nu = Delta^2: undefined
+    if(sqD == 0) { act[0] = act[1] = NAN; return; }   // lambda = nu = Delta^2: undefined
     FudgeFunction fnc;
     fnc.M = &M;
     fnc.lambda = lambda;
@@ -319,14 +366,23 @@ __device__ void fudgeActions(const MultipoleView& M, const GLRules& gl, const do
     fnc.flambda = -lambda * Phi0;
     fnc.fnu = fnc.flambda + Phi * (lambda - absnu);
     fnc.I3 = lambda * (Phi - Phi0) + 0.5 * (pow2(z * vphi) + pow2(R * vz - z * vR) + pow2(vz) * D2);
-    if(!isFinite(fnc.E + fnc.I3 + fnc.Lz) || fnc.E >= 0) {
-        act[0] = act[1] = NAN; act[2] = Lz;
-        return;
-    }
-    const FudgeLimits lim = fudgeLimits(fnc, rootIters);
-    act[0] = fudgeMomentumIntegral(fnc, gl, lim.lambda_min, lim.lambda_max, lim.order) / M_PI;
-    act[1] = fudgeMomentumIntegral(fnc, gl, lim.nu_min, lim.nu_max, lim.order) / M_PI * 2;
-    act[2] = Lz;
+    if(!isFinite(fnc.E + fnc.I3 + fnc.Lz) || fnc.E >= 0) { act[0] = act[1] = NAN; return; }
+    rec.lambda = fnc.lambda; rec.nu = fnc.nu; rec.D2 = D2; rec.E = fnc.E; rec.Lz = Lz; rec.I3 = fnc.I3;
+    rec.flambda = fnc.flambda; rec.fnu = fnc.fnu; rec.phi = phi;
+    fudgeLimitsSetup(fnc, rec);
+    rec.valid = 1;
+}
+
+/** Last phase: one of the two action integrals of a prepared point whose roots are found
+    (computeActions, src/actions_staeckel.cpp:604-619): which = 0 gives Jr, 1 gives Jz. */
+static __device__ double fudgeIntegral(const MultipoleView& M, const GLRules& gl, const FudgeRecord& rec, int which)
+{
+    FudgeFunction fnc;
+    loadFudgeFunction(M, rec, fnc);
+    const FudgeLimits lim = fudgeLimitsFinish(rec);
+    return which == 0 ?
+        fudgeMomentumIntegral(fnc, gl, lim.lambda_min, lim.lambda_max, lim.order) / M_PI :
+        fudgeMomentumIntegral(fnc, gl, 0, lim.nu_max, lim.order) / M_PI * 2;
 }
 
 /// Cartesian posvel -> cylindrical (R, z, phi, vR, vz, vphi); reference src/coord.cpp:476-484
@@ -348,7 +404,7 @@ __device__ __forceinline__ void carToCylPosVel(const double* w, double* pc)
 /** focal distance of the action finder at a point with potential Phi: E, Lz -> Lcirc(E) ->
     (xi, chi) -> Delta; reference ActionFinderAxisymFudge::eval steps 0-1,
     src/actions_staeckel.cpp:957-977 */
-__device__ double finderFocalDistance(const FudgeTables& F, const double* pc, double Phi)
+static __device__ double finderFocalDistance(const FudgeTables& F, const double* pc, double Phi)
 {
     const double E = Phi + 0.5 * (pc[3] * pc[3] + pc[4] * pc[4] + pc[5] * pc[5]);
     const double Lz = pc[0] * pc[5];

@@ -1,0 +1,19 @@
+// Launchers of the phases of the Staeckel-fudge action computation (one record per point, see
+// FudgeRecord): phase 1 (prepare) lives in actions.cu, phases 2 and 3 in their own units.
+#pragma once
+#include <cuda_runtime.h>
+#include "multipole.h"
+#include "fudge_types.h"
+
+namespace agb {
+
+struct FudgeRecord;
+
+/// phase 2: the root searches of the integration limits (three launches, one per kind of limit)
+void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, cudaStream_t stream);
+
+/// phase 3: Jr and Jz of every valid record into act[3 i], act[3 i + 1]
+void launchFudgeIntegrals(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,
+    cudaStream_t stream);
+
+}  // namespace agb

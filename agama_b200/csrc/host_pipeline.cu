@@ -87,6 +87,20 @@ struct Call {
 
 }  // namespace
 
+void* scratchAlloc(size_t bytes, cudaStream_t stream)
+{
+    int device;
+    AGB_CUDA(cudaGetDevice(&device));
+    void* p = nullptr;
+    AGB_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, ALIGN), poolFor(device), stream));
+    return p;
+}
+
+void scratchFree(void* ptr, cudaStream_t stream)
+{
+    if(ptr) cudaFreeAsync(ptr, stream);
+}
+
 void runChunked(long n, const std::vector<HostIn>& ins, const std::vector<HostOut>& outs,
     const ChunkLaunch& launch, long chunk)
 {

@@ -26,4 +26,18 @@ using ChunkLaunch = std::function<void(long first, long count, void* const* dIn,
 void runChunked(long n, const std::vector<HostIn>& ins, const std::vector<HostOut>& outs,
     const ChunkLaunch& launch, long chunk = 0);
 
+/// stream-ordered scratch of the current device from the engine's pool (kept between calls)
+void* scratchAlloc(size_t bytes, cudaStream_t stream);
+void scratchFree(void* ptr, cudaStream_t stream);
+
+/// RAII holder of pool scratch, released on its stream
+struct Scratch {
+    void* ptr = nullptr;
+    cudaStream_t stream = 0;
+    Scratch(size_t bytes, cudaStream_t s) : ptr(scratchAlloc(bytes, s)), stream(s) {}
+    Scratch(const Scratch&) = delete;
+    Scratch& operator=(const Scratch&) = delete;
+    ~Scratch() { if(ptr) scratchFree(ptr, stream); }
+};
+
 }  // namespace agb
