@@ -110,8 +110,9 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
     if(n <= 0) return;
     const GLRules& gl = glRulesForCurrentDevice();
     const long pass = std::min(n, POINTS_PER_PASS);
-    Scratch recs(pass * sizeof(FudgeRecord), stream);
+    Scratch recs(pass * sizeof(FudgeRecord) + 256, stream);     // records, then the work counter
     FudgeRecord* rec = static_cast<FudgeRecord*>(recs.ptr);
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(rec + pass);
     for(long first = 0; first < n; first += pass) {
         const long count = std::min(pass, n - first);
         int* it = iters ? iters + first : nullptr;
@@ -119,7 +120,7 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
             M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, act + 3 * first,
             fdOut ? fdOut + first : nullptr, it);
         AGB_CUDA(cudaGetLastError());
-        launchFudgeRoots(M, count, rec, it, stream);
+        launchFudgeRoots(M, count, rec, it, counter, stream);
         launchFudgeIntegrals(M, gl, count, rec, act + 3 * first, stream);
     }
 }

@@ -287,4 +287,108 @@ AGB_HD double findRoot(const F& fnc, double xlower, double xupper, double reltol
     return b;
 }
 
+/** findRoot (with derivatives) as a resumable state machine: the caller evaluates the function
+    wherever the search asks, so that lanes of a warp that run different searches, at different
+    iterations, meet at one evaluation site.  Arithmetic and results are those of findRoot above:
+
+        double x = s.start(lo, hi, reltol);
+        while(true) { f(x, &fx, &dx); if(s.feed(fx, dx, &x)) break; }
+        root = s.result; iterations = s.iter;                                               */
+struct RootSearch {
+    double a, b, c, fa, fb, fc, da, db, dc, d, e, abstol;
+    double result;
+    int iter, phase;     // phase 0: wants f(xlower), 1: f(xupper), 2: f(next iterate)
+
+    AGB_HD double start(double xlower, double xupper, double reltol)
+    {
+        a = xlower; b = xupper;
+        abstol = fabs(xlower - xupper) * reltol;
+        iter = 0; phase = 0;
+        return a;
+    }
+
+    /// take f and f' at the requested point; true when the search has finished (result set),
+    /// otherwise *xnext is the next point to evaluate
+    AGB_HD bool feed(double fx, double dx, double* xnext)
+    {
+        if(phase == 0) {
+            fa = fx; da = dx;
+            phase = 1;
+            *xnext = b;
+            return false;
+        }
+        if(phase == 1) {
+            fb = fx; db = dx;
+            if((fa < 0 && fb < 0) || (fa > 0 && fb > 0) || !isFinite(fa + fb)) { result = NAN; return true; }
+            if(fa == 0) { result = fb == 0 ? 0.5 * (a + b) : a; return true; }
+            if(fb == 0) { result = b; return true; }
+            c = a; fc = fa; dc = da; d = b - c; e = b - c;
+            if(fabs(fc) < fabs(fb)) {
+                a = b; b = c; c = a;  fa = fb; fb = fc; fc = fa;  da = db; db = dc; dc = da;
+            }
+            phase = 2;
+            return propose(xnext);
+        }
+        fb = fx; db = dx;
+        if(!isFinite(fb)) { result = NAN; return true; }
+        if((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) {
+            c = a; fc = fa; dc = da; d = b - c; e = b - c;
+        }
+        if(fabs(fc) < fabs(fb)) {
+            a = b; b = c; c = a;  fa = fb; fb = fc; fc = fa;  da = db; db = dc; dc = da;
+        }
+        iter++;
+        if(fabs(b - c) <= abstol) {
+            const double off = fb * (b - c) / (fc - fb);
+            if((off > 0 && off < c - b) || (off < 0 && off > c - b))
+                b += off;
+            result = b;
+            return true;
+        }
+        const double off = -fb / db;
+        const bool inside = (off > 0 && off < c - b) || (off < 0 && off > c - b);
+        if(inside && fabs(off) < abstol) { result = b + off; return true; }
+        if(iter >= ROOT_MAXITER) { result = b; return true; }
+        return propose(xnext);
+    }
+
+    /// the head of one iteration: convergence test and the next iterate
+    AGB_HD bool propose(double* xnext)
+    {
+        const double tol = 0.5 * DBL_EPSILON * fabs(b), cb = c - b, m = 0.5 * cb;
+        if(fb == 0 || fabs(m) <= tol) { result = b; return true; }
+        if(fabs(e) < tol || fabs(fa) <= fabs(fb)) {
+            d = m; e = m;
+        } else {
+            double dd = NAN;
+            if(db * dc > 0)
+                dd = hermiteMonotone(0, fb, fc, 0, cb, 1 / db, 1 / dc);
+            if(isFinite(dd) && fmin(fabs(dd), fabs(cb - dd)) > fabs(cb) * ROOT_DELTA_HERMITE) {
+                d = dd;
+            } else {
+                double p, q, r, s = fb / fa;
+                if(a == c) {
+                    p = 2 * m * s;
+                    q = 1 - s;
+                } else {
+                    q = fa / fc;
+                    r = fb / fc;
+                    p = s * (2 * m * q * (q - r) - (b - a) * (r - 1));
+                    q = (q - 1) * (r - 1) * (s - 1);
+                }
+                if(p > 0) q = -q; else p = -p;
+                if(2 * p < fmin(3 * m * q - fabs(tol * q), fabs(e * q))) {
+                    e = d; d = p / q;
+                } else {
+                    d = m; e = m;
+                }
+            }
+        }
+        a = b; fa = fb; da = db;
+        b += fabs(d) > tol ? d : (m > 0 ? tol : -tol);
+        *xnext = b;
+        return false;
+    }
+};
+
 }  // namespace agb

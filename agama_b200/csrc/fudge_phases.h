@@ -9,8 +9,10 @@ namespace agb {
 
 struct FudgeRecord;
 
-/// phase 2: the root searches of the integration limits (three launches, one per kind of limit)
-void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, cudaStream_t stream);
+/// phase 2: the root searches of the integration limits, drained by a persistent grid from a
+/// device work counter (8 bytes, zeroed here on the stream)
+void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, unsigned long long* counter,
+    cudaStream_t stream);
 
 /// phase 3: Jr and Jz of every valid record into act[3 i], act[3 i + 1]
 void launchFudgeIntegrals(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,

@@ -238,8 +238,8 @@ def run_engine(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = n * world / (float(t.item()) / 1000)
     if rank == 0:
-        # ---- roofline of the dominant kernel (FP64-pipe bound): executed FP64 flops per action
-        # from the ncu summary (profiles/fudge_actions_cfg2.md); peak measured on this device
+        # ---- roofline of the action kernels (FP64-pipe bound): executed FP64 flops per action
+        # from an ncu capture of this workload; peak measured on this device
         import ctypes
         pk = ctypes.c_double(0)
         _native.check(lib.agama_measureFP64Throughput(ctypes.byref(pk)))
@@ -253,7 +253,7 @@ def run_engine(args):
                        "l2": "flushed between steps (256 MB write)", "parallelism": "replicas x%d" % world},
             "e2e": {"value": e2e_val, "unit": "actions/s", "h2d_bytes_per_step": int(pts.nbytes),
                     "d2h_bytes_per_step": int(n * 3 * 8)},
-            "gpu_launches": args.steps,
+            "gpu_launches": ACTION_LAUNCHES_PER_STEP * args.steps,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
                          "frac": achieved / pk.value if pk.value else None, "traffic": TRAFFIC_PER_LAUNCH_CFG2,
                          "peak_source": "measured FP64 FMA throughput of this device (agama_measureFP64Throughput)",
@@ -267,8 +267,10 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
-# executed FP64 flops per action (dadd + dmul + 2 dfma, ncu, config-2 workload) and DRAM bytes per
-# launch of the fudge kernel for 1e6 particles; see profiles/fudge_actions_cfg2.md
+# kernels per action step: prepare, three root-search kinds, integrals
+ACTION_LAUNCHES_PER_STEP = 5
+# executed FP64 flops per action (dadd + dmul + 2 dfma summed over the five kernels, ncu, config-2
+# workload) and DRAM bytes of one step for 1e6 particles
 FLOPS_PER_ACTION_CFG2 = 26206.0
 # dram read + write of one 200 000-particle launch (9.89 MB + 0.22 MB), scaled to 1e6 particles
 TRAFFIC_PER_LAUNCH_CFG2 = 5 * (9.888256e6 + 0.220416e6)
