@@ -110,7 +110,7 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
     if(n <= 0) return;
     const GLRules& gl = glRulesForCurrentDevice();
     const long pass = std::min(n, POINTS_PER_PASS);
-    Scratch recs(pass * sizeof(FudgeRecord) + 256, stream);     // records, then the work counter
+    Scratch recs(pass * sizeof(FudgeRecord) + 256, stream);     // records, then two work counters
     FudgeRecord* rec = static_cast<FudgeRecord*>(recs.ptr);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(rec + pass);
     for(long first = 0; first < n; first += pass) {
@@ -121,7 +121,7 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
             fdOut ? fdOut + first : nullptr, it);
         AGB_CUDA(cudaGetLastError());
         launchFudgeRoots(M, count, rec, it, counter, stream);
-        launchFudgeIntegrals(M, gl, count, rec, act + 3 * first, stream);
+        launchFudgeIntegrals(M, gl, count, rec, act + 3 * first, counter + 1, stream);
     }
 }
 

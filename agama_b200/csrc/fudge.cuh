@@ -151,39 +151,6 @@ struct FudgeFunction {
     __device__ double value(double tau) const { double v; eval<false, false>(tau, &v, nullptr, nullptr); return v; }
 };
 
-/// F(tau) with its first derivative, as the root finder sees it
-struct FudgeRootFn {
-    static constexpr bool hasDeriv = true;
-    const FudgeFunction* f;
-    __device__ void operator()(double x, double* v, double* d) const {
-        if(d) f->eval<true, false>(x, v, d, nullptr); else f->eval<false, false>(x, v, nullptr, nullptr);
-    }
-};
-
-/// F(tau)/tau^2 on [lambda_pos, inf) mapped to s in [0, 1] by the semi-infinite scaling
-/// (AxisymScaledForRootfinder inside ScaledFnc<ScalingSemiInf>, src/actions_staeckel.cpp:329-354,
-/// src/math_core.h:214-232)
-struct FudgeRootFnSemiInf {
-    static constexpr bool hasDeriv = true;
-    const FudgeFunction* f;
-    double u0;
-    __device__ void operator()(double s, double* v, double* d) const {
-        double duds;
-        const double tau = unscaleSemiInf(u0, s, d ? &duds : nullptr);
-        double fv, dfdu = NAN;
-        if(tau > 1e100) {
-            fv = f->E;
-        } else {
-            double fval, fder;
-            if(d) f->eval<true, false>(tau, &fval, &fder, nullptr); else f->eval<false, false>(tau, &fval, nullptr, nullptr);
-            fv = fval / pow2(tau);
-            if(d) dfdu = (fder - 2 * fval / tau) / pow2(tau);
-        }
-        *v = fv;
-        if(d) *d = dfdu * duds;
-    }
-};
-
 /// State of one point between the phases of the action computation: the point in prolate
 /// spheroidal coordinates, its integrals of motion, the integration limits known so far and the
 /// brackets of the roots still to be found.  One 128-byte record per point.
@@ -199,6 +166,27 @@ struct __align__(16) FudgeRecord {
 static_assert(sizeof(FudgeRecord) == 128, "FudgeRecord is one 128-byte line");
 
 enum { ROOT_NU_MAX = 1, ROOT_LAMBDA_MIN = 2, ROOT_LAMBDA_MAX = 4 };
+
+/** The root functions of the three integration limits behind one evaluation site (kind
+    ROOT_NU_MAX, ROOT_LAMBDA_MIN: F(tau) and F'(tau); ROOT_LAMBDA_MAX: F(tau)/tau^2 on
+    [u0, inf) mapped to s in [0, 1] by the semi-infinite scaling, AxisymScaledForRootfinder inside
+    ScaledFnc<ScalingSemiInf>, src/actions_staeckel.cpp:329-354, src/math_core.h:214-232). */
+__device__ __forceinline__ void limitRootEval(const FudgeFunction& f, int kind, double u0, double x,
+    double* v, double* d)
+{
+    const bool semiInf = kind == ROOT_LAMBDA_MAX;
+    double duds = 1, tau = x;
+    if(semiInf) tau = unscaleSemiInf(u0, x, &duds);
+    const bool far = semiInf && tau > 1e100;
+    double fval = 0, fder = 0;
+    if(!far) f.eval<true, false>(tau, &fval, &fder, nullptr);
+    if(!semiInf) { *v = fval; *d = fder; }
+    else if(far) { *v = f.E; *d = NAN; }
+    else {
+        *v = fval / pow2(tau);
+        *d = (fder - 2 * fval / tau) / pow2(tau) * duds;
+    }
+}
 
 __device__ __forceinline__ void loadFudgeFunction(const MultipoleView& M, const FudgeRecord& r, FudgeFunction& f)
 {
@@ -260,28 +248,10 @@ static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& r
     rec.roots = roots;
 }
 
-/** Part 2: one of the root searches of part 1 (ROOT_* kind); returns the limit. */
-static __device__ double fudgeLimitRoot(const FudgeFunction& fnc, const FudgeRecord& rec, int kind, int* rootIters)
-{
-    int it = 0;
-    double x;
-    if(kind == ROOT_NU_MAX) {
-        x = findRoot(FudgeRootFn{ &fnc }, fabs(fnc.nu), rec.nuUpper, FUDGE_ACCURACY_RANGE, &it);
-        if(!isFinite(x)) x = fabs(fnc.nu);
-    } else if(kind == ROOT_LAMBDA_MIN) {
-        x = findRoot(FudgeRootFn{ &fnc }, rec.lambdaLower, rec.lambdaPos, FUDGE_ACCURACY_RANGE, &it);
-    } else {
-        FudgeRootFnSemiInf sf{ &fnc, rec.lambdaPos };
-        const double sroot = findRoot(sf, 0, 1, FUDGE_ACCURACY_RANGE, &it);
-        x = unscaleSemiInf(rec.lambdaPos, sroot, nullptr);
-    }
-    *rootIters += it;
-    return x;
-}
-
 struct FudgeLimits { double lambda_min, lambda_max, nu_max; int order; };
 
-/** Part 3: the final checks of the limits and the Gauss-Legendre order of both integrals. */
+/** Part 3 (part 2 is the root searches: RootSearch driven by limitRootEval): the final checks of
+    the limits and the Gauss-Legendre order of both integrals. */
 static __device__ FudgeLimits fudgeLimitsFinish(const FudgeRecord& rec)
 {
     const double delta = rec.D2;
@@ -300,25 +270,18 @@ static __device__ FudgeLimits fudgeLimitsFinish(const FudgeRecord& rec)
     return lim;
 }
 
-/// integral of sqrt(p^2(tau)) over [lo, hi] with the cubic end-point stretch
-/// (integrateGL of ScaledIntegrand<ScalingCub>(AxisymIntegrand), src/math_core.cpp:1191-1205)
-static __device__ double fudgeMomentumIntegral(const FudgeFunction& fnc, const GLRules& gl, double lo, double hi, int order)
+/** One node of the momentum integral of sqrt(p^2(tau)) over [lo, hi] with the cubic end-point
+    stretch (integrateGL of ScaledIntegrand<ScalingCub>(AxisymIntegrand), src/math_core.cpp:1191-1205,
+    src/actions_staeckel.cpp:276-299): the integrand times du/ds at the scaled node s. */
+static __device__ double fudgeMomentumNode(const FudgeFunction& fnc, double lo, double hi, double s)
 {
-    int N = order < 1 ? 1 : order;
-    while(gl.offset[N] < 0) N++;
-    const double* x = gl.nodes + gl.offset[N];
-    const double* w = gl.weights + gl.offset[N];
-    double sum = 0;
-    for(int i = 0; i < N; i++) {
-        double duds;
-        const double tau = unscaleCub(lo, hi, ldg(x + i), &duds);
-        const double tmd = tau - fnc.D2;
-        const double p2 = fnc.value(tau) / (2 * pow2(tmd) * tau);
-        double v = p2 < 0 ? 0 : sqrt(p2);
-        if(!isFinite(v)) v = 0;
-        sum += ldg(w + i) * (v * duds);
-    }
-    return sum;
+    double duds;
+    const double tau = unscaleCub(lo, hi, s, &duds);
+    const double tmd = tau - fnc.D2;
+    const double p2 = fnc.value(tau) / (2 * pow2(tmd) * tau);
+    double v = p2 < 0 ? 0 : sqrt(p2);
+    if(!isFinite(v)) v = 0;
+    return v * duds;
 }
 
 /** Phase 1 of the actions of one point (R, z, phi, vR, vz, vphi) for focal distance fd
@@ -371,18 +334,6 @@ static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, do
     rec.flambda = fnc.flambda; rec.fnu = fnc.fnu; rec.phi = phi;
     fudgeLimitsSetup(fnc, rec);
     rec.valid = 1;
-}
-
-/** Last phase: one of the two action integrals of a prepared point whose roots are found
-    (computeActions, src/actions_staeckel.cpp:604-619): which = 0 gives Jr, 1 gives Jz. */
-static __device__ double fudgeIntegral(const MultipoleView& M, const GLRules& gl, const FudgeRecord& rec, int which)
-{
-    FudgeFunction fnc;
-    loadFudgeFunction(M, rec, fnc);
-    const FudgeLimits lim = fudgeLimitsFinish(rec);
-    return which == 0 ?
-        fudgeMomentumIntegral(fnc, gl, lim.lambda_min, lim.lambda_max, lim.order) / M_PI :
-        fudgeMomentumIntegral(fnc, gl, 0, lim.nu_max, lim.order) / M_PI * 2;
 }
 
 /// Cartesian posvel -> cylindrical (R, z, phi, vR, vz, vphi); reference src/coord.cpp:476-484

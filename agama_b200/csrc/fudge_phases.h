@@ -14,8 +14,9 @@ struct FudgeRecord;
 void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, unsigned long long* counter,
     cudaStream_t stream);
 
-/// phase 3: Jr and Jz of every valid record into act[3 i], act[3 i + 1]
+/// phase 3: Jr and Jz of every valid record into act[3 i], act[3 i + 1], drained by a persistent
+/// grid from a device work counter (8 bytes, zeroed here on the stream)
 void launchFudgeIntegrals(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,
-    cudaStream_t stream);
+    unsigned long long* counter, cudaStream_t stream);
 
 }  // namespace agb

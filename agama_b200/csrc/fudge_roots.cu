@@ -15,26 +15,6 @@ namespace {
 constexpr int ROOT_BLOCK = 128;
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
-/// the root functions of the three limits behind one evaluation site: F(tau) with F'(tau) for
-/// nu_max and lambda_min (FudgeRootFn), F(tau)/tau^2 in the semi-infinite scaling about u0 for
-/// lambda_max (FudgeRootFnSemiInf); same arithmetic as those functors
-__device__ __forceinline__ void limitRootEval(const FudgeFunction& f, int kind, double u0, double x,
-    double* v, double* d)
-{
-    const bool semiInf = kind == ROOT_LAMBDA_MAX;
-    double duds = 1, tau = x;
-    if(semiInf) tau = unscaleSemiInf(u0, x, &duds);
-    const bool far = semiInf && tau > 1e100;
-    double fval = 0, fder = 0;
-    if(!far) f.eval<true, false>(tau, &fval, &fder, nullptr);
-    if(!semiInf) { *v = fval; *d = fder; }
-    else if(far) { *v = f.E; *d = NAN; }
-    else {
-        *v = fval / pow2(tau);
-        *d = (fder - 2 * fval / tau) / pow2(tau) * duds;
-    }
-}
-
 /// Phase 2: every root search of the integration limits (task t = kind * n + i for the kinds
 /// nu_max, lambda_min, lambda_max of point i) drained from one work counter by a persistent grid.
 /// Each lane runs one search as a RootSearch state machine and takes the next task as soon as
