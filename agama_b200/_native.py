@@ -48,6 +48,12 @@ SIGNATURES = {
     "agama_evalActionsStandaloneMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, D]),
     "agama_evalActionsStandaloneManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double, VP,
                                                              VP, VP]),
+    "agama_evalActionsAnglesFrequenciesMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, D, D]),
+    "agama_evalActionsAnglesFrequenciesManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
+    "agama_evalActionsAnglesFrequenciesStandaloneMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double,
+                                                                         D, D, D]),
+    "agama_evalActionsAnglesFrequenciesStandaloneManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP,
+                                                                               ctypes.c_double, VP, VP, VP, VP]),
 }
 
 _lib = None

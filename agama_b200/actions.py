@@ -5,6 +5,7 @@ Mirror of the reference's Python ActionFinder / actions (src/interface_python.cp
     af = ActionFinder(potential, tables=...)     # focal-distance table + L_circ(E) interpolator
     J  = af(points)                              # (n, 3): Jr, Jz, Jphi
     J  = actions(potential, points, fd=...)      # fixed focal distance(s)
+    J, theta, Omega = af(points, angles=True, frequencies=True)
 
 `points` are Cartesian phase-space points (n x 6) as numpy arrays (host) or CUDA torch tensors
 (device, processed on the current stream).
@@ -69,9 +70,20 @@ class ActionFinder:
         return dict(gridE=gE, gridL=gL, delta=dl, lofe=lofe, rofl=rofl, phiofr=phr, invPhi0=scal[0],
                     interp_invPhi0=scal[1], slopeOut=scal[2], coefOut=scal[3], massOut=scal[4])
 
-    def __call__(self, points, fd=False):
-        """actions (n x 3); with fd=True also the focal distance used for each point"""
+    def __call__(self, points, fd=False, actions=True, angles=False, frequencies=False):
+        """actions (n x 3: Jr, Jz, Jphi); with fd=True also the focal distance used for each point.
+        With angles / frequencies (n x 3: theta_r, theta_z, theta_phi / Omega_r, Omega_z,
+        Omega_phi), the requested arrays come back as a tuple in the order actions, angles,
+        frequencies, as the reference's ActionFinder does."""
         from . import _is_device_array, _dev_ptr, _current_stream
+        if angles or frequencies:
+            if fd:
+                raise ValueError("fd=True is not combined with angles / frequencies")
+            return _angles_call(points, actions, angles, frequencies,
+                                lambda n, p, a, t, f, dev: (
+                                    _native.lib().agama_evalActionsAnglesFrequenciesManyDevice(
+                                        self._h, n, p, a, t, f, _current_stream()) if dev else
+                                    _native.lib().agama_evalActionsAnglesFrequenciesMany(self._h, n, p, a, t, f)))
         if _is_device_array(points):
             import torch
             p = points.contiguous().view(-1, 6)
@@ -93,9 +105,52 @@ class ActionFinder:
         return (act, fdo) if fd else act
 
 
-def actions(potential, points, fd, iters=False):
-    """Staeckel-fudge actions for given focal distance(s) fd (scalar or per point)."""
+def _angles_call(points, want_act, want_ang, want_freq, call):
+    """run one of the angle / frequency entry points on host arrays or CUDA tensors"""
+    from . import _is_device_array, _dev_ptr
+    if _is_device_array(points):
+        import torch
+        p = points.contiguous().view(-1, 6)
+        n = p.shape[0]
+        outs = [torch.empty((n, 3), dtype=torch.float64, device=p.device) if w else None
+                for w in (want_act, want_ang, want_freq)]
+        check(call(n, _dev_ptr(p), *[_dev_ptr(o) for o in outs], True))
+        single = False
+    else:
+        p = np.ascontiguousarray(points, dtype=np.float64)
+        single = p.ndim == 1
+        p = p.reshape(-1, 6)
+        n = len(p)
+        outs = [np.empty((n, 3)) if w else None for w in (want_act, want_ang, want_freq)]
+        check(call(n, ptr(p), *[ptr(o) for o in outs], False))
+        if single:
+            outs = [o[0] if o is not None else None for o in outs]
+    res = [o for o in outs if o is not None]
+    return res[0] if len(res) == 1 else tuple(res)
+
+
+def actions(potential, points, fd, iters=False, angles=False, frequencies=False):
+    """Staeckel-fudge actions for given focal distance(s) fd (scalar or per point); with angles /
+    frequencies the tuple (actions, angles?, frequencies?) as in ActionFinder.__call__."""
     from . import _is_device_array, _dev_ptr, _current_stream
+    if angles or frequencies:
+        if iters:
+            raise ValueError("iters=True is not combined with angles / frequencies")
+        if _is_device_array(points):
+            fda = fd.contiguous() if _is_device_array(fd) else None
+            fdp, fd0 = _dev_ptr(fda), (0.0 if fda is not None else float(fd))
+        elif np.ndim(fd) == 0:
+            fda, fdp, fd0 = None, None, float(fd)
+        else:
+            n = len(np.reshape(points, (-1, 6)))
+            fda = np.ascontiguousarray(np.broadcast_to(np.asarray(fd, dtype=np.float64), (n,)))
+            fdp, fd0 = ptr(fda), 0.0
+        return _angles_call(points, True, angles, frequencies,
+                            lambda n, p, a, t, f, dev: (
+                                _native.lib().agama_evalActionsAnglesFrequenciesStandaloneManyDevice(
+                                    potential.handle, n, p, fdp, fd0, a, t, f, _current_stream()) if dev else
+                                _native.lib().agama_evalActionsAnglesFrequenciesStandaloneMany(
+                                    potential.handle, n, p, fdp, fd0, a, t, f)))
     if _is_device_array(points):
         import torch
         p = points.contiguous().view(-1, 6)

@@ -102,42 +102,52 @@ __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __g
     if(iters) iters[i] = 0;
 }
 
-/// the three phases over passes of at most POINTS_PER_PASS points (bounded scratch)
+/// the three phases over passes of at most POINTS_PER_PASS points (bounded scratch); with ang or
+/// freq the last phase also computes angles / frequencies (act may then be null)
 template<bool FINDER>
 void runActions(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel, const double* fd,
-    double fd0, double* act, double* fdOut, int* iters, cudaStream_t stream)
+    double fd0, double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream)
 {
     if(n <= 0) return;
     const GLRules& gl = glRulesForCurrentDevice();
     const long pass = std::min(n, POINTS_PER_PASS);
-    Scratch recs(pass * sizeof(FudgeRecord) + 256, stream);     // records, then two work counters
-    FudgeRecord* rec = static_cast<FudgeRecord*>(recs.ptr);
+    // records, two work counters, and the actions of a pass when the caller wants none
+    const size_t recBytes = pass * sizeof(FudgeRecord) + 256;
+    Scratch scratch(recBytes + (act ? 0 : pass * 3 * sizeof(double)), stream);
+    FudgeRecord* rec = static_cast<FudgeRecord*>(scratch.ptr);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(rec + pass);
+    double* actTmp = reinterpret_cast<double*>(static_cast<char*>(scratch.ptr) + recBytes);
+    const bool angles = ang || freq;
     for(long first = 0; first < n; first += pass) {
         const long count = std::min(pass, n - first);
         int* it = iters ? iters + first : nullptr;
+        double* a = act ? act + 3 * first : actTmp;
         fudgePrepareKernel<FINDER><<<(count + PREPARE_BLOCK - 1) / PREPARE_BLOCK, PREPARE_BLOCK, 0, stream>>>(
-            M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, act + 3 * first,
+            M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, a,
             fdOut ? fdOut + first : nullptr, it);
         AGB_CUDA(cudaGetLastError());
         launchFudgeRoots(M, count, rec, it, counter, stream);
-        launchFudgeIntegrals(M, gl, count, rec, act + 3 * first, counter + 1, stream);
+        if(angles)
+            launchFudgeAngles(M, gl, count, rec, a, ang ? ang + 3 * first : nullptr,
+                freq ? freq + 3 * first : nullptr, stream);
+        else
+            launchFudgeIntegrals(M, gl, count, rec, a, counter + 1, stream);
     }
 }
 
 }  // namespace
 
 void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
-    double* act, int* iters, cudaStream_t stream)
+    double* act, double* ang, double* freq, int* iters, cudaStream_t stream)
 {
     FudgeTables dummy{};
-    runActions<false>(M, dummy, n, posvel, fd, fd0, act, nullptr, iters, stream);
+    runActions<false>(M, dummy, n, posvel, fd, fd0, act, ang, freq, nullptr, iters, stream);
 }
 
 void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
-    double* act, double* fdOut, int* iters, cudaStream_t stream)
+    double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream)
 {
-    runActions<true>(M, F, n, posvel, nullptr, 0, act, fdOut, iters, stream);
+    runActions<true>(M, F, n, posvel, nullptr, 0, act, ang, freq, fdOut, iters, stream);
 }
 
 // ------------------------------------------------------------------------------------------

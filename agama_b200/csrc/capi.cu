@@ -331,13 +331,45 @@ extern "C" void agama_deleteActionFinder(agama_ActionFinder* a)
     delete a;
 }
 
+extern "C" int agama_evalActionsAnglesFrequenciesManyDevice(const agama_ActionFinder* a, long n,
+    const double* posvel, double* act, double* ang, double* freq, void* stream)
+{
+    return guarded([&] {
+        if(!a || n < 0 || (n > 0 && (!posvel || !(act || ang || freq))))
+            throw std::invalid_argument("evalActionsAnglesFrequenciesManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        launchActionsFinder(a->af->pot->view, a->af->view, n, posvel, act, ang, freq, nullptr, nullptr,
+            static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int agama_evalActionsAnglesFrequenciesMany(const agama_ActionFinder* a, long n,
+    const double* posvel, double* act, double* ang, double* freq)
+{
+    return guarded([&] {
+        if(!a || n < 0 || (n > 0 && (!posvel || !(act || ang || freq))))
+            throw std::invalid_argument("evalActionsAnglesFrequenciesMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        const DeviceActionFinder& F = *a->af;
+        runChunked(n, { { posvel, 6 * sizeof(double) } },
+            { { act, 3 * sizeof(double) }, { ang, 3 * sizeof(double) }, { freq, 3 * sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchActionsFinder(F.pot->view, F.view, count, static_cast<const double*>(in[0]),
+                    static_cast<double*>(out[0]), static_cast<double*>(out[1]), static_cast<double*>(out[2]),
+                    nullptr, nullptr, s);
+            });
+    });
+}
+
 extern "C" int agama_evalActionsManyDevice(const agama_ActionFinder* a, long n, const double* posvel,
     double* act, double* fdOut, void* stream)
 {
     return guarded([&] {
         if(!a || n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsManyDevice: invalid arguments");
         AGB_CUDA(cudaSetDevice(a->af->pot->device));
-        launchActionsFinder(a->af->pot->view, a->af->view, n, posvel, act, fdOut, nullptr, static_cast<cudaStream_t>(stream));
+        launchActionsFinder(a->af->pot->view, a->af->view, n, posvel, act, nullptr, nullptr, fdOut, nullptr,
+            static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -352,7 +384,40 @@ extern "C" int agama_evalActionsMany(const agama_ActionFinder* a, long n, const 
         runChunked(n, { { posvel, 6 * sizeof(double) } }, { { act, 3 * sizeof(double) }, { fdOut, sizeof(double) } },
             [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
                 launchActionsFinder(F.pot->view, F.view, count, static_cast<const double*>(in[0]),
-                    static_cast<double*>(out[0]), static_cast<double*>(out[1]), nullptr, s);
+                    static_cast<double*>(out[0]), nullptr, nullptr, static_cast<double*>(out[1]), nullptr, s);
+            });
+    });
+}
+
+extern "C" int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential* p, long n,
+    const double* posvel, const double* fd, double fd0, double* act, double* ang, double* freq, void* stream)
+{
+    return guarded([&] {
+        requireAxisymmetric(p);
+        if(n < 0 || (n > 0 && (!posvel || !(act || ang || freq))))
+            throw std::invalid_argument("evalActionsAnglesFrequenciesStandaloneManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        launchActionsFixedDelta(p->pot->view, n, posvel, fd, fd0, act, ang, freq, nullptr,
+            static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int agama_evalActionsAnglesFrequenciesStandaloneMany(const agama_Potential* p, long n,
+    const double* posvel, const double* fd, double fd0, double* act, double* ang, double* freq)
+{
+    return guarded([&] {
+        requireAxisymmetric(p);
+        if(n < 0 || (n > 0 && (!posvel || !(act || ang || freq))))
+            throw std::invalid_argument("evalActionsAnglesFrequenciesStandaloneMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const MultipoleView& M = p->pot->view;
+        runChunked(n, { { posvel, 6 * sizeof(double) }, { fd, sizeof(double) } },
+            { { act, 3 * sizeof(double) }, { ang, 3 * sizeof(double) }, { freq, 3 * sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchActionsFixedDelta(M, count, static_cast<const double*>(in[0]), static_cast<const double*>(in[1]),
+                    fd0, static_cast<double*>(out[0]), static_cast<double*>(out[1]), static_cast<double*>(out[2]),
+                    nullptr, s);
             });
     });
 }
@@ -364,7 +429,8 @@ extern "C" int agama_evalActionsStandaloneManyDevice(const agama_Potential* p, l
         requireAxisymmetric(p);
         if(n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsStandaloneManyDevice: invalid arguments");
         AGB_CUDA(cudaSetDevice(p->pot->device));
-        launchActionsFixedDelta(p->pot->view, n, posvel, fd, fd0, act, rootIters, static_cast<cudaStream_t>(stream));
+        launchActionsFixedDelta(p->pot->view, n, posvel, fd, fd0, act, nullptr, nullptr, rootIters,
+            static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -380,29 +446,40 @@ extern "C" int agama_evalActionsStandaloneMany(const agama_Potential* p, long n,
         runChunked(n, { { posvel, 6 * sizeof(double) }, { fd, sizeof(double) } }, { { act, 3 * sizeof(double) } },
             [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
                 launchActionsFixedDelta(M, count, static_cast<const double*>(in[0]), static_cast<const double*>(in[1]),
-                    fd0, static_cast<double*>(out[0]), nullptr, s);
+                    fd0, static_cast<double*>(out[0]), nullptr, nullptr, nullptr, s);
             });
     });
 }
 
+namespace {
+/// the single-point outputs of the reference's C interface: NaN everywhere when the call failed
+void storeSinglePoint(int rc, const double* act, const double* ang, const double* freq,
+    double actions[3], double angles[3], double frequencies[3])
+{
+    for(int k = 0; k < 3; k++) {
+        if(actions) actions[k] = rc == 0 ? act[k] : NAN;
+        if(angles) angles[k] = rc == 0 ? ang[k] : NAN;
+        if(frequencies) frequencies[k] = rc == 0 ? freq[k] : NAN;
+    }
+}
+}  // namespace
+
 extern "C" void agama_evalActionsAnglesFrequencies(const agama_ActionFinder* a, const double posvel[6],
     double actions[3], double angles[3], double frequencies[3])
 {
-    double act[3] = { NAN, NAN, NAN };
-    if(agama_evalActionsMany(a, 1, posvel, act, nullptr) != 0) act[0] = act[1] = act[2] = NAN;
-    if(actions) for(int k = 0; k < 3; k++) actions[k] = act[k];
-    if(angles) { angles[0] = angles[1] = angles[2] = NAN; setError("angles are not provided by this engine yet"); }
-    if(frequencies) { frequencies[0] = frequencies[1] = frequencies[2] = NAN; setError("frequencies are not provided by this engine yet"); }
+    double act[3], ang[3], freq[3];
+    const int rc = agama_evalActionsAnglesFrequenciesMany(a, 1, posvel, act, angles ? ang : nullptr,
+        frequencies ? freq : nullptr);
+    storeSinglePoint(rc, act, ang, freq, actions, angles, frequencies);
 }
 
 extern "C" void agama_evalActionsAnglesFrequenciesStandalone(const agama_Potential* p, double fd,
     const double posvel[6], double actions[3], double angles[3], double frequencies[3])
 {
-    double act[3] = { NAN, NAN, NAN };
-    if(agama_evalActionsStandaloneMany(p, 1, posvel, nullptr, fd, act) != 0) act[0] = act[1] = act[2] = NAN;
-    if(actions) for(int k = 0; k < 3; k++) actions[k] = act[k];
-    if(angles) { angles[0] = angles[1] = angles[2] = NAN; setError("angles are not provided by this engine yet"); }
-    if(frequencies) { frequencies[0] = frequencies[1] = frequencies[2] = NAN; setError("frequencies are not provided by this engine yet"); }
+    double act[3], ang[3], freq[3];
+    const int rc = agama_evalActionsAnglesFrequenciesStandaloneMany(p, 1, posvel, nullptr, fd, act,
+        angles ? ang : nullptr, frequencies ? freq : nullptr);
+    storeSinglePoint(rc, act, ang, freq, actions, angles, frequencies);
 }
 
 // ------------------------------------------------------------------------------------------

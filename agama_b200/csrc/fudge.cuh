@@ -161,8 +161,13 @@ struct __align__(16) FudgeRecord {
     double lambdaLower, lambdaPos;          // lambda_min root in [lambdaLower, lambdaPos];
                                             // lambda_max root in [lambdaPos, inf)
     int roots;                              // ROOT_* bits of the roots still to be found
-    int valid;                              // 0: the point has no integrals to do
+    int valid;                              // 0: the point has no integrals to do; otherwise
+                                            // REC_VALID | the REC_* direction-of-motion bits
 };
+
+/// bits of FudgeRecord::valid: the point has integrals to do, and the signs of its motion in
+/// prolate spheroidal coordinates that the angles need (lambdadot >= 0, nudot * nu >= 0, nudot < 0)
+enum { REC_VALID = 1, REC_LDOT_POS = 2, REC_NDOT_NU_POS = 4, REC_NUDOT_NEG = 8 };
 static_assert(sizeof(FudgeRecord) == 128, "FudgeRecord is one 128-byte line");
 
 enum { ROOT_NU_MAX = 1, ROOT_LAMBDA_MIN = 2, ROOT_LAMBDA_MAX = 4 };
@@ -333,7 +338,177 @@ static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, do
     rec.lambda = fnc.lambda; rec.nu = fnc.nu; rec.D2 = D2; rec.E = fnc.E; rec.Lz = Lz; rec.I3 = fnc.I3;
     rec.flambda = fnc.flambda; rec.fnu = fnc.fnu; rec.phi = phi;
     fudgeLimitsSetup(fnc, rec);
-    rec.valid = 1;
+    // velocities in prolate spheroidal coordinates (src/coord.cpp:317-322, :525-531)
+    const double lambdadot = R * 2 * lambda / sqD * vR + z * 2 * lmd / sqD * vz;
+    const double nudot = R * 2 * -absnu / sqD * signz * vR + z * 2 * dmn / sqD * signz * vz;
+    rec.valid = REC_VALID | (lambdadot >= 0 ? REC_LDOT_POS : 0) | (nudot * fnc.nu >= 0 ? REC_NDOT_NU_POS : 0) |
+        (nudot < 0 ? REC_NUDOT_NEG : 0);
+}
+
+/** Inverse of the cubic end-point scaling (math::scale of ScalingCub, src/math_core.cpp:370-386):
+    s in [0, 1] with u = ul (1-s)^2 (1+2s) + ur s^2 (3-2s).  On the nearer half, w = s^2 (3 - 2s) is
+    a depressed cubic in y = s - 1/2 whose trigonometric root s = 1/2 + cos((acos(1 - 2w) - 2pi)/3)
+    is polished by three Newton steps; u outside [ul, ur] gives NaN, as in the reference. */
+static __device__ double scaleCubInverse(double ul, double ur, double u)
+{
+    if(u == ul) return 0;
+    if(u == ur) return 1;
+    const double half = 0.5 * (ul + ur);
+    if(u == half) return 0.5;
+    const double w = u < half ? (u - ul) / (ur - ul) : (ur - u) / (ur - ul);
+    double s = 0.5 + cos((acos(1 - 2 * w) - 2 * M_PI) / 3);
+    for(int i = 0; i < 3; i++)
+        s -= (s * s * (3 - 2 * s) - w) / (6 * s * (1 - s));
+    return u < half ? s : 1 - s;
+}
+
+/// the three integrands of AxisymIntegrand::value with p in the denominator (n = -1), from one
+/// F(tau): (tau-Delta^2)^-1 [E], (tau-Delta^2)^-1 tau^-1 [I3], (tau-Delta^2)^-2 with the singular
+/// part at nu_max removed [Lz] (src/actions_staeckel.cpp:276-299)
+struct InverseMomentumTerms { double e, i3, lz; };
+
+static __device__ InverseMomentumTerms inverseMomentumTerms(double ft, double tau, double D2, double nuMax,
+    double dfdnuMax)
+{
+    InverseMomentumTerms t{ 0, 0, 0 };
+    const double tmd = tau - D2;
+    const double p2 = ft / (2 * pow2(tmd) * tau);
+    if(p2 < 0) return t;
+    const double r = 1 / sqrt(p2);
+    double v = r / tmd;
+    t.e = isFinite(v) ? v : 0;
+    v = r / tmd / tau;
+    t.i3 = isFinite(v) ? v : 0;
+    v = r / pow2(tmd);
+    if(tmd < 0) v += sqrt(2 * nuMax / dfdnuMax / (tau - nuMax)) / tmd;
+    t.lz = isFinite(v) ? v : 0;
+    return t;
+}
+
+/// GL rule of the requested order (the next tabulated one at or above it)
+static __device__ __forceinline__ int glRule(const GLRules& gl, int order, const double** x, const double** w)
+{
+    int N = order < 1 ? 1 : order;
+    while(gl.offset[N] < 0) N++;
+    *x = gl.nodes + gl.offset[N];
+    *w = gl.weights + gl.offset[N];
+    return N;
+}
+
+/** the inverse-momentum integrals of one branch over the scaled interval [0, y] of [lo, hi]
+    (integrateGL(ScaledIntegrand<ScalingCub>, 0, y, N), src/math_core.cpp:1191-1205); with
+    ACT also the action integral (p in the numerator) over the same nodes, when y = 1 */
+template<bool ACT>
+static __device__ InverseMomentumTerms branchIntegrals(const FudgeFunction& fnc, const GLRules& gl, int order,
+    double lo, double hi, double y, double nuMax, double dfdnuMax, double* act)
+{
+    InverseMomentumTerms sum{ 0, 0, 0 };
+    if(ACT) *act = 0;
+    if(y == 0) return sum;
+    const double *x, *w;
+    const int N = glRule(gl, order, &x, &w);
+    double sa = 0;
+    for(int i = 0; i < N; i++) {
+        const double xi = ldg(x + i), wi = ldg(w + i);
+        double duds;
+        const double tau = unscaleCub(lo, hi, y * xi + 0 * (1 - xi), &duds);
+        const double ft = fnc.value(tau);
+        const InverseMomentumTerms t = inverseMomentumTerms(ft, tau, fnc.D2, nuMax, dfdnuMax);
+        sum.e += wi * (t.e * duds);
+        sum.i3 += wi * (t.i3 * duds);
+        sum.lz += wi * (t.lz * duds);
+        if(ACT) {
+            const double tmd = tau - fnc.D2;
+            const double p2 = ft / (2 * pow2(tmd) * tau);
+            double v = p2 < 0 ? 0 : sqrt(p2);
+            if(!isFinite(v)) v = 0;
+            sa += wi * (v * duds);
+        }
+    }
+    sum.e *= y; sum.i3 *= y; sum.lz *= y;
+    if(ACT) *act = sa * y;
+    return sum;
+}
+
+/// 2 pi wrap of an angle into [0, 2 pi) (math::wrapAngle, src/math_core.cpp:149-157; NaN -> 0)
+static __device__ __forceinline__ double wrapAngle(double x)
+{
+    x -= 2 * M_PI * floor(1 / (2 * M_PI) * x);
+    return x >= 0 && x < 2 * M_PI ? x : 0;
+}
+
+/** Actions, frequencies and angles of a prepared point whose roots are found (evalAxisym,
+    src/actions_staeckel.cpp:645-670): computeActions (:604-619), computeActionDerivatives
+    (:489-527), computeIntDerivatives (:532-560), computeGenFuncDerivatives (:566-600) and
+    computeAngles (:624-636).  The action integrals and the derivative integrals share their
+    potential evaluations (same nodes); ang / freq may be null. */
+static __device__ void fudgeAnglesFrequencies(const MultipoleView& M, const GLRules& gl, const FudgeRecord& rec,
+    double* act, double* ang, double* freq)
+{
+    FudgeFunction fnc;
+    loadFudgeFunction(M, rec, fnc);
+    const FudgeLimits lim = fudgeLimitsFinish(rec);
+    const double D2 = rec.D2, Lz = rec.Lz;
+    double dfdnuMax, unused;
+    fnc.eval<true, false>(lim.nu_max, &unused, &dfdnuMax, nullptr);
+    // action derivatives over (E, I3, Lz), full ranges; the actions from the same nodes
+    double Jr, Jz;
+    InverseMomentumTerms L = branchIntegrals<true>(fnc, gl, lim.order, lim.lambda_min, lim.lambda_max, 1,
+        lim.nu_max, dfdnuMax, &Jr);
+    const InverseMomentumTerms N = branchIntegrals<true>(fnc, gl, lim.order, 0, lim.nu_max, 1,
+        lim.nu_max, dfdnuMax, &Jz);
+    act[0] = Jr / M_PI;
+    act[1] = Jz / M_PI * 2;
+    if(lim.lambda_min == lim.lambda_max) {      // limitingIntegralValue, :307-323
+        const double tau = lim.lambda_min, tmd = tau - D2;
+        double d2, v0;
+        fnc.eval<false, true>(tau, &v0, nullptr, &d2);
+        const double base = 2 * M_PI * sqrt(-tau / d2) * fabs(tmd);
+        L.e = base / tmd;
+        L.i3 = base / tmd / tau;
+        L.lz = base / pow2(tmd);
+    }
+    const double dJrdE = L.e / (4 * M_PI), dJzdE = N.e / (2 * M_PI);
+    const double dJrdI3 = -L.i3 / (4 * M_PI), dJzdI3 = -N.i3 / (2 * M_PI);
+    const double dJrdLz = -Lz * L.lz / (4 * M_PI);
+    const double dmn = D2 - lim.nu_max;
+    const double singpart = 2 * sqrt(-2 * lim.nu_max / dfdnuMax / dmn) * atan(sqrt(lim.nu_max / dmn));
+    const double dJzdLz = -Lz * (N.lz + singpart) / (2 * M_PI);
+    // inverse matrix: frequencies and the derivatives of I3 over the actions
+    double Or, Oz, Ophi, dI3dJr, dI3dJz, dI3dJphi;
+    const double det = dJrdE * dJzdI3 - dJrdI3 * dJzdE;
+    if(lim.nu_max == 0 || det == 0) {
+        Or = 1 / dJrdE;
+        Ophi = -dJrdLz / dJrdE;
+        dI3dJr = dI3dJz = dI3dJphi = Oz = 0;
+    } else {
+        Or = dJzdI3 / det;
+        Oz = -dJrdI3 / det;
+        Ophi = (dJrdI3 * dJzdLz - dJrdLz * dJzdI3) / det;
+        dI3dJr = -dJzdE / det;
+        dI3dJz = dJrdE / det;
+        dI3dJphi = -(dJrdE * dJzdLz - dJrdLz * dJzdE) / det;
+    }
+    if(freq) { freq[0] = Or; freq[1] = Oz; freq[2] = Ophi; }
+    if(!ang) return;
+    // derivatives of the generating function over (E, I3, Lz): integrals up to the point
+    const double signl = rec.valid & REC_LDOT_POS ? 1 : -1, signn = rec.valid & REC_NDOT_NU_POS ? 1 : -1;
+    const double absnu = fabs(rec.nu);
+    const double yl = scaleCubInverse(lim.lambda_min, lim.lambda_max, rec.lambda);
+    const double yn = lim.nu_max == 0 ? 0 : scaleCubInverse(0, lim.nu_max, absnu);
+    const InverseMomentumTerms Lp = branchIntegrals<false>(fnc, gl, lim.order, lim.lambda_min, lim.lambda_max, yl,
+        lim.nu_max, dfdnuMax, nullptr);
+    const InverseMomentumTerms Np = branchIntegrals<false>(fnc, gl, lim.order, 0, lim.nu_max, yn,
+        lim.nu_max, dfdnuMax, nullptr);
+    const double dSdE = signl * Lp.e / 4 + signn * Np.e / 4;
+    const double dSdI3 = signl * -Lp.i3 / 4 + signn * -Np.i3 / 4;
+    const double singS = 2 * sqrt(-2 * lim.nu_max / dfdnuMax / dmn) *
+        (atan(sqrt(lim.nu_max / dmn)) - atan(sqrt((lim.nu_max - absnu) / dmn)));
+    const double dSdLz = Lz == 0 ? 0 : rec.phi + signl * -Lz * Lp.lz / 4 + signn * -Lz * (Np.lz + singS) / 4;
+    const bool addPi = (rec.valid & REC_NUDOT_NEG) && Lz != 0;
+    ang[0] = wrapAngle(dSdE * Or + dSdI3 * dI3dJr + dSdLz * 0);
+    ang[1] = wrapAngle(dSdE * Oz + dSdI3 * dI3dJz + dSdLz * 0 + M_PI * addPi);
+    ang[2] = wrapAngle(dSdE * Ophi + dSdI3 * dI3dJphi + dSdLz * 1);
 }
 
 /// Cartesian posvel -> cylindrical (R, z, phi, vR, vz, vphi); reference src/coord.cpp:476-484

@@ -19,4 +19,10 @@ void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* ite
 void launchFudgeIntegrals(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,
     unsigned long long* counter, cudaStream_t stream);
 
+/// phase 3 with angles / frequencies: actions into act (n x 3, Jphi already there), frequencies
+/// (Omega_r, Omega_z, Omega_phi) and angles (theta_r, theta_z, theta_phi) into freq / ang when
+/// not null; one point per thread
+void launchFudgeAngles(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,
+    double* ang, double* freq, cudaStream_t stream);
+
 }  // namespace agb

@@ -81,11 +81,12 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
 void launchOrbitsNoAlloc(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     double* out, long* nsteps, long* nrej, int* status, int slot, cudaStream_t stream);
 int noallocQueueSlots();
-/// Staeckel fudge with a given focal distance per point (fd) or one for all (fd0 when fd is null)
+/// Staeckel fudge with a given focal distance per point (fd) or one for all (fd0 when fd is null);
+/// outputs n x 3 each: actions (Jr, Jz, Jphi), angles and frequencies (any of them may be null)
 void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
-    double* act, int* iters, cudaStream_t stream);
+    double* act, double* ang, double* freq, int* iters, cudaStream_t stream);
 /// Staeckel fudge with the focal distance from the action finder's table
 void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
-    double* act, double* fdOut, int* iters, cudaStream_t stream);
+    double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream);
 
 }  // namespace agb

@@ -130,14 +130,14 @@ int agama_getActionFinderTables(const agama_ActionFinder* actionFinder, double* 
 void agama_deleteActionFinder(agama_ActionFinder* actionFinder);
 
 /* reference: agama_evalActionsAnglesFrequencies, src/interface_c.h:135 (src/interface_c.cpp:129-155):
-   actions of one point through the action finder; angles / frequencies are not computed by
-   this engine (they come back NaN with a message in agama_getError()). */
+   actions, angles and frequencies of one point through the action finder (any output pointer
+   may be NULL); NaN in every output when the call fails, with the message in agama_getError(). */
 void agama_evalActionsAnglesFrequencies(const agama_ActionFinder* actionFinder, const double posvel[6],
     double actions[3], double angles[3], double frequencies[3]);
 
 /* reference: agama_evalActionsAnglesFrequenciesStandalone, src/interface_c.h:155
-   (src/interface_c.cpp:157-192): actions of one point for a given focal distance fd
-   (actions::evalAxisymFudge, src/actions_staeckel.cpp:683-693). */
+   (src/interface_c.cpp:157-192): actions, angles and frequencies of one point for a given focal
+   distance fd (actions::evalAxisymFudge, src/actions_staeckel.cpp:683-693). */
 void agama_evalActionsAnglesFrequenciesStandalone(const agama_Potential* potential, double fd,
     const double posvel[6], double actions[3], double angles[3], double frequencies[3]);
 
@@ -172,6 +172,27 @@ int agama_evalActionsStandaloneMany(const agama_Potential* potential, long n, co
    iterations spent on each point. */
 int agama_evalActionsStandaloneManyDevice(const agama_Potential* potential, long n, const double* posvel,
     const double* fd, double fd0, double* act, int* rootIters, void* stream);
+
+/* Batched actions, angles (theta_r, theta_z, theta_phi) and frequencies (Omega_r, Omega_z,
+   Omega_phi) through the action finder, host buffers of n x 3 each; any of act / ang / freq may
+   be NULL (not all three).  Replaces n calls of agama_evalActionsAnglesFrequencies
+   (actions::evalAxisym, src/actions_staeckel.cpp:645-670, batched as by the reference's Python
+   ActionFinder with angles / frequencies, src/interface_python.cpp:3761-3822). */
+int agama_evalActionsAnglesFrequenciesMany(const agama_ActionFinder* actionFinder, long n,
+    const double* posvel, double* act, double* ang, double* freq);
+
+/* The same on device buffers. */
+int agama_evalActionsAnglesFrequenciesManyDevice(const agama_ActionFinder* actionFinder, long n,
+    const double* posvel, double* act, double* ang, double* freq, void* stream);
+
+/* Batched actions, angles and frequencies for given focal distances fd[n] (or fd0 for all
+   points when fd is NULL); replaces n calls of agama_evalActionsAnglesFrequenciesStandalone. */
+int agama_evalActionsAnglesFrequenciesStandaloneMany(const agama_Potential* potential, long n,
+    const double* posvel, const double* fd, double fd0, double* act, double* ang, double* freq);
+
+/* The same on device buffers. */
+int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential* potential, long n,
+    const double* posvel, const double* fd, double fd0, double* act, double* ang, double* freq, void* stream);
 
 /* ---------------------------------------------------------------------------------------
    Measurement helper (no reference counterpart): FP64 fused-multiply-add throughput of the

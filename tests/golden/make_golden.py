@@ -184,9 +184,10 @@ def make_action_vectors():
         act_af, fd = af.actions(pts, with_fd=True)
         evals_per_point = af.evalcount(reset=True) / len(pts)
         act_fd, counts = pot.actions_fd(pts, fd, count=True)
+        _, ang_fd, freq_fd = pot.actions_angles_fd(pts, fd)
         tab = af.tables()
         np.savez_compressed(os.path.join(HERE, "actions_%s.npz" % name), points=pts, fd=fd,
-                            act_finder=act_af, act_fd=act_fd, evals_fd=counts,
+                            act_finder=act_af, act_fd=act_fd, evals_fd=counts, ang_fd=ang_fd, freq_fd=freq_fd,
                             evals_per_point_finder=evals_per_point, **{"tab_" + k: v for k, v in tab.items()})
         print(name, "actions", len(pts), "evals/point %.1f" % evals_per_point,
               "table", tab["delta"].shape, "LofE", tab["lofe"].shape)
