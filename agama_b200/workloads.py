@@ -85,3 +85,63 @@ def vcirc_from_force(force_fn):
         pts = np.column_stack([R, np.zeros_like(R), np.zeros_like(R)])
         return np.sqrt(-R * force_fn(pts)[:, 0])
     return vc
+
+
+def equatorial_average(fn, R, nphi=16):
+    """azimuthal average over nphi angles in the equatorial plane of fn(points) -> (n, k) or (n,):
+    the m = 0 part exactly for harmonics m < nphi (the "axisymmetrized" potential of the
+    reference's R_circ / v_circ, src/potential_utils.cpp:608-619)"""
+    phi = (np.arange(nphi) + 0.5) * (2 * np.pi / nphi)
+    c, s = np.cos(phi), np.sin(phi)
+    pts = np.stack([R[:, None] * c, R[:, None] * s, np.zeros((len(R), nphi))], axis=-1).reshape(-1, 3)
+    v = np.asarray(fn(pts))
+    if v.ndim == 2:   # radial component of a vector field
+        v = (v.reshape(len(R), nphi, 3)[:, :, :2] * np.stack([c, s], axis=-1)[None]).sum(-1)
+        return v.mean(axis=1)
+    return v.reshape(len(R), nphi).mean(axis=1)
+
+
+def tcirc(potential_fn, force_fn, E, nphi=16, iters=80):
+    """T_circ(E) = 2 pi R_circ / v_circ(R_circ) of the axisymmetrized potential, R_circ from
+    Phi(R) + R dPhi/dR / 2 = E by bisection in ln R (the definition of T_circ,
+    src/potential_utils.h:83-87); NaN for E outside the range of circular-orbit energies"""
+    E = np.asarray(E, dtype=np.float64)
+    lo, hi = np.full(E.shape, np.log(1e-8)), np.full(E.shape, np.log(1e8))
+    for _ in range(iters):
+        mid = 0.5 * (lo + hi)
+        R = np.exp(mid)
+        Ec = equatorial_average(potential_fn, R, nphi) - 0.5 * R * equatorial_average(force_fn, R, nphi)
+        below = Ec < E
+        lo = np.where(below, mid, lo)
+        hi = np.where(below, hi, mid)
+    R = np.exp(0.5 * (lo + hi))
+    vc = np.sqrt(-R * equatorial_average(force_fn, R, nphi))
+    return 2 * np.pi * R / vc
+
+
+def orbit_workload(cfg, potential_fn, force_fn, n=None):
+    """initial conditions and integration times of the orbit configurations:
+    1: 1e4 orbits from the config-1 points, T = 10 T_circ(E);
+    3: 1e5 orbits, T = T_circ(E) 10^U[1, 3] (10-1000 dynamical times), Omega = 0.05;
+    5: 1e6 orbits, T = 100 T_circ(E)"""
+    if cfg == 1:
+        n = n or 10000
+        pos = dehnen_positions(n, 1.0, q=(0.8, 0.6), seed=SEEDS["points1"])
+        ic = orbit_ics(pos, potential_fn, seed=SEEDS["orbits1"])
+        scale = np.full(n, 10.0)
+    elif cfg == 3:
+        n = n or 100000
+        pos = dehnen_positions(n, 0.5, q=(0.7, 0.5), seed=SEEDS["orbits3"])
+        ic = orbit_ics(pos, potential_fn, seed=SEEDS["orbits3"] + 100)
+        rng = np.random.Generator(np.random.PCG64(SEEDS["orbits3"] + 200))
+        scale = 10 ** rng.uniform(1, 3, size=n)
+    elif cfg == 5:
+        n = n or 1000000
+        pos = dehnen_positions(n, 1.0, q=(1.0, 0.6), seed=SEEDS["orbits5"])
+        ic = orbit_ics(pos, potential_fn, seed=SEEDS["orbits5"] + 100)
+        scale = np.full(n, 100.0)
+    else:
+        raise ValueError("no orbit workload for config %d" % cfg)
+    E = potential_fn(ic[:, :3]) + 0.5 * np.sum(ic[:, 3:] ** 2, axis=1)
+    T = scale * tcirc(potential_fn, force_fn, E)
+    return ic, T
