@@ -26,170 +26,235 @@ struct StageStore {
     __device__ double& at(int v, int c) const { return base[(v * 6 + c) * stride]; }
 };
 
-/// integrate one orbit; writes the final point (rotating frame), counters and status
-template<int KIND>
-__device__ void integrateOrbit(const MultipoleView& M, const OrbitParams& P, const double* ic,
-    double tEnd, const StageStore& S, double* out, long* nAccepted, long* nRejected, int* status)
+/// The Runge-Kutta stages of one DOP853 attempt as table rows: row r forms the point of stage
+/// r+2 (k_{r+2}) as x + h sum coef * k_src, row 11 the 8th-order solution (weights b).  Sources:
+/// -1 = k1 (registers), otherwise a stage slot; results go to slot dest[r].  Terms and their order
+/// are those of OdeStepperDOP853::doStep (src/math_ode.cpp:243-300); unused terms have coef 0.
+constexpr int NUM_ROWS = 12, MAX_TERMS = 9, K1 = -1;
+struct StageTable {
+    double coef[NUM_ROWS][MAX_TERMS];
+    double c[NUM_ROWS];
+    signed char src[NUM_ROWS][MAX_TERMS];
+    signed char dest[NUM_ROWS];
+};
+
+__host__ __device__ constexpr StageTable makeStageTable()
 {
     using namespace dp853;
-    const double Om = P.Omega;
-    double x[6], k1[6], xt[6], k13[6];
-    for(int c = 0; c < 6; c++) x[c] = ic[c];
-    double t = 0;
-    long steps = 0, rejects = 0;
-    int st = ORBIT_OK;
-    // --- init: derivatives at the start and the initial step (OdeStepperDOP853::init)
-    double accFac = 1;
-    orbitRHS<3, KIND>(M, Om, t, x, k1, &accFac);
-    double hNext;
-    {
-        // initTimeStep (src/math_ode.cpp:35-91): Euler + Heun probes, Aarseth-like estimate
-        double nx = 0, nd = 0;
-        for(int c = 0; c < 6; c++) { nx += x[c] * x[c]; nd += k1[c] * k1[c]; }
-        const double h1 = fmax(HMIN, fmin(HMAX, sqrt(nx / nd) * 0.01));
-        double k2[6], k3[6];
-        for(int c = 0; c < 6; c++) xt[c] = x[c] + h1 * k1[c];
-        orbitRHS<3, KIND>(M, Om, t + h1, xt, k2, nullptr);
-        for(int c = 0; c < 6; c++) xt[c] = x[c] + 0.5 * h1 * (k1[c] + k2[c]);
-        orbitRHS<3, KIND>(M, Om, t + h1, xt, k3, nullptr);
-        double h2 = INFINITY;
-        for(int c = 0; c < 6; c++) {
-            const double d0 = fmax(P.accAbs, fmax(fabs(x[c]), fabs(xt[c])));
-            const double d1 = fmax(fabs(k1[c]), fabs(k3[c]));
-            const double d2 = fabs((3 * k2[c] - k1[c] - 2 * k3[c]) / h1);
-            const double d3 = fabs(6 * (k3[c] - k2[c]) / (h1 * h1));
-            h2 = fmin(h2, (d0 * d2 + d1 * d1) / (d1 * d3 + d2 * d2));
+    StageTable T{};
+    const double coef[NUM_ROWS][MAX_TERMS] = {
+        { a21 },
+        { a31, a32 },
+        { a41, a43 },
+        { a51, a53, a54 },
+        { a61, a64, a65 },
+        { a71, a74, a75, a76 },
+        { a81, a84, a85, a86, a87 },
+        { a91, a94, a95, a96, a97, a98 },
+        { a101, a104, a105, a106, a107, a108, a109 },
+        { a111, a114, a115, a116, a117, a118, a119, a1110 },
+        { a121, a124, a125, a126, a127, a128, a129, a1210, a1211 },
+        { b1, b6, b7, b8, b9, b10, b11, b12 } };
+    const signed char src[NUM_ROWS][MAX_TERMS] = {
+        { K1 }, { K1, 0 }, { K1, 1 }, { K1, 1, 2 }, { K1, 2, 3 }, { K1, 2, 3, 4 }, { K1, 2, 3, 4, 5 },
+        { K1, 2, 3, 4, 5, 6 }, { K1, 2, 3, 4, 5, 6, 7 }, { K1, 2, 3, 4, 5, 6, 7, 8 },
+        { K1, 2, 3, 4, 5, 6, 7, 8, 0 }, { K1, 4, 5, 6, 7, 8, 0, 1 } };
+    const int nterms[NUM_ROWS] = { 1, 2, 2, 3, 3, 4, 5, 6, 7, 8, 9, 8 };
+    const double c[NUM_ROWS] = { c2, c3, c4, c5, c6, c7, c8, c9, c10, c11, 1, 1 };
+    const signed char dest[NUM_ROWS] = { 0, 1, 2, 3, 4, 5, 6, 7, 8, 0, 1, -1 };
+    for(int r = 0; r < NUM_ROWS; r++) {
+        for(int t = 0; t < MAX_TERMS; t++) {
+            T.coef[r][t] = t < nterms[r] ? coef[r][t] : 0;
+            T.src[r][t] = t < nterms[r] ? src[r][t] : K1;
         }
-        hNext = fmax(HMIN, fmin(HMAX, pow(P.accRel, 1. / 8) * sqrt(h2))) * accFac;
+        T.c[r] = c[r];
+        T.dest[r] = dest[r];
     }
-    double tb = 0, hLast = 0;
-    if(tEnd != 0 && isFinite(tEnd)) {
-        const double sign = tEnd >= 0 ? 1 : -1;
-        while(t != tEnd) {
-            const double remaining = tEnd - t;
-            double h = fmin(remaining * sign, hNext) * sign;
-            int nbad = 0, attempts = 0;
-            double preverr = INFINITY;
-            bool accepted = false;
-            while(!accepted) {
-                if(h == 0 || !isFinite(h) || ++attempts > MAX_ATTEMPTS_PER_STEP) { st = ORBIT_BAD_STEP; break; }
-                // ---- the twelve stages (xt = x + h * sum a_ij k_j), then k13 at the end point
-                for(int c = 0; c < 6; c++) xt[c] = x[c] + h * a21 * k1[c];
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c2 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(0, c) = k[c]; }
-                for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a31 * k1[c] + a32 * S.at(0, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c3 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(1, c) = k[c]; }
-                for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a41 * k1[c] + a43 * S.at(1, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c4 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(2, c) = k[c]; }
-                for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a51 * k1[c] + a53 * S.at(1, c) + a54 * S.at(2, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c5 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(3, c) = k[c]; }
-                for(int c = 0; c < 6; c++) xt[c] = x[c] + h * (a61 * k1[c] + a64 * S.at(2, c) + a65 * S.at(3, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c6 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(4, c) = k[c]; }
-                for(int c = 0; c < 6; c++)
-                    xt[c] = x[c] + h * (a71 * k1[c] + a74 * S.at(2, c) + a75 * S.at(3, c) + a76 * S.at(4, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c7 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(5, c) = k[c]; }
-                for(int c = 0; c < 6; c++)
-                    xt[c] = x[c] + h * (a81 * k1[c] + a84 * S.at(2, c) + a85 * S.at(3, c) + a86 * S.at(4, c) +
-                        a87 * S.at(5, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c8 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(6, c) = k[c]; }
-                for(int c = 0; c < 6; c++)
-                    xt[c] = x[c] + h * (a91 * k1[c] + a94 * S.at(2, c) + a95 * S.at(3, c) + a96 * S.at(4, c) +
-                        a97 * S.at(5, c) + a98 * S.at(6, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c9 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(7, c) = k[c]; }
-                for(int c = 0; c < 6; c++)
-                    xt[c] = x[c] + h * (a101 * k1[c] + a104 * S.at(2, c) + a105 * S.at(3, c) + a106 * S.at(4, c) +
-                        a107 * S.at(5, c) + a108 * S.at(6, c) + a109 * S.at(7, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c10 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(8, c) = k[c]; }
-                // stage 11 -> slot of k2, stage 12 -> slot of k3
-                for(int c = 0; c < 6; c++)
-                    xt[c] = x[c] + h * (a111 * k1[c] + a114 * S.at(2, c) + a115 * S.at(3, c) + a116 * S.at(4, c) +
-                        a117 * S.at(5, c) + a118 * S.at(6, c) + a119 * S.at(7, c) + a1110 * S.at(8, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + c11 * h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(0, c) = k[c]; }
-                for(int c = 0; c < 6; c++)
-                    xt[c] = x[c] + h * (a121 * k1[c] + a124 * S.at(2, c) + a125 * S.at(3, c) + a126 * S.at(4, c) +
-                        a127 * S.at(5, c) + a128 * S.at(6, c) + a129 * S.at(7, c) + a1210 * S.at(8, c) +
-                        a1211 * S.at(0, c));
-                { double k[6]; orbitRHS<3, KIND>(M, Om, t + h, xt, k, nullptr); for(int c = 0; c < 6; c++) S.at(1, c) = k[c]; }
-                double k1b[6];
-                for(int c = 0; c < 6; c++) {
-                    k1b[c] = b1 * k1[c] + b6 * S.at(4, c) + b7 * S.at(5, c) + b8 * S.at(6, c) + b9 * S.at(7, c) +
-                        b10 * S.at(8, c) + b11 * S.at(0, c) + b12 * S.at(1, c);
-                    xt[c] = x[c] + h * k1b[c];
-                }
-                double af = 1;
-                orbitRHS<3, KIND>(M, Om, t + h, xt, k13, &af);
-                // ---- error estimate (3rd and 5th order embedded solutions)
-                double err5 = 0, err3 = 0;
-                for(int c = 0; c < 6; c++) {
-                    const double sk = (P.accAbs + P.accRel * fmax(fabs(x[c]), fabs(xt[c]))) * af;
-                    if(sk == 0) continue;
-                    err3 += pow2((k1b[c] - bhh1 * k1[c] - bhh2 * S.at(7, c) - bhh3 * S.at(1, c)) / sk);
-                    err5 += pow2((er1 * k1[c] + er6 * S.at(4, c) + er7 * S.at(5, c) + er8 * S.at(6, c) +
-                        er9 * S.at(7, c) + er10 * S.at(8, c) + er11 * S.at(0, c) + er12 * S.at(1, c)) / sk);
-                }
-                const double den = sqrt(6 * (err5 + 0.01 * err3));
-                const double err = den == 0 ? 0 : err5 * fabs(h) / den;
-                if(!isFinite(err)) { st = ORBIT_NONFINITE; break; }
-                double fac = sqrt(sqrt(sqrt(err)));
-                if(err <= 1) {
-                    hNext = fabs(h) * fmin(finc, safe / fac);
-                    accepted = true;
-                } else {
-                    if(err > 0.5 * preverr) {
-                        nbad++;
-                        if(nbad >= 2) fac = 1 / fdec;
-                        if(nbad >= 4) { hNext = fabs(h); accepted = true; }
-                    } else
-                        nbad = 0;
-                    if(!accepted) {
-                        preverr = err;
-                        h *= fmax(fdec, safe / fac);
-                        rejects++;
-                    }
-                }
-            }
-            if(st != ORBIT_OK) break;
-            for(int c = 0; c < 6; c++) { x[c] = xt[c]; k1[c] = k13[c]; }
-            tb = t;
-            hLast = h;
-            t = h == remaining ? tEnd : t + h;
-            if(++steps >= P.maxSteps) { if(t != tEnd) st = ORBIT_MAX_STEPS; break; }
-        }
-    }
-    // final point in the rotating frame at time tb + hLast (RuntimeTrajectory semantics)
-    double ca = 1, sa = 0;
-    if(Om != 0) sincos(Om * (hLast + tb), &sa, &ca);
-    out[0] = x[0] * ca + x[1] * sa;
-    out[1] = x[1] * ca - x[0] * sa;
-    out[2] = x[2];
-    out[3] = x[3] * ca + x[4] * sa;
-    out[4] = x[4] * ca - x[3] * sa;
-    out[5] = x[5];
-    *nAccepted = steps;
-    *nRejected = rejects;
-    *status = st;
+    return T;
 }
+__constant__ StageTable STAGE_TABLE = makeStageTable();
 
-/// one orbit per thread (queue == nullptr) or a persistent grid draining a work queue
+/// phases of the per-lane integration state machine
+enum { PH_FETCH, PH_INIT1, PH_INIT2, PH_INIT3, PH_STAGE, PH_FINISH };
+
+/** One orbit per lane, driven as a state machine around ONE call of the right-hand side per
+    loop iteration: lanes of a warp at different stages, attempts, orbits or in the initial-step
+    estimate all meet at that call, instead of serialising at twelve separate call sites.  The
+    step algorithm (OdeStepperDOP853::initTimeStep / doStep and the run loop of
+    BaseOrbitIntegrator::run, src/math_ode.cpp:35-406, src/orbit.cpp:52-84) is unchanged:
+    initial step from Euler and Heun probes, error norm err5 |h| / sqrt(6 (err5 + 0.01 err3))
+    weighted by (accAbs + accRel max|x|) accFac, accept at err <= 1, step factor
+    min(finc, safe / err^(1/8)), rejection with the nbad counter; the final point is rotated
+    to the frame of the potential at time tb + hLast (RuntimeTrajectory semantics).
+    queue != nullptr: lanes take orbits from the work counter until it passes n; otherwise lane
+    i integrates orbit i only. */
 template<int KIND>
 __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constant__ MultipoleView M, const OrbitParams P,
     long n, const double* __restrict__ ic, const double* __restrict__ T, double* __restrict__ out,
     long* __restrict__ nsteps, long* __restrict__ nrej, int* __restrict__ status,
     unsigned long long* queue)
 {
+    using namespace dp853;
     extern __shared__ double smem[];
+    __shared__ StageTable tab;
+    for(int k = threadIdx.x; k < static_cast<int>(sizeof(StageTable) / sizeof(double)); k += blockDim.x)
+        reinterpret_cast<double*>(&tab)[k] = reinterpret_cast<const double*>(&STAGE_TABLE)[k];
+    __syncthreads();
     const StageStore S{ smem + threadIdx.x, static_cast<int>(blockDim.x) };
-    long i = queue ? static_cast<long>(atomicAdd(queue, 1ull)) : blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
-    while(i < n) {
-        double o[6];
-        long na, nr;
-        int s;
-        integrateOrbit<KIND>(M, P, ic + 6 * i, T[i], S, o, &na, &nr, &s);
-        for(int c = 0; c < 6; c++) out[6 * i + c] = o[c];
-        if(nsteps) nsteps[i] = na;
-        if(nrej) nrej[i] = nr;
-        if(status) status[i] = s;
-        if(!queue) break;
-        i = static_cast<long>(atomicAdd(queue, 1ull));
+    const double Om = P.Omega;
+
+    long i = queue ? -1 : blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    if(!queue && i >= n) return;
+    int phase = queue ? PH_FETCH : PH_INIT1;
+    double x[6], k1[6], xt[6], k1b[6];
+    double t = 0, tEnd = 0, sign = 1, h = 0, h1 = 0, hNext = 0, accFac = 1, preverr = INFINITY, tb = 0, hLast = 0,
+        remaining = 0;
+    long steps = 0, rejects = 0;
+    int st = ORBIT_OK, row = 0, nbad = 0, attempts = 0;
+
+    // begin an attempt with the current h (zero, non-finite or endlessly rejected: give up)
+    auto startAttempt = [&]() {
+        if(h == 0 || !isFinite(h) || ++attempts > MAX_ATTEMPTS_PER_STEP) { st = ORBIT_BAD_STEP; phase = PH_FINISH; return; }
+        row = 0;
+        phase = PH_STAGE;
+    };
+    // begin the next step, or finish the orbit when the end time is reached
+    auto startStep = [&]() {
+        if(t == tEnd) { phase = PH_FINISH; return; }
+        remaining = tEnd - t;
+        h = fmin(remaining * sign, hNext) * sign;
+        nbad = 0; attempts = 0; preverr = INFINITY;
+        startAttempt();
+    };
+
+    while(true) {
+        if(phase == PH_FETCH) {
+            i = static_cast<long>(atomicAdd(queue, 1ull));
+            if(i >= n) break;
+            phase = PH_INIT1;
+        }
+        if(phase == PH_INIT1) {          // a new orbit: load its start
+            for(int c = 0; c < 6; c++) x[c] = ic[6 * i + c];
+            tEnd = T[i];
+            t = 0; tb = 0; hLast = 0; steps = 0; rejects = 0; st = ORBIT_OK; accFac = 1;
+            sign = tEnd >= 0 ? 1 : -1;
+        }
+        if(phase == PH_FINISH) {
+            double ca = 1, sa = 0;
+            if(Om != 0) sincos(Om * (hLast + tb), &sa, &ca);
+            out[6 * i + 0] = x[0] * ca + x[1] * sa;
+            out[6 * i + 1] = x[1] * ca - x[0] * sa;
+            out[6 * i + 2] = x[2];
+            out[6 * i + 3] = x[3] * ca + x[4] * sa;
+            out[6 * i + 4] = x[4] * ca - x[3] * sa;
+            out[6 * i + 5] = x[5];
+            if(nsteps) nsteps[i] = steps;
+            if(nrej) nrej[i] = rejects;
+            if(status) status[i] = st;
+            if(!queue) break;
+            phase = PH_FETCH;
+            continue;
+        }
+        // ---- the point at which the right-hand side is wanted
+        double tt;
+        if(phase == PH_INIT1) {
+            tt = t;
+            for(int c = 0; c < 6; c++) xt[c] = x[c];
+        } else if(phase == PH_INIT2) {
+            tt = t + h1;
+            for(int c = 0; c < 6; c++) xt[c] = x[c] + h1 * k1[c];
+        } else if(phase == PH_INIT3) {
+            tt = t + h1;
+            for(int c = 0; c < 6; c++) xt[c] = x[c] + 0.5 * h1 * (k1[c] + S.at(0, c));
+        } else {
+            tt = t + tab.c[row] * h;     // c = 1 for k12 and the 8th-order point: t + h
+            for(int c = 0; c < 6; c++) {
+                double acc = tab.coef[row][0] * k1[c];
+                for(int m = 1; m < MAX_TERMS; m++) {
+                    const int sl = tab.src[row][m];
+                    acc += tab.coef[row][m] * (sl < 0 ? k1[c] : S.at(sl, c));
+                }
+                if(row == NUM_ROWS - 1) k1b[c] = acc;
+                xt[c] = x[c] + h * acc;
+            }
+        }
+        // ---- the one evaluation site
+        const bool wantAcc = phase == PH_INIT1 || (phase == PH_STAGE && row == NUM_ROWS - 1);
+        double k[6], af = 1;
+        orbitRHS<3, KIND>(M, Om, tt, xt, k, wantAcc ? &af : nullptr);
+        // ---- use the result
+        if(phase == PH_INIT1) {
+            for(int c = 0; c < 6; c++) k1[c] = k[c];
+            accFac = af;
+            if(tEnd == 0 || !isFinite(tEnd)) { phase = PH_FINISH; continue; }
+            double nx = 0, nd = 0;
+            for(int c = 0; c < 6; c++) { nx += x[c] * x[c]; nd += k1[c] * k1[c]; }
+            h1 = fmax(HMIN, fmin(HMAX, sqrt(nx / nd) * 0.01));
+            phase = PH_INIT2;
+        } else if(phase == PH_INIT2) {
+            for(int c = 0; c < 6; c++) S.at(0, c) = k[c];
+            phase = PH_INIT3;
+        } else if(phase == PH_INIT3) {
+            // initTimeStep (src/math_ode.cpp:35-91): Euler + Heun probes, Aarseth-like estimate
+            double h2 = INFINITY;
+            for(int c = 0; c < 6; c++) {
+                const double k2c = S.at(0, c);
+                const double d0 = fmax(P.accAbs, fmax(fabs(x[c]), fabs(xt[c])));
+                const double d1 = fmax(fabs(k1[c]), fabs(k[c]));
+                const double d2 = fabs((3 * k2c - k1[c] - 2 * k[c]) / h1);
+                const double d3 = fabs(6 * (k[c] - k2c) / (h1 * h1));
+                h2 = fmin(h2, (d0 * d2 + d1 * d1) / (d1 * d3 + d2 * d2));
+            }
+            hNext = fmax(HMIN, fmin(HMAX, pow(P.accRel, 1. / 8) * sqrt(h2))) * accFac;
+            startStep();
+        } else if(row < NUM_ROWS - 1) {
+            const int d = tab.dest[row];
+            for(int c = 0; c < 6; c++) S.at(d, c) = k[c];
+            row++;
+        } else {
+            // ---- error estimate (3rd and 5th order embedded solutions), k13 = k
+            double err5 = 0, err3 = 0;
+            for(int c = 0; c < 6; c++) {
+                const double sk = (P.accAbs + P.accRel * fmax(fabs(x[c]), fabs(xt[c]))) * af;
+                if(sk == 0) continue;
+                err3 += pow2((k1b[c] - bhh1 * k1[c] - bhh2 * S.at(7, c) - bhh3 * S.at(1, c)) / sk);
+                err5 += pow2((er1 * k1[c] + er6 * S.at(4, c) + er7 * S.at(5, c) + er8 * S.at(6, c) +
+                    er9 * S.at(7, c) + er10 * S.at(8, c) + er11 * S.at(0, c) + er12 * S.at(1, c)) / sk);
+            }
+            const double den = sqrt(6 * (err5 + 0.01 * err3));
+            const double err = den == 0 ? 0 : err5 * fabs(h) / den;
+            if(!isFinite(err)) { st = ORBIT_NONFINITE; phase = PH_FINISH; continue; }
+            double fac = sqrt(sqrt(sqrt(err)));
+            bool accepted = false;
+            if(err <= 1) {
+                hNext = fabs(h) * fmin(finc, safe / fac);
+                accepted = true;
+            } else {
+                if(err > 0.5 * preverr) {
+                    nbad++;
+                    if(nbad >= 2) fac = 1 / fdec;
+                    if(nbad >= 4) { hNext = fabs(h); accepted = true; }
+                } else
+                    nbad = 0;
+                if(!accepted) {
+                    preverr = err;
+                    h *= fmax(fdec, safe / fac);
+                    rejects++;
+                    startAttempt();
+                    continue;
+                }
+            }
+            for(int c = 0; c < 6; c++) { x[c] = xt[c]; k1[c] = k[c]; }
+            tb = t;
+            hLast = h;
+            t = h == remaining ? tEnd : t + h;
+            if(++steps >= P.maxSteps) {
+                if(t != tEnd) st = ORBIT_MAX_STEPS;
+                phase = PH_FINISH;
+                continue;
+            }
+            startStep();
+        }
     }
 }
 
