@@ -46,6 +46,8 @@ def lib():
         L.ref_eval_cyl_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, _D, _D]
         L.ref_orbits_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_long, _D, _L, _I, ctypes.c_int]
+        L.ref_orbits_evals.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_long, _LL, ctypes.c_int]
         L.ref_actions_fd_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, _D, _LL, ctypes.c_int]
         L.ref_actions_angles_fd_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, _D, _D, _D,
                                                  ctypes.c_int]
@@ -116,6 +118,15 @@ class Potential:
         _check(lib().ref_orbits_many(self.h, n, _p(ic), _p(T), Omega, accuracy, maxSteps,
                                      _p(final), _p(nsteps, _L), _p(status, _I), nthreads))
         return final, nsteps, status
+
+    def orbit_evals(self, ic, T, Omega=0.0, accuracy=1e-8, maxSteps=0, nthreads=0):
+        """potential evaluations spent on each orbit"""
+        ic = np.ascontiguousarray(ic, dtype=np.float64).reshape(-1, 6)
+        n = len(ic)
+        T = np.ascontiguousarray(np.broadcast_to(np.asarray(T, dtype=np.float64), (n,)))
+        ev = np.zeros(n, dtype=np.int64)
+        _check(lib().ref_orbits_evals(self.h, n, _p(ic), _p(T), Omega, accuracy, maxSteps, _p(ev, _LL), nthreads))
+        return ev
 
     def actions_fd(self, posvel, fd, count=False, nthreads=0):
         posvel = np.ascontiguousarray(posvel, dtype=np.float64).reshape(-1, 6)

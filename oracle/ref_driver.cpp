@@ -183,6 +183,31 @@ int ref_orbits_many(void* handle, long n, const double* ic, const double* T, dou
     return 0;
 }
 
+/// the number of potential evaluations each orbit of ref_orbits_many costs (counting wrapper)
+int ref_orbits_evals(void* handle, long n, const double* ic, const double* T, double Omega,
+    double accuracy, long maxSteps, long long* nevals, int nthreads)
+{
+    potential::PtrPotential base = static_cast<PotHandle*>(handle)->pot;
+    setThreads(nthreads);
+    orbit::OrbitIntParams params(accuracy, maxSteps > 0 ? (size_t)maxSteps : (size_t)1e8);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 1)
+    for(long i = 0; i < n; i++) {
+        try {
+            CountingPotential cnt(base);
+            orbit::OrbitIntegrator<coord::Car> orbint(cnt, Omega, params);
+            orbint.init(coord::PosVelCar(ic + 6*i));
+            orbint.run(T[i]);
+            nevals[i] = cnt.count;
+        } catch(std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
 /// Staeckel-fudge actions with a given focal distance per point (Cartesian posvel input);
 /// if countEvals is not NULL, it receives the number of potential evaluations per point
 int ref_actions_fd_many(void* handle, long n, const double* posvel, const double* fd, double* act,
