@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--particles", type=int, default=1000000)
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the force / orbit workloads")
     return ap.parse_args()
 
 
@@ -140,7 +141,28 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "actions/s", "cores": cores, "kind": "reference",
                          "sample": "%d of the %d config-2 particles per step" % (sample, args.particles)},
         "e2e": {"value": value, "unit": "actions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "secondary": None if args.no_secondary else run_reference_secondary(),
     }))
+
+
+def run_reference_secondary():
+    """the secondary workloads on the reference's CPU code (bounded samples, all host cores)"""
+    from oracle import ref
+
+    class RefPot:
+        def __init__(self, f):
+            self.p = ref.Potential(file=f)
+
+        def potential(self, x):
+            return self.p.eval(x)[0]
+
+        def force(self, x):
+            return -self.p.eval(x)[1]
+    _, pts1, ic1, T1, _, ic3, T3 = secondary_workloads(RefPot, lambda c: os.path.join(GOLDEN, c + ".coef"))
+    names = [("force evals/s", "config 1 forces"), ("orbit-steps/s", "config 1 orbits"),
+             ("orbit-steps/s", "config 3 orbits, at most %d steps per orbit" % ORBIT3_MAX_STEPS)]
+    return [dict(metric=m, value=b and b["value"], unit=b and b.get("unit"), config=c, cpu_baseline=b)
+            for (m, c), b in zip(names, reference_secondary(pts1, ic1, T1, ic3, T3))]
 
 
 def cpu_baseline_line(pts):
@@ -162,6 +184,114 @@ def cpu_baseline_line(pts):
     except Exception as e:   # the baseline is reported, never required
         return {"value": None, "unit": "actions/s", "cores": os.cpu_count(), "kind": "reference",
                 "sample": "failed: %s" % e}
+
+
+# ------------------------------------------------------------------------------------------
+# Secondary workloads: the other headline throughputs of the path, measured in the same run.
+#   config 1 forces:  1e5 points of the triaxial Dehnen Multipole (lmax 6, 50 nodes), potential
+#                     and force per point                                   -> force evals/s
+#   config 1 orbits:  1e4 orbits, T = 10 T_circ(E), DOP853 accuracy 1e-8     -> orbit-steps/s
+#   config 3 orbits:  2e4 of the 1e5 config-3 orbits (T = 10-1000 T_circ, Omega = 0.05), at most
+#                     ORBIT3_MAX_STEPS accepted steps per orbit: the workload's tail (orbits near
+#                     r ~ 1e3 whose T spans 1e4-1e6 turns of the rotating frame) needs up to 1e7
+#                     steps per orbit, hours of integration on either arm   -> orbit-steps/s
+ORBIT3_ORBITS = 20000
+ORBIT3_MAX_STEPS = 5000
+
+
+def secondary_workloads(potential_cls, coef):
+    """inputs of the secondary workloads for a potential class with .potential / .force"""
+    from agama_b200 import workloads
+    pot1 = potential_cls(coef("cfg1"))
+    pts1 = workloads.dehnen_positions(100000, 1.0, q=(0.8, 0.6), seed=workloads.SEEDS["points1"])
+    ic1, T1 = workloads.orbit_workload(1, pot1.potential, pot1.force)
+    pot3 = potential_cls(coef("cfg3"))
+    ic3, T3 = workloads.orbit_workload(3, pot3.potential, pot3.force, ORBIT3_ORBITS)
+    return pot1, pts1, ic1, T1, pot3, ic3, T3
+
+
+def run_engine_secondary(dev, flush, dist, cpu):
+    """device-timed throughputs of the secondary workloads (max over ranks), with the reference
+    on the host cores beside each when cpu is true"""
+    import torch
+    import agama_b200
+
+    class Pot(agama_b200.Potential):
+        def __init__(self, f):
+            super().__init__(file=f)
+    pot1, pts1, ic1, T1, pot3, ic3, T3 = secondary_workloads(Pot, lambda c: os.path.join(GOLDEN, c + ".coef"))
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, warmup, steps):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r = fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        t = float(np.mean(ms))
+        if dist:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, r
+
+    out = []
+    d1 = torch.tensor(pts1, device=dev)
+    t, _ = timed(lambda: pot1.eval(d1, pot=True, acc=True), 3, 10)
+    out.append({"metric": "force evals/s", "value": len(pts1) / (t / 1000), "unit": "evals/s", "ms_per_step": t,
+                "config": "config 1: 1e5 points, triaxial Dehnen Multipole lmax 6 / 50 nodes, potential + force",
+                "steps": 10, "warmup": 3, "gpu_launches_per_step": 1})
+    for name, pot, ic, T, Om, mx, warm, steps in (
+            ("config 1: 1e4 orbits x 10 T_circ, DOP853 1e-8", pot1, ic1, T1, 0.0, 0, 3, 5),
+            ("config 3: %d of the 1e5 orbits (10-1000 T_circ, Omega 0.05), DOP853 1e-8, at most %d steps per orbit"
+             % (ORBIT3_ORBITS, ORBIT3_MAX_STEPS), pot3, ic3, T3, 0.05, ORBIT3_MAX_STEPS, 1, 2)):
+        dic, dT = torch.tensor(ic, device=dev), torch.tensor(T, device=dev)
+        t, r = timed(lambda: agama_b200.orbit(pot, dic, dT, Omega=Om, maxNumSteps=mx, info=True), warm, steps)
+        info = r[1]
+        nst, nrej = int(info["steps"].sum().item()), int(info["rejected"].sum().item())
+        out.append({"metric": "orbit-steps/s", "value": nst / (t / 1000), "unit": "accepted DOP853 steps/s",
+                    "ms_per_step": t, "config": name, "steps": steps, "warmup": warm, "accepted_steps": nst,
+                    "rejected_attempts": nrej, "gpu_launches_per_step": 1})
+    if cpu:
+        for line, base in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3)):
+            line["cpu_baseline"] = base
+    return out
+
+
+def reference_secondary(pts1, ic1, T1, ic3, T3):
+    """the reference's own CPU code on bounded samples of the secondary workloads, all host cores"""
+    try:
+        from oracle import ref
+        if not ref.available():
+            return [None, None, None]
+        cores = os.cpu_count()
+        p1 = ref.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+        p3 = ref.Potential(file=os.path.join(GOLDEN, "cfg3.coef"))
+        res = []
+        p1.eval(pts1[:1000], nthreads=cores)
+        t0 = time.perf_counter()
+        p1.eval(pts1, nthreads=cores)
+        dt = time.perf_counter() - t0
+        res.append({"value": len(pts1) / dt, "unit": "evals/s", "cores": cores, "kind": "reference",
+                    "sample": "all 1e5 config-1 points, potential + force, OpenMP"})
+        for ic, T, Om, mx, n, what in ((ic1, T1, 0.0, 0, 2000, "config 1"),
+                                       (ic3, T3, 0.05, ORBIT3_MAX_STEPS, 400, "config 3")):
+            t0 = time.perf_counter()
+            _, steps, _ = p1.orbits(ic[:n], T[:n], Omega=Om, maxSteps=mx, nthreads=cores) if what == "config 1" else \
+                p3.orbits(ic[:n], T[:n], Omega=Om, maxSteps=mx, nthreads=cores)
+            dt = time.perf_counter() - t0
+            res.append({"value": float(steps.sum()) / dt, "unit": "accepted DOP853 steps/s", "cores": cores,
+                        "kind": "reference", "sample": "first %d orbits of the %s workload, OpenMP dynamic 1" % (n, what)})
+        return res
+    except Exception as e:   # the baseline is reported, never required
+        return [{"value": None, "kind": "reference", "sample": "failed: %s" % e}] * 3
 
 
 def run_engine(args):
@@ -261,14 +391,18 @@ def run_engine(args):
             "clocks": clocks,
             "cpu_baseline": None if args.no_baseline else cpu_baseline_line(pts),
         }
+    secondary = None if args.no_secondary else run_engine_secondary(dev, flush, dist, rank == 0 and not args.no_baseline)
+    if rank == 0:
+        if secondary is not None:
+            line["secondary"] = secondary
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
-# kernels per action step: prepare, three root-search kinds, integrals
-ACTION_LAUNCHES_PER_STEP = 5
+# kernels per action step: prepare, root searches, integrals
+ACTION_LAUNCHES_PER_STEP = 3
 # executed FP64 flops per action (dadd + dmul + 2 dfma summed over the five kernels, ncu, config-2
 # workload) and DRAM bytes of one step for 1e6 particles
 FLOPS_PER_ACTION_CFG2 = 26206.0
