@@ -43,6 +43,20 @@ def _current_stream():
         return None
 
 
+def _host_empty(shape, dtype=np.float64):
+    """a host output array in page-locked memory (torch's caching host allocator, so repeated
+    calls reuse the same blocks) when CUDA is usable: device-to-host copies into it run at full
+    PCIe speed and overlap the kernels of the next chunk; plain numpy memory otherwise"""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            tdt = {np.float64: torch.float64, np.int64: torch.int64, np.int32: torch.int32}[np.dtype(dtype).type]
+            return torch.empty(shape, dtype=tdt, pin_memory=True).numpy()
+    except Exception:
+        pass
+    return np.empty(shape, dtype=dtype)
+
+
 def _points(a, ncol):
     a = np.ascontiguousarray(a, dtype=np.float64)
     single = a.ndim == 1
@@ -99,9 +113,9 @@ class Potential:
             return self._eval_device(points, pot, acc, der)
         p, single = _points(points, 3)
         n = len(p)
-        phi = np.empty(n)
-        grad = np.empty((n, 3)) if (acc or der) else None
-        hess = np.empty((n, 6)) if der else None
+        phi = _host_empty(n)
+        grad = _host_empty((n, 3)) if (acc or der) else None
+        hess = _host_empty((n, 6)) if der else None
         check(_native.lib().agama_evalPotentialMany(self._h, n, ptr(p), 0.0, ptr(phi), ptr(grad), ptr(hess)))
         out = []
         if pot:

@@ -18,6 +18,11 @@ from . import _native
 from ._native import check, ptr
 
 
+def _host_empty(shape):
+    from . import _host_empty as he
+    return he(shape)
+
+
 class ActionFinder:
     """Staeckel-fudge action finder (the reference's ActionFinderAxisymFudge, non-interpolated).
 
@@ -97,8 +102,8 @@ class ActionFinder:
         single = p.ndim == 1
         p = p.reshape(-1, 6)
         n = len(p)
-        act = np.empty((n, 3))
-        fdo = np.empty(n) if fd else None
+        act = _host_empty((n, 3))
+        fdo = _host_empty(n) if fd else None
         check(_native.lib().agama_evalActionsMany(self._h, n, ptr(p), ptr(act), ptr(fdo)))
         if single:
             act = act[0]
@@ -121,7 +126,7 @@ def _angles_call(points, want_act, want_ang, want_freq, call):
         single = p.ndim == 1
         p = p.reshape(-1, 6)
         n = len(p)
-        outs = [np.empty((n, 3)) if w else None for w in (want_act, want_ang, want_freq)]
+        outs = [_host_empty((n, 3)) if w else None for w in (want_act, want_ang, want_freq)]
         check(call(n, ptr(p), *[ptr(o) for o in outs], False))
         if single:
             outs = [o[0] if o is not None else None for o in outs]
@@ -166,7 +171,7 @@ def actions(potential, points, fd, iters=False, angles=False, frequencies=False)
     single = p.ndim == 1
     p = p.reshape(-1, 6)
     n = len(p)
-    act = np.empty((n, 3))
+    act = _host_empty((n, 3))
     if np.ndim(fd) == 0:
         check(_native.lib().agama_evalActionsStandaloneMany(potential.handle, n, ptr(p), None, float(fd), ptr(act)))
     else:

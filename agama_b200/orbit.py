@@ -41,9 +41,10 @@ def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=Tr
     x = x.reshape(-1, 6)
     n = len(x)
     T = np.ascontiguousarray(np.broadcast_to(np.asarray(time, dtype=np.float64), (n,)))
-    out = np.empty((n, 6))
-    steps = np.zeros(n, dtype=np.int64)
-    st = np.zeros(n, dtype=np.int32)
+    from . import _host_empty
+    out = _host_empty((n, 6))
+    steps = _host_empty(n, np.int64)
+    st = _host_empty(n, np.int32)
     check(_native.lib().agama_integrateOrbitsMany(
         potential.handle, n, ptr(x), ptr(T), float(Omega), float(accuracy), int(maxNumSteps),
         ptr(out), steps.ctypes.data_as(_native.L), st.ctypes.data_as(_native.I)))
