@@ -405,9 +405,10 @@ def run_engine(args):
 ACTION_LAUNCHES_PER_STEP = 3
 # executed FP64 flops per action (dadd + dmul + 2 dfma summed over the five kernels, ncu, config-2
 # workload) and DRAM bytes of one step for 1e6 particles
-FLOPS_PER_ACTION_CFG2 = 26206.0
-# dram read + write of one 200 000-particle launch (9.89 MB + 0.22 MB), scaled to 1e6 particles
-TRAFFIC_PER_LAUNCH_CFG2 = 5 * (9.888256e6 + 0.220416e6)
+FLOPS_PER_ACTION_CFG2 = 26508.0
+# dram read + write of the three kernels of one 200 000-particle step (prepare 11.00 + 1.79 MB,
+# roots 25.76 + 22.79 MB, integrals 26.00 + 0.01 MB), scaled to 1e6 particles
+TRAFFIC_PER_LAUNCH_CFG2 = 5 * 87.35e6
 
 
 def ctypes_stream(stream):
