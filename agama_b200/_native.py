@@ -35,6 +35,8 @@ SIGNATURES = {
                                                               ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
                                                               ctypes.c_int, VP]),
     "agama_measureFP64Throughput": (ctypes.c_int, [D]),
+    "agama_gemmBf16Device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, VP, VP, ctypes.c_int,
+                                            ctypes.c_int, VP]),
     "agama_createActionFinder": (VP, [VP]),
     "agama_getActionFinderTableSizes": (ctypes.c_int, [VP, I, I, I, I, I]),
     "agama_getActionFinderTables": (ctypes.c_int, [VP, D, D, D, D, D, D, D]),

@@ -4,6 +4,7 @@
 // batched calls return a non-zero status, with the message in agama_getError().
 #include "runtime.h"
 #include "host_pipeline.h"
+#include "mlp.h"
 #include "../../include/agama_b200.h"
 #include <cstring>
 #include <sstream>
@@ -480,6 +481,17 @@ extern "C" void agama_evalActionsAnglesFrequenciesStandalone(const agama_Potenti
     const int rc = agama_evalActionsAnglesFrequenciesStandaloneMany(p, 1, posvel, nullptr, fd, act,
         angles ? ang : nullptr, frequencies ? freq : nullptr);
     storeSinglePoint(rc, act, ang, freq, actions, angles, frequencies);
+}
+
+extern "C" int agama_gemmBf16Device(int M, int N, int K, const void* A, const void* B, float* C, int ldc,
+    int accumulate, void* stream)
+{
+    return guarded([&] {
+        if(M < 0 || N < 0 || K < 0 || (M > 0 && N > 0 && K > 0 && (!A || !B || !C)))
+            throw std::invalid_argument("gemmBf16Device: invalid arguments");
+        requireDevice();
+        launchGemmBf16(M, N, K, A, B, C, ldc, accumulate != 0, static_cast<cudaStream_t>(stream));
+    });
 }
 
 // ------------------------------------------------------------------------------------------

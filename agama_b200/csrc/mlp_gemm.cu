@@ -1,0 +1,130 @@
+// BF16 x BF16 -> FP32 GEMM on the fifth-generation tensor cores, the building block of the
+// bracket-predictor network's training (umma.cuh: descriptors, tensor memory, MMA).
+//
+//   C[M x N] (FP32, row-major, leading dimension ldc) = A[M x K] * B[N x K]^T  (+ C if accumulate)
+//
+// A and B are BF16 row-major with K contiguous (both "K-major"), M and N multiples of 128, K a
+// multiple of 64.  One CTA of 4 warps computes one 128 x 128 tile: K is walked in chunks of 64,
+// each chunk staged into shared memory in the canonical layout and consumed by four 128x128x16
+// MMAs issued by one thread into a 128-column tensor-memory accumulator; the accumulator is read
+// back by all four warps (warp w owns rows 32w..32w+31).
+#include "runtime.h"
+#include "umma.cuh"
+#include "mlp.h"
+#include <cuda_bf16.h>
+
+namespace agb {
+
+namespace {
+
+constexpr int GEMM_BM = 128, GEMM_BN = 128, GEMM_BK = 64;
+constexpr int TILE_BYTES = GEMM_BM * GEMM_BK * 2;            // 16 KB per operand tile
+// 64 KB of shared memory per CTA keeps at most 3 CTAs (384 tensor-memory columns) on an SM, so an
+// allocation never waits for another CTA's columns
+constexpr int GEMM_SMEM = 64 * 1024;
+constexpr long MBAR_MAX_POLLS = 1L << 22;
+
+__global__ void __launch_bounds__(128) gemmBf16Kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
+    const __nv_bfloat16* __restrict__ B, float* __restrict__ C, int ldc, int accumulate, int* __restrict__ error)
+{
+    extern __shared__ unsigned char smemRaw[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmemBase;
+    unsigned char* tiles = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+    unsigned char* tileA = tiles;
+    unsigned char* tileB = tiles + TILE_BYTES;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int bm = blockIdx.y * GEMM_BM, bn = blockIdx.x * GEMM_BN;
+
+    if(warp == 0) umma::tmemAlloc(&tmemBase, 128);
+    if(threadIdx.x == 0) umma::mbarInit(&mbar, 1);
+    umma::fenceBeforeSync();
+    __syncthreads();
+    umma::fenceAfterSync();
+    const uint32_t tmem = tmemBase;
+    constexpr uint32_t idesc = umma::instrDescBf16(GEMM_BM, GEMM_BN);
+    constexpr uint32_t SBO = GEMM_BK / 8 * umma::CORE_BYTES;
+
+    uint32_t parity = 0;
+    bool ok = true;
+    for(int k0 = 0; k0 < K && ok; k0 += GEMM_BK) {
+        // stage the 128 x 64 chunks of A and B: 16-byte vectors = one row of one core matrix
+        for(int v = threadIdx.x; v < GEMM_BM * GEMM_BK / 8; v += blockDim.x) {
+            const int r = v / (GEMM_BK / 8), kc = v % (GEMM_BK / 8);
+            const uint32_t off = umma::tileOffset(r, kc * 8, GEMM_BK);
+            *reinterpret_cast<uint4*>(tileA + off) =
+                *reinterpret_cast<const uint4*>(A + static_cast<size_t>(bm + r) * K + k0 + kc * 8);
+            *reinterpret_cast<uint4*>(tileB + off) =
+                *reinterpret_cast<const uint4*>(B + static_cast<size_t>(bn + r) * K + k0 + kc * 8);
+        }
+        umma::fenceSmemForAsync();
+        __syncthreads();
+        if(threadIdx.x == 0) {
+            umma::fenceAfterSync();
+            for(int kk = 0; kk < GEMM_BK / 16; kk++) {
+                const uint64_t da = umma::smemDescriptor(umma::smemAddr(tileA) + kk * 2 * umma::LBO, umma::LBO, SBO);
+                const uint64_t db = umma::smemDescriptor(umma::smemAddr(tileB) + kk * 2 * umma::LBO, umma::LBO, SBO);
+                umma::mmaBf16(tmem, da, db, idesc, k0 > 0 || kk > 0);
+            }
+            umma::commitTo(&mbar);
+        }
+        // every thread waits for the MMAs of this chunk before the tiles are overwritten
+        const bool done = umma::mbarWait(&mbar, parity, MBAR_MAX_POLLS);
+        parity ^= 1;
+        ok = __syncthreads_and(done);
+    }
+    umma::fenceAfterSync();
+    if(ok) {
+        const int row = bm + warp * 32 + lane;
+        for(int c0 = 0; c0 < GEMM_BN; c0 += 32) {
+            float v[32];
+            umma::tmemLoad32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
+            float* out = C + static_cast<size_t>(row) * ldc + bn + c0;
+#pragma unroll
+            for(int j = 0; j < 32; j++) out[j] = accumulate ? out[j] + v[j] : v[j];
+        }
+    } else if(threadIdx.x == 0) {
+        atomicExch(error, 1);
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+    if(warp == 0) umma::tmemFree(tmem, 128);
+}
+
+int* gemmErrorFlag()
+{
+    static int* flag = nullptr;     // one per process on the first device used (zeroed at allocation)
+    if(!flag) {
+        AGB_CUDA(cudaMalloc(&flag, sizeof(int)));
+        AGB_CUDA(cudaMemset(flag, 0, sizeof(int)));
+    }
+    return flag;
+}
+
+}  // namespace
+
+void launchGemmBf16(int M, int N, int K, const void* A, const void* B, float* C, int ldc, bool accumulate,
+    cudaStream_t stream)
+{
+    if(M <= 0 || N <= 0 || K <= 0) return;
+    if(M % GEMM_BM || N % GEMM_BN || K % GEMM_BK || ldc < N)
+        throw std::invalid_argument("gemmBf16: M, N must be multiples of 128, K of 64, ldc >= N");
+    static bool attr = false;
+    if(!attr) {
+        AGB_CUDA(cudaFuncSetAttribute(gemmBf16Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+        attr = true;
+    }
+    const dim3 grid(N / GEMM_BN, M / GEMM_BM);
+    gemmBf16Kernel<<<grid, 128, GEMM_SMEM, stream>>>(M, N, K, static_cast<const __nv_bfloat16*>(A),
+        static_cast<const __nv_bfloat16*>(B), C, ldc, accumulate ? 1 : 0, gemmErrorFlag());
+    AGB_CUDA(cudaGetLastError());
+}
+
+void checkGemmError()
+{
+    int h = 0;
+    AGB_CUDA(cudaMemcpy(&h, gemmErrorFlag(), sizeof(int), cudaMemcpyDeviceToHost));
+    if(h) throw std::runtime_error("gemmBf16: tensor-core completion barrier timed out");
+}
+
+}  // namespace agb

@@ -195,6 +195,14 @@ int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential
     const double* posvel, const double* fd, double fd0, double* act, double* ang, double* freq, void* stream);
 
 /* ---------------------------------------------------------------------------------------
+   Tensor-core GEMM of the bracket-predictor network (no reference counterpart; the reference has
+   no learned part): C[M x N] (FP32, leading dimension ldc) = A[M x K] * B[N x K]^T, plus the old C
+   when accumulate is non-zero.  A and B are BF16 row-major with K contiguous, device pointers
+   aligned to 16 bytes; M and N multiples of 128, K a multiple of 64.  Asynchronous on stream. */
+int agama_gemmBf16Device(int M, int N, int K, const void* A, const void* B, float* C, int ldc,
+    int accumulate, void* stream);
+
+/* ---------------------------------------------------------------------------------------
    Measurement helper (no reference counterpart): FP64 fused-multiply-add throughput of the
    current device in TFLOP/s, measured with independent FMA chains; the roofline denominator
    of the FP64-bound kernels above. */
