@@ -158,3 +158,4 @@ class Potential:
 
 from .actions import ActionFinder, actions  # noqa: E402,F401
 from .orbit import orbit  # noqa: E402,F401
+from .mlp import BracketNet  # noqa: E402,F401

@@ -35,6 +35,16 @@ SIGNATURES = {
                                                               ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
                                                               ctypes.c_int, VP]),
     "agama_measureFP64Throughput": (ctypes.c_int, [D]),
+    "agama_mlpCreate": (VP, [ctypes.c_ulonglong]),
+    "agama_mlpDelete": (None, [VP]),
+    "agama_mlpNumParams": (ctypes.c_int, []),
+    "agama_mlpGetParams": (ctypes.c_int, [VP, F, F]),
+    "agama_mlpSetParams": (ctypes.c_int, [VP, F, F]),
+    "agama_mlpLossGrad": (ctypes.c_int, [VP, ctypes.c_int, F, F, F, F, F]),
+    "agama_mlpTrain": (ctypes.c_int, [VP, ctypes.c_long, F, F, F, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                      ctypes.c_ulonglong, F]),
+    "agama_mlpPredictDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP]),
+    "agama_mlpCheck": (ctypes.c_int, [VP]),
     "agama_gemmBf16Device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, VP, VP, ctypes.c_int,
                                             ctypes.c_int, VP]),
     "agama_createActionFinder": (VP, [VP]),

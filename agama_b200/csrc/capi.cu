@@ -495,6 +495,96 @@ extern "C" int agama_gemmBf16Device(int M, int N, int K, const void* A, const vo
 }
 
 // ------------------------------------------------------------------------------------------
+// the bracket-predictor network
+
+struct agama_Mlp { Mlp* net; };
+
+extern "C" agama_Mlp* agama_mlpCreate(unsigned long long seed)
+{
+    try {
+        requireDevice();
+        return new agama_Mlp{ new Mlp(seed) };
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+extern "C" void agama_mlpDelete(agama_Mlp* m)
+{
+    if(!m) return;
+    delete m->net;
+    delete m;
+}
+
+extern "C" int agama_mlpNumParams() { return MLP_NUM_PARAMS; }
+
+extern "C" int agama_mlpGetParams(const agama_Mlp* m, float* params, float* scaling)
+{
+    return guarded([&] {
+        if(!m) throw std::invalid_argument("mlpGetParams: null network");
+        AGB_CUDA(cudaSetDevice(m->net->device));
+        if(params) AGB_CUDA(cudaMemcpy(params, m->net->params.ptr, sizeof(float) * MLP_NUM_PARAMS, cudaMemcpyDeviceToHost));
+        if(scaling) AGB_CUDA(cudaMemcpy(scaling, m->net->scaling.ptr, sizeof(float) * 18, cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" int agama_mlpSetParams(agama_Mlp* m, const float* params, const float* scaling)
+{
+    return guarded([&] {
+        if(!m) throw std::invalid_argument("mlpSetParams: null network");
+        AGB_CUDA(cudaSetDevice(m->net->device));
+        if(params) AGB_CUDA(cudaMemcpy(m->net->params.ptr, params, sizeof(float) * MLP_NUM_PARAMS, cudaMemcpyHostToDevice));
+        if(scaling) AGB_CUDA(cudaMemcpy(m->net->scaling.ptr, scaling, sizeof(float) * 18, cudaMemcpyHostToDevice));
+        m->net->refreshWeights(0);
+        AGB_CUDA(cudaDeviceSynchronize());
+    });
+}
+
+extern "C" int agama_mlpLossGrad(agama_Mlp* m, int batch, const float* x, const float* t, const float* mask,
+    float* grad, float* loss)
+{
+    return guarded([&] {
+        if(!m || !x || !t || !mask || !grad) throw std::invalid_argument("mlpLossGrad: invalid arguments");
+        AGB_CUDA(cudaSetDevice(m->net->device));
+        DevBuf<float> g(MLP_NUM_PARAMS);
+        const float l = m->net->lossGradDevice(batch, x, t, mask, g.ptr, 0);
+        AGB_CUDA(cudaMemcpy(grad, g.ptr, sizeof(float) * MLP_NUM_PARAMS, cudaMemcpyDeviceToHost));
+        if(loss) *loss = l;
+    });
+}
+
+extern "C" int agama_mlpTrain(agama_Mlp* m, long n, const float* x, const float* t, const float* mask, int epochs,
+    int batch, float lr, unsigned long long seed, float* lossHistory)
+{
+    return guarded([&] {
+        if(!m || n <= 0 || !x || !t || !mask || epochs < 0) throw std::invalid_argument("mlpTrain: invalid arguments");
+        AGB_CUDA(cudaSetDevice(m->net->device));
+        const std::vector<float> h = m->net->train(n, x, t, mask, epochs, batch, lr, seed, 0);
+        if(lossHistory) for(size_t k = 0; k < h.size(); k++) lossHistory[k] = h[k];
+    });
+}
+
+extern "C" int agama_mlpPredictDevice(const agama_Mlp* m, long n, const float* x, float* y, void* stream)
+{
+    return guarded([&] {
+        if(!m || n < 0 || (n > 0 && (!x || !y))) throw std::invalid_argument("mlpPredictDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(m->net->device));
+        m->net->predict(n, x, y, static_cast<cudaStream_t>(stream));
+    });
+}
+
+extern "C" int agama_mlpCheck(const agama_Mlp* m)
+{
+    return guarded([&] {
+        if(!m) throw std::invalid_argument("mlpCheck: null network");
+        AGB_CUDA(cudaSetDevice(m->net->device));
+        AGB_CUDA(cudaDeviceSynchronize());
+        m->net->checkError();
+    });
+}
+
+// ------------------------------------------------------------------------------------------
 // device FP64 throughput probe (the roofline denominator for the FP64-bound kernels)
 
 namespace {

@@ -203,6 +203,33 @@ int agama_gemmBf16Device(int M, int N, int K, const void* A, const void* B, floa
     int accumulate, void* stream);
 
 /* ---------------------------------------------------------------------------------------
+   Bracket-predictor network (no reference counterpart; the reference has no learned part):
+   6 -> 128 -> 128 -> 128 -> 3 with SiLU, BF16 weights in the hidden products on the tensor cores,
+   FP32 master parameters, Adam.  Parameters (agama_mlpNumParams() floats): W1[128x6] b1
+   W2[128x128] b2 W3[128x128] b3 W4[3x128] b4, weights row-major [out][in]; scaling (18 floats):
+   input mean[6], input std[6], output mean[3], output std[3]. */
+typedef struct agama_Mlp agama_Mlp;
+agama_Mlp* agama_mlpCreate(unsigned long long seed);
+void agama_mlpDelete(agama_Mlp* net);
+int agama_mlpNumParams(void);
+int agama_mlpGetParams(const agama_Mlp* net, float* params, float* scaling);
+int agama_mlpSetParams(agama_Mlp* net, const float* params, const float* scaling);
+/* loss (masked mean squared error) and gradient (host output) of one batch of STANDARDISED inputs
+   x[batch x 6], targets t[batch x 3] and masks (0/1) [batch x 3]; batch a multiple of 128 */
+int agama_mlpLossGrad(agama_Mlp* net, int batch, const float* x, const float* t, const float* mask,
+    float* grad, float* loss);
+/* Adam training on n raw samples (the standardisation is derived from them and kept); lossHistory
+   (epochs floats, may be NULL) receives the mean loss of each epoch; batch a multiple of 128 */
+int agama_mlpTrain(agama_Mlp* net, long n, const float* x, const float* t, const float* mask, int epochs,
+    int batch, float lr, unsigned long long seed, float* lossHistory);
+/* predictions y[n x 3] (raw units) for raw inputs x[n x 6], device pointers, on stream: the fused
+   tensor-core inference kernel */
+int agama_mlpPredictDevice(const agama_Mlp* net, long n, const float* x, float* y, void* stream);
+/* synchronises and reports whether an inference kernel of this network gave up waiting for its
+   tensor cores */
+int agama_mlpCheck(const agama_Mlp* net);
+
+/* ---------------------------------------------------------------------------------------
    Measurement helper (no reference counterpart): FP64 fused-multiply-add throughput of the
    current device in TFLOP/s, measured with independent FMA chains; the roofline denominator
    of the FP64-bound kernels above. */
