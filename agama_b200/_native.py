@@ -35,6 +35,11 @@ SIGNATURES = {
                                                               ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
                                                               ctypes.c_int, VP]),
     "agama_measureFP64Throughput": (ctypes.c_int, [D]),
+    "agama_actionFinderBracketSamples": (ctypes.c_int, [VP, ctypes.c_long, D, F, F, F]),
+    "agama_actionFinderTrainBrackets": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_int, ctypes.c_int,
+                                                       ctypes.c_float, ctypes.c_ulonglong, F, F]),
+    "agama_actionFinderUseBrackets": (ctypes.c_int, [VP, ctypes.c_int]),
+    "agama_actionFinderBracketStats": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     "agama_mlpCreate": (VP, [ctypes.c_ulonglong]),
     "agama_mlpDelete": (None, [VP]),
     "agama_mlpNumParams": (ctypes.c_int, []),

@@ -75,6 +75,35 @@ class ActionFinder:
         return dict(gridE=gE, gridL=gL, delta=dl, lofe=lofe, rofl=rofl, phiofr=phr, invPhi0=scal[0],
                     interp_invPhi0=scal[1], slopeOut=scal[2], coefOut=scal[3], massOut=scal[4])
 
+    # ---- learned root brackets
+    def bracket_samples(self, points):
+        """inputs (n x 6), targets (n x 3) and masks (n x 3) of the bracket predictor from the plain
+        root searches of the points"""
+        p = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 6)
+        n = len(p)
+        f, t, m = (np.empty((n, k), dtype=np.float32) for k in (6, 3, 3))
+        check(_native.lib().agama_actionFinderBracketSamples(self._h, n, ptr(p), ptr(f, _native.F), ptr(t, _native.F),
+                                                             ptr(m, _native.F)))
+        return f, t, m
+
+    def train_brackets(self, points, epochs=10, batch=2048, lr=2e-3, seed=0):
+        """train the bracket predictor on the finder's own root searches for these points and
+        switch it on; returns (loss per epoch, bracket half-widths)"""
+        p = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 6)
+        hist, w = np.empty(epochs, dtype=np.float32), np.empty(3, dtype=np.float32)
+        check(_native.lib().agama_actionFinderTrainBrackets(self._h, len(p), ptr(p), int(epochs), int(batch), float(lr),
+                                                            int(seed), ptr(hist, _native.F), ptr(w, _native.F)))
+        return hist, w
+
+    def use_brackets(self, on=True):
+        check(_native.lib().agama_actionFinderUseBrackets(self._h, 1 if on else 0))
+
+    def bracket_stats(self, reset=False):
+        """{searches, narrowed, fallbacks, iterations} of the root searches since the last reset"""
+        st = (ctypes.c_longlong * 4)()
+        check(_native.lib().agama_actionFinderBracketStats(self._h, st, 1 if reset else 0))
+        return dict(searches=st[0], narrowed=st[1], fallbacks=st[2], iterations=st[3])
+
     def __call__(self, points, fd=False, actions=True, angles=False, frequencies=False):
         """actions (n x 3: Jr, Jz, Jphi); with fd=True also the focal distance used for each point.
         With angles / frequencies (n x 3: theta_r, theta_z, theta_phi / Omega_r, Omega_z,

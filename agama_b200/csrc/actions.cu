@@ -3,6 +3,7 @@
 #include "fudge.cuh"
 #include "host_pipeline.h"
 #include "fudge_phases.h"
+#include "mlp.h"
 #include <algorithm>
 #include <mutex>
 #include <map>
@@ -81,7 +82,7 @@ template<bool FINDER>
 __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __grid_constant__ MultipoleView M,
     const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd,
     double fd0, FudgeRecord* __restrict__ rec, double* __restrict__ act, double* __restrict__ fdOut,
-    int* __restrict__ iters)
+    int* __restrict__ iters, float* __restrict__ features)
 {
     const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
     if(i >= n) return;
@@ -100,34 +101,60 @@ __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __g
     if(!r.valid) { act[3 * i] = a[0]; act[3 * i + 1] = a[1]; }
     if(fdOut) fdOut[i] = delta;
     if(iters) iters[i] = 0;
+    if(features) {
+        // inputs of the bracket predictor: the point's (R, z, vR, vz, vphi) with E and Lz in
+        // scale-free form -- ln r, |z| / r, velocities over the escape speed sqrt(-2 Phi) (so
+        // that E = Phi (1 - v^2 / v_esc^2) and Lz = R vphi follow), ln(Delta / r); symmetric
+        // under z -> -z and Lz -> -Lz like the limits themselves
+        const double r = fmax(sqrt(pc[0] * pc[0] + pc[1] * pc[1]), 1e-300), vesc = sqrt(fmax(-2 * Phi, 1e-300));
+        const float f[6] = { static_cast<float>(log(r)), static_cast<float>(fabs(pc[1]) / r),
+            static_cast<float>(pc[3] / vesc), static_cast<float>((pc[1] >= 0 ? pc[4] : -pc[4]) / vesc),
+            static_cast<float>(fabs(pc[5]) / vesc), static_cast<float>(log(fmax(delta, 1e-300) / r)) };
+        for(int k = 0; k < 6; k++) features[6 * i + k] = f[k];
+    }
 }
 
 /// the three phases over passes of at most POINTS_PER_PASS points (bounded scratch); with ang or
-/// freq the last phase also computes angles / frequencies (act may then be null)
+/// freq the last phase also computes angles / frequencies (act may then be null).  With a
+/// bracket predictor (bp), phase 1 also writes its inputs and the root searches start on its
+/// predictions; with samples, phase 3 is replaced by the predictor's training targets.
 template<bool FINDER>
 void runActions(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel, const double* fd,
-    double fd0, double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream)
+    double fd0, double* act, double* ang, double* freq, double* fdOut, int* iters, const BracketPlan* bp,
+    const BracketSamples* samples, cudaStream_t stream)
 {
     if(n <= 0) return;
     const GLRules& gl = glRulesForCurrentDevice();
     const long pass = std::min(n, POINTS_PER_PASS);
-    // records, two work counters, and the actions of a pass when the caller wants none
+    const bool predict = bp && bp->net;
+    // records, two work counters, the actions of a pass when the caller wants none, and the
+    // predictor's inputs and outputs
     const size_t recBytes = pass * sizeof(FudgeRecord) + 256;
-    Scratch scratch(recBytes + (act ? 0 : pass * 3 * sizeof(double)), stream);
+    const size_t actBytes = act ? 0 : pass * 3 * sizeof(double);
+    const size_t featBytes = (predict ? pass * 9 * sizeof(float) : 0) + 256;
+    Scratch scratch(recBytes + actBytes + featBytes, stream);
     FudgeRecord* rec = static_cast<FudgeRecord*>(scratch.ptr);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(rec + pass);
     double* actTmp = reinterpret_cast<double*>(static_cast<char*>(scratch.ptr) + recBytes);
+    float* feat = predict ? reinterpret_cast<float*>(static_cast<char*>(scratch.ptr) + recBytes + actBytes) : nullptr;
+    float* pred = predict ? feat + pass * 6 : nullptr;
     const bool angles = ang || freq;
+    BracketWidths widths{ { 0, 0, 0 } };
+    if(predict) for(int k = 0; k < 3; k++) widths.w[k] = bp->widths[k];
     for(long first = 0; first < n; first += pass) {
         const long count = std::min(pass, n - first);
         int* it = iters ? iters + first : nullptr;
         double* a = act ? act + 3 * first : actTmp;
+        float* f = samples ? samples->features + 6 * first : feat;
         fudgePrepareKernel<FINDER><<<(count + PREPARE_BLOCK - 1) / PREPARE_BLOCK, PREPARE_BLOCK, 0, stream>>>(
             M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, a,
-            fdOut ? fdOut + first : nullptr, it);
+            fdOut ? fdOut + first : nullptr, it, f);
         AGB_CUDA(cudaGetLastError());
-        launchFudgeRoots(M, count, rec, it, counter, stream);
-        if(angles)
+        if(predict) bp->net->predict(count, feat, pred, stream);
+        launchFudgeRoots(M, count, rec, it, counter, pred, widths, bp ? bp->stats : nullptr, stream);
+        if(samples)
+            launchBracketTargets(count, rec, samples->target + 3 * first, samples->mask + 3 * first, stream);
+        else if(angles)
             launchFudgeAngles(M, gl, count, rec, a, ang ? ang + 3 * first : nullptr,
                 freq ? freq + 3 * first : nullptr, stream);
         else
@@ -141,16 +168,24 @@ void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posve
     double* act, double* ang, double* freq, int* iters, cudaStream_t stream)
 {
     FudgeTables dummy{};
-    runActions<false>(M, dummy, n, posvel, fd, fd0, act, ang, freq, nullptr, iters, stream);
+    runActions<false>(M, dummy, n, posvel, fd, fd0, act, ang, freq, nullptr, iters, nullptr, nullptr, stream);
 }
 
 void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
-    double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream)
+    double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream, const BracketPlan* bp)
 {
-    runActions<true>(M, F, n, posvel, nullptr, 0, act, ang, freq, fdOut, iters, stream);
+    runActions<true>(M, F, n, posvel, nullptr, 0, act, ang, freq, fdOut, iters, bp, nullptr, stream);
+}
+
+void launchBracketSamples(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
+    const BracketSamples& samples, cudaStream_t stream)
+{
+    runActions<true>(M, F, n, posvel, nullptr, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, &samples, stream);
 }
 
 // ------------------------------------------------------------------------------------------
+
+DeviceActionFinder::~DeviceActionFinder() { delete brackets; }
 
 DeviceActionFinder* createDeviceActionFinder(DevicePotential* pot, const FinderTablesHost& T)
 {

@@ -7,6 +7,8 @@
 #include "mlp.h"
 #include "../../include/agama_b200.h"
 #include <cstring>
+#include <algorithm>
+#include <cmath>
 #include <sstream>
 #include <cctype>
 
@@ -332,6 +334,19 @@ extern "C" void agama_deleteActionFinder(agama_ActionFinder* a)
     delete a;
 }
 
+namespace {
+/// the bracket predictor of a finder when it is switched on, and its search counters (null when no
+/// predictor was ever trained)
+const BracketPlan* planOf(const DeviceActionFinder& F, BracketPlan& tmp)
+{
+    if(!F.bracketStats.ptr) return nullptr;     // no predictor trained: plain searches, no counters
+    tmp.net = F.useBrackets ? F.brackets : nullptr;
+    for(int k = 0; k < 3; k++) tmp.widths[k] = F.bracketWidths[k];
+    tmp.stats = F.bracketStats.ptr;
+    return &tmp;
+}
+}  // namespace
+
 extern "C" int agama_evalActionsAnglesFrequenciesManyDevice(const agama_ActionFinder* a, long n,
     const double* posvel, double* act, double* ang, double* freq, void* stream)
 {
@@ -339,8 +354,9 @@ extern "C" int agama_evalActionsAnglesFrequenciesManyDevice(const agama_ActionFi
         if(!a || n < 0 || (n > 0 && (!posvel || !(act || ang || freq))))
             throw std::invalid_argument("evalActionsAnglesFrequenciesManyDevice: invalid arguments");
         AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        BracketPlan plan;
         launchActionsFinder(a->af->pot->view, a->af->view, n, posvel, act, ang, freq, nullptr, nullptr,
-            static_cast<cudaStream_t>(stream));
+            static_cast<cudaStream_t>(stream), planOf(*a->af, plan));
     });
 }
 
@@ -356,9 +372,10 @@ extern "C" int agama_evalActionsAnglesFrequenciesMany(const agama_ActionFinder* 
         runChunked(n, { { posvel, 6 * sizeof(double) } },
             { { act, 3 * sizeof(double) }, { ang, 3 * sizeof(double) }, { freq, 3 * sizeof(double) } },
             [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                BracketPlan plan;
                 launchActionsFinder(F.pot->view, F.view, count, static_cast<const double*>(in[0]),
                     static_cast<double*>(out[0]), static_cast<double*>(out[1]), static_cast<double*>(out[2]),
-                    nullptr, nullptr, s);
+                    nullptr, nullptr, s, planOf(F, plan));
             });
     });
 }
@@ -369,8 +386,9 @@ extern "C" int agama_evalActionsManyDevice(const agama_ActionFinder* a, long n, 
     return guarded([&] {
         if(!a || n < 0 || (n > 0 && (!posvel || !act))) throw std::invalid_argument("evalActionsManyDevice: invalid arguments");
         AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        BracketPlan plan;
         launchActionsFinder(a->af->pot->view, a->af->view, n, posvel, act, nullptr, nullptr, fdOut, nullptr,
-            static_cast<cudaStream_t>(stream));
+            static_cast<cudaStream_t>(stream), planOf(*a->af, plan));
     });
 }
 
@@ -384,8 +402,10 @@ extern "C" int agama_evalActionsMany(const agama_ActionFinder* a, long n, const 
         const DeviceActionFinder& F = *a->af;
         runChunked(n, { { posvel, 6 * sizeof(double) } }, { { act, 3 * sizeof(double) }, { fdOut, sizeof(double) } },
             [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                BracketPlan plan;
                 launchActionsFinder(F.pot->view, F.view, count, static_cast<const double*>(in[0]),
-                    static_cast<double*>(out[0]), nullptr, nullptr, static_cast<double*>(out[1]), nullptr, s);
+                    static_cast<double*>(out[0]), nullptr, nullptr, static_cast<double*>(out[1]), nullptr, s,
+                    planOf(F, plan));
             });
     });
 }
@@ -491,6 +511,107 @@ extern "C" int agama_gemmBf16Device(int M, int N, int K, const void* A, const vo
             throw std::invalid_argument("gemmBf16Device: invalid arguments");
         requireDevice();
         launchGemmBf16(M, N, K, A, B, C, ldc, accumulate != 0, static_cast<cudaStream_t>(stream));
+    });
+}
+
+// ------------------------------------------------------------------------------------------
+// the bracket predictor of an action finder
+
+extern "C" int agama_actionFinderBracketSamples(const agama_ActionFinder* a, long n, const double* posvel,
+    float* features, float* target, float* mask)
+{
+    return guarded([&] {
+        if(!a || n <= 0 || !posvel || !features || !target || !mask)
+            throw std::invalid_argument("actionFinderBracketSamples: invalid arguments");
+        AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        DevBuf<double> dpv(6 * n);
+        DevBuf<float> f(6 * n), t(3 * n), m(3 * n);
+        AGB_CUDA(cudaMemcpy(dpv.ptr, posvel, sizeof(double) * 6 * n, cudaMemcpyHostToDevice));
+        launchBracketSamples(a->af->pot->view, a->af->view, n, dpv.ptr, BracketSamples{ f.ptr, t.ptr, m.ptr }, 0);
+        AGB_CUDA(cudaMemcpy(features, f.ptr, sizeof(float) * 6 * n, cudaMemcpyDeviceToHost));
+        AGB_CUDA(cudaMemcpy(target, t.ptr, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+        AGB_CUDA(cudaMemcpy(mask, m.ptr, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+    });
+}
+
+extern "C" int agama_actionFinderTrainBrackets(agama_ActionFinder* a, long n, const double* posvel, int epochs,
+    int batch, float lr, unsigned long long seed, float* lossHistory, float* widths)
+{
+    return guarded([&] {
+        if(!a || n < 1024 || !posvel || epochs < 1) throw std::invalid_argument("actionFinderTrainBrackets: invalid arguments");
+        DeviceActionFinder& F = *a->af;
+        AGB_CUDA(cudaSetDevice(F.pot->device));
+        // inputs and targets of every sample from the plain root searches
+        DevBuf<double> dpv(6 * n);
+        DevBuf<float> f(6 * n), t(3 * n), m(3 * n);
+        AGB_CUDA(cudaMemcpy(dpv.ptr, posvel, sizeof(double) * 6 * n, cudaMemcpyHostToDevice));
+        launchBracketSamples(F.pot->view, F.view, n, dpv.ptr, BracketSamples{ f.ptr, t.ptr, m.ptr }, 0);
+        AGB_CUDA(cudaDeviceSynchronize());
+        // train on the first 90 %, size the brackets on the held-out 10 %
+        const long nVal = std::max(128L, n / 10), nTrain = n - nVal;
+        Mlp* net = new Mlp(seed);
+        try {
+            const std::vector<float> hist = net->train(nTrain, f.ptr, t.ptr, m.ptr, epochs, batch, lr, seed + 1, 0);
+            if(lossHistory) for(size_t k = 0; k < hist.size(); k++) lossHistory[k] = hist[k];
+            DevBuf<float> y(3 * nVal);
+            net->predict(nVal, f.ptr + 6 * nTrain, y.ptr, 0);
+            AGB_CUDA(cudaDeviceSynchronize());
+            net->checkError();
+            std::vector<float> hy(3 * nVal), ht(3 * nVal), hm(3 * nVal);
+            AGB_CUDA(cudaMemcpy(hy.data(), y.ptr, sizeof(float) * 3 * nVal, cudaMemcpyDeviceToHost));
+            AGB_CUDA(cudaMemcpy(ht.data(), t.ptr + 3 * nTrain, sizeof(float) * 3 * nVal, cudaMemcpyDeviceToHost));
+            AGB_CUDA(cudaMemcpy(hm.data(), m.ptr + 3 * nTrain, sizeof(float) * 3 * nVal, cudaMemcpyDeviceToHost));
+            float w[3];
+            for(int k = 0; k < 3; k++) {
+                // half-width: twice the 95th percentile of the held-out error (at least 1e-4): the
+                // few percent of searches that miss fall back to the plain bracket
+                std::vector<float> e;
+                for(long i = 0; i < nVal; i++)
+                    if(hm[3 * i + k] > 0 && std::isfinite(hy[3 * i + k])) e.push_back(std::fabs(hy[3 * i + k] - ht[3 * i + k]));
+                float q = 1;
+                if(!e.empty()) {
+                    const size_t at = std::min(e.size() - 1, static_cast<size_t>(0.95 * e.size()));
+                    std::nth_element(e.begin(), e.begin() + at, e.end());
+                    q = e[at];
+                }
+                w[k] = std::max(2 * q, 1e-4f);
+            }
+            delete F.brackets;
+            F.brackets = net;
+            for(int k = 0; k < 3; k++) F.bracketWidths[k] = w[k];
+            if(widths) for(int k = 0; k < 3; k++) widths[k] = w[k];
+            F.useBrackets = true;
+            if(!F.bracketStats.ptr) F.bracketStats.alloc(4);
+            AGB_CUDA(cudaMemset(F.bracketStats.ptr, 0, 4 * sizeof(unsigned long long)));
+        } catch(...) {
+            delete net;
+            throw;
+        }
+    });
+}
+
+extern "C" int agama_actionFinderUseBrackets(agama_ActionFinder* a, int on)
+{
+    return guarded([&] {
+        if(!a) throw std::invalid_argument("actionFinderUseBrackets: null finder");
+        if(on && !a->af->brackets) throw std::invalid_argument("actionFinderUseBrackets: no bracket predictor trained");
+        a->af->useBrackets = on != 0;
+    });
+}
+
+extern "C" int agama_actionFinderBracketStats(agama_ActionFinder* a, long long* stats, int reset)
+{
+    return guarded([&] {
+        if(!a || !stats) throw std::invalid_argument("actionFinderBracketStats: invalid arguments");
+        DeviceActionFinder& F = *a->af;
+        unsigned long long h[4] = { 0, 0, 0, 0 };
+        if(F.bracketStats.ptr) {
+            AGB_CUDA(cudaSetDevice(F.pot->device));
+            AGB_CUDA(cudaDeviceSynchronize());
+            AGB_CUDA(cudaMemcpy(h, F.bracketStats.ptr, sizeof(h), cudaMemcpyDeviceToHost));
+            if(reset) AGB_CUDA(cudaMemset(F.bracketStats.ptr, 0, sizeof(h)));
+        }
+        for(int k = 0; k < 4; k++) stats[k] = static_cast<long long>(h[k]);
     });
 }
 

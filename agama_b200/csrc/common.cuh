@@ -301,8 +301,15 @@ struct RootSearch {
 
     AGB_HD double start(double xlower, double xupper, double reltol)
     {
+        return startAbs(xlower, xupper, fabs(xlower - xupper) * reltol);
+    }
+
+    /// the same search with its tolerance given directly (a bracket narrowed inside the original
+    /// one keeps the original bracket's tolerance)
+    AGB_HD double startAbs(double xlower, double xupper, double tol)
+    {
         a = xlower; b = xupper;
-        abstol = fabs(xlower - xupper) * reltol;
+        abstol = tol;
         iter = 0; phase = 0;
         return a;
     }

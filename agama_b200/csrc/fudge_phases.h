@@ -9,10 +9,19 @@ namespace agb {
 
 struct FudgeRecord;
 
+/// half-widths of the predicted brackets, in units of the predicted fractions (order of the ROOT_*
+/// kinds: nu_max, lambda_min, lambda_max)
+struct BracketWidths { float w[3]; };
+
 /// phase 2: the root searches of the integration limits, drained by a persistent grid from a
-/// device work counter (8 bytes, zeroed here on the stream)
+/// device work counter (8 bytes, zeroed here on the stream); with pred (n x 3 predictions) the
+/// searches start on the predicted brackets; stats (4 counters, may be null) accumulates
+/// searches, narrowed searches, fallbacks to the plain bracket and iterations
 void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, unsigned long long* counter,
-    cudaStream_t stream);
+    const float* pred, const BracketWidths& widths, unsigned long long* stats, cudaStream_t stream);
+
+/// training targets of the bracket predictor from records whose plain searches are done
+void launchBracketTargets(long n, const FudgeRecord* rec, float* target, float* mask, cudaStream_t stream);
 
 /// phase 3: Jr and Jz of every valid record into act[3 i], act[3 i + 1], drained by a persistent
 /// grid from a device work counter (8 bytes, zeroed here on the stream)

@@ -15,20 +15,29 @@ namespace {
 constexpr int ROOT_BLOCK = 128;
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
-/// Phase 2: every root search of the integration limits (task t = kind * n + i for the kinds
-/// nu_max, lambda_min, lambda_max of point i) drained from one work counter by a persistent grid.
-/// Each lane runs one search as a RootSearch state machine and takes the next task as soon as
-/// its search ends, so that the lanes of a warp meet at one potential evaluation per step instead
-/// of waiting for the warp's longest search.
+/** Phase 2: every root search of the integration limits (task t = kind * n + i for the kinds
+    nu_max, lambda_min, lambda_max of point i) drained from one work counter by a persistent grid.
+    Each lane runs one search as a RootSearch state machine and takes the next task as soon as
+    its search ends, so that the lanes of a warp meet at one potential evaluation per step instead
+    of waiting for the warp's longest search.
+
+    With bracket predictions (pred != null: per point, in the order of the kinds, the fractions
+    (nu_max - |nu|)/(D2 - |nu|), (lambda_min - D2)/(lambda - D2), (lambda - D2)/(lambda_max - D2),
+    all in [0, 1]) a search first runs
+    on the predicted bracket (t -+ width, inside the plain bracket) with the plain bracket's
+    tolerance; when that bracket holds no sign change the plain search takes over.  stats (may be
+    null) accumulates {searches, narrowed, fallbacks, iterations}. */
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
-    FudgeRecord* __restrict__ rec, int* __restrict__ iters, unsigned long long* __restrict__ counter)
+    FudgeRecord* __restrict__ rec, int* __restrict__ iters, unsigned long long* __restrict__ counter,
+    const float* __restrict__ pred, const BracketWidths widths, unsigned long long* __restrict__ stats)
 {
     const long total = 3 * n;
     const unsigned lane = threadIdx.x & 31;
-    bool busy = false, drained = false;
+    bool busy = false, drained = false, narrow = false;
     long point = 0;
     int kind = 0;
-    double x = 0, u0 = 0;
+    double x = 0, u0 = 0, plainLo = 0, plainHi = 0, tol = 0;
+    unsigned long long nSearch = 0, nNarrow = 0, nFallback = 0, nIter = 0;
     FudgeFunction fnc;
     RootSearch s;
     while(true) {
@@ -52,9 +61,48 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         kind = 1 << k;
                         loadFudgeFunction(M, r, fnc);
                         u0 = r.lambdaPos;
-                        x = kind == ROOT_NU_MAX ? s.start(fabs(r.nu), r.nuUpper, FUDGE_ACCURACY_RANGE) :
-                            kind == ROOT_LAMBDA_MIN ? s.start(r.lambdaLower, r.lambdaPos, FUDGE_ACCURACY_RANGE) :
-                            s.start(0, 1, FUDGE_ACCURACY_RANGE);
+                        plainLo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
+                        plainHi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
+                        tol = fabs(plainLo - plainHi) * FUDGE_ACCURACY_RANGE;
+                        double lo = plainLo, hi = plainHi;
+                        narrow = false;
+                        // points predicted near the focal line (nu_max bracket reaching D2, or the
+                        // lambda_min bracket reaching D2) keep the plain searches for all limits:
+                        // there the GL action integrals resolve the integrands poorly and depend
+                        // on the limits to the last bits of the plain searches
+                        const bool nearFocal = pred && (pred[3 * i] + widths.w[0] >= 1 || pred[3 * i + 1] - widths.w[1] <= 0);
+                        if(pred && !nearFocal) {
+                            const double tp = pred[3 * i + k], w = widths.w[k];
+                            double nlo, nhi;
+                            const double lmd = r.lambda - r.D2;
+                            if(kind == ROOT_NU_MAX) {
+                                const double span = r.D2 - fabs(r.nu);
+                                nlo = fabs(r.nu) + (tp - w) * span;
+                                nhi = fabs(r.nu) + (tp + w) * span;
+                            } else if(kind == ROOT_LAMBDA_MIN) {
+                                nlo = r.D2 + (tp - w) * lmd;
+                                nhi = r.D2 + (tp + w) * lmd;
+                            } else {                    // in the semi-infinite scaling about lambda_pos
+                                const double L0 = log(fmax(r.D2 + lmd / (tp + w), u0) / u0);
+                                nlo = L0 / (1 + L0);
+                                if(tp - w > 0) {
+                                    const double L1 = log(fmax(r.D2 + lmd / (tp - w), u0) / u0);
+                                    nhi = L1 / (1 + L1);
+                                } else
+                                    nhi = plainHi;
+                            }
+                            // only a bracket strictly inside the plain one: a prediction that reaches a
+                            // plain end (limits near the focal line lambda = nu = D2, or lambda_max
+                            // far out) leaves the search to the plain bracket, where the limit
+                            // is only fixed to the tolerance of the plain search and the actions
+                            // follow that search's own path
+                            if(isFinite(nlo) && isFinite(nhi) && nlo > plainLo && nhi < plainHi && nlo < nhi) {
+                                lo = nlo; hi = nhi; narrow = true;
+                            }
+                        }
+                        x = s.startAbs(lo, hi, tol);
+                        nSearch++;
+                        nNarrow += narrow;
                         busy = true;
                     }
                 }
@@ -65,14 +113,50 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
             double fx, dx;
             limitRootEval(fnc, kind, u0, x, &fx, &dx);
             if(s.feed(fx, dx, &x)) {
-                busy = false;
-                FudgeRecord& r = rec[point];
-                if(kind == ROOT_NU_MAX) r.nuMax = isFinite(s.result) ? s.result : fabs(fnc.nu);
-                else if(kind == ROOT_LAMBDA_MIN) r.lambdaMin = s.result;
-                else r.lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
-                if(iters) atomicAdd(iters + point, s.iter);
+                nIter += s.iter;
+                if(narrow && !isFinite(s.result)) {     // the predicted bracket missed: plain search
+                    narrow = false;
+                    nFallback++;
+                    x = s.startAbs(plainLo, plainHi, tol);
+                } else {
+                    busy = false;
+                    FudgeRecord& r = rec[point];
+                    if(kind == ROOT_NU_MAX) r.nuMax = isFinite(s.result) ? s.result : fabs(fnc.nu);
+                    else if(kind == ROOT_LAMBDA_MIN) r.lambdaMin = s.result;
+                    else r.lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
+                    if(iters) atomicAdd(iters + point, s.iter);
+                }
             }
         }
+    }
+    if(stats) {     // one atomic per warp and counter
+        nSearch = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nSearch));
+        nNarrow = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nNarrow));
+        nFallback = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nFallback));
+        nIter = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nIter));
+        if(lane == 0) {
+            atomicAdd(stats, nSearch);
+            atomicAdd(stats + 1, nNarrow);
+            atomicAdd(stats + 2, nFallback);
+            atomicAdd(stats + 3, nIter);
+        }
+    }
+}
+
+/// bracket-predictor training targets of the records (after the plain searches), as described at
+/// fudgeRootKernel, and a 0/1 mask of the searched limits
+__global__ void bracketTargetKernel(long n, const FudgeRecord* __restrict__ rec, float* __restrict__ target,
+    float* __restrict__ mask)
+{
+    const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    if(i >= n) return;
+    const FudgeRecord r = rec[i];
+    const double lmd = r.lambda - r.D2, span = r.D2 - fabs(r.nu);
+    const double t[3] = { (r.nuMax - fabs(r.nu)) / span, (r.lambdaMin - r.D2) / lmd, lmd / (r.lambdaMax - r.D2) };
+    for(int k = 0; k < 3; k++) {
+        const bool ok = r.valid && (r.roots & (1 << k)) && isFinite(t[k]);
+        target[3 * i + k] = ok ? static_cast<float>(t[k]) : 0.f;
+        mask[3 * i + k] = ok ? 1.f : 0.f;
     }
 }
 
@@ -97,12 +181,19 @@ int rootGridSize()
 }  // namespace
 
 void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, unsigned long long* counter,
-    cudaStream_t stream)
+    const float* pred, const BracketWidths& widths, unsigned long long* stats, cudaStream_t stream)
 {
     if(n <= 0) return;
     AGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
     const long grid = std::min<long>(rootGridSize(), (3 * n + ROOT_BLOCK - 1) / ROOT_BLOCK);
-    fudgeRootKernel<<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, iters, counter);
+    fudgeRootKernel<<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, iters, counter, pred, widths, stats);
+    AGB_CUDA(cudaGetLastError());
+}
+
+void launchBracketTargets(long n, const FudgeRecord* rec, float* target, float* mask, cudaStream_t stream)
+{
+    if(n <= 0) return;
+    bracketTargetKernel<<<(n + 255) / 256, 256, 0, stream>>>(n, rec, target, mask);
     AGB_CUDA(cudaGetLastError());
 }
 

@@ -58,12 +58,19 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
 
 struct OrbitParams;
 
+struct Mlp;
+
 /// a Staeckel-fudge action finder: tables on the device of its potential
 struct DeviceActionFinder {
     DevicePotential* pot = nullptr;   // not owned
     FinderTablesHost host;
     DevBuf<double> gridE, gridL, delta, lofe, rofl, phiofr;
     FudgeTables view;
+    Mlp* brackets = nullptr;          // owned; null until a predictor is trained
+    float bracketWidths[3] = { 0, 0, 0 };
+    bool useBrackets = false;
+    DevBuf<unsigned long long> bracketStats;
+    ~DeviceActionFinder();
 };
 DeviceActionFinder* createDeviceActionFinder(DevicePotential* pot, const FinderTablesHost& T);
 /// build the focal-distance table and the L_circ interpolator of a potential (finder_build.cu)
@@ -85,8 +92,19 @@ int noallocQueueSlots();
 /// outputs n x 3 each: actions (Jr, Jz, Jphi), angles and frequencies (any of them may be null)
 void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
     double* act, double* ang, double* freq, int* iters, cudaStream_t stream);
-/// Staeckel fudge with the focal distance from the action finder's table
+/// a trained bracket predictor attached to an action finder: the network, the half-widths of its
+/// brackets (nu_max, lambda_min, lambda_max; see fudgeRootKernel) and 4 device counters
+/// {searches, narrowed, fallbacks, iterations} (may be null)
+struct BracketPlan { const Mlp* net; float widths[3]; unsigned long long* stats; };
+/// outputs of launchBracketSamples (device arrays n x 6, n x 3, n x 3)
+struct BracketSamples { float* features; float* target; float* mask; };
+
+/// Staeckel fudge with the focal distance from the action finder's table (bp: optional predictor)
 void launchActionsFinder(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
-    double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream);
+    double* act, double* ang, double* freq, double* fdOut, int* iters, cudaStream_t stream,
+    const BracketPlan* bp = nullptr);
+/// the predictor's inputs and training targets of n points (plain root searches)
+void launchBracketSamples(const MultipoleView& M, const FudgeTables& F, long n, const double* posvel,
+    const BracketSamples& samples, cudaStream_t stream);
 
 }  // namespace agb

@@ -195,6 +195,33 @@ int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential
     const double* posvel, const double* fd, double fd0, double* act, double* ang, double* freq, void* stream);
 
 /* ---------------------------------------------------------------------------------------
+   Learned root brackets of the action finder (no reference counterpart): a network trained on the
+   finder's own root searches predicts nu_max, lambda_min and lambda_max of each point; the
+   searches then start on the predicted bracket (strictly inside the plain one, with the plain
+   bracket's tolerance) and fall back to the plain bracket when the prediction holds no sign
+   change; points predicted near the focal line keep the plain searches, so the actions keep the
+   finder's accuracy (1e-6 of the plain searches' actions).
+
+   agama_actionFinderBracketSamples: the network's inputs (n x 6: the point's E, Lz, R, z, vR, vz
+   in scale-free form: ln r, |z|/r, vR/v_esc, vz sign(z)/v_esc, |vphi|/v_esc with v_esc =
+   sqrt(-2 Phi), ln(Delta/r)) and targets (n x 3, fractions in [0, 1]: (nu_max - |nu|)/(Delta^2 -
+   |nu|), (lambda_min - Delta^2)/(lambda - Delta^2), (lambda - Delta^2)/(lambda_max - Delta^2))
+   with 0/1 masks of the limits that needed a search, from the plain searches of n points (host
+   buffers).
+   agama_actionFinderTrainBrackets: trains a new network on n points (90 % training, 10 % to size
+   the brackets: half-width = twice the 95th percentile of the held-out error, reported in
+   widths[3]), attaches it and switches it on; lossHistory (epochs floats) may be NULL.
+   agama_actionFinderUseBrackets: switches the trained predictor on or off.
+   agama_actionFinderBracketStats: {root searches, searches on a predicted bracket, fallbacks to
+   the plain bracket, root-finder iterations} since the last reset. */
+int agama_actionFinderBracketSamples(const agama_ActionFinder* actionFinder, long n, const double* posvel,
+    float* features, float* target, float* mask);
+int agama_actionFinderTrainBrackets(agama_ActionFinder* actionFinder, long n, const double* posvel, int epochs,
+    int batch, float lr, unsigned long long seed, float* lossHistory, float* widths);
+int agama_actionFinderUseBrackets(agama_ActionFinder* actionFinder, int on);
+int agama_actionFinderBracketStats(agama_ActionFinder* actionFinder, long long* stats, int reset);
+
+/* ---------------------------------------------------------------------------------------
    Tensor-core GEMM of the bracket-predictor network (no reference counterpart; the reference has
    no learned part): C[M x N] (FP32, leading dimension ldc) = A[M x K] * B[N x K]^T, plus the old C
    when accumulate is non-zero.  A and B are BF16 row-major with K contiguous, device pointers

@@ -1,0 +1,50 @@
+"""Learned root brackets of the action finder (the config-4 form: the config-1 potential made
+axisymmetric, trained on its own distribution): the network is trained on the finder's own root
+searches, the searches start on its brackets and fall back to the plain ones when a prediction
+misses.  The actions must stay those of the plain searches (1e-6) and of the reference (golden
+vectors), and the network must save root-finder iterations."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from test_actions_gpu import check_actions
+
+pytestmark = pytest.mark.gpu
+
+
+def _config1_points(n, seed):
+    import agama_b200
+    from agama_b200 import workloads
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg4.coef"))
+    pos = workloads.dehnen_positions(n, 1.0, q=(0.8, 0.6), seed=seed)
+    return pot, workloads.orbit_ics(pos, pot.potential, seed=seed + 1000)
+
+
+def test_learned_brackets_keep_the_actions_and_save_iterations():
+    import agama_b200
+    pot, train = _config1_points(1000000, 5)
+    _, evalpts = _config1_points(100000, 55)
+    af = agama_b200.ActionFinder(pot)
+    hist, widths = af.train_brackets(train, epochs=20, batch=2048, lr=2e-3, seed=1)
+    print('loss per epoch', hist)
+    assert hist[-1] < 0.2 * hist[0], hist
+    af.use_brackets(False)
+    af.bracket_stats(reset=True)
+    J0 = af(evalpts)
+    plain = af.bracket_stats(reset=True)
+    af.use_brackets(True)
+    J1 = af(evalpts)
+    learned = af.bracket_stats(reset=True)
+    print("bracket half-widths", widths, "loss", hist[0], "->", hist[-1])
+    print("plain", plain, "learned", learned)
+    check_actions(J1, J0)
+    # the network saves root-finder iterations: searches start on its brackets for most points,
+    # a few percent of them miss and fall back
+    assert learned["searches"] == plain["searches"] and learned["narrowed"] > 0.4 * learned["searches"]
+    assert learned["fallbacks"] < 0.03 * learned["narrowed"]
+    assert learned["iterations"] < 0.8 * plain["iterations"]
+    # the reference's actions of the golden points (disk-like: partly outside the training set)
+    g = np.load(os.path.join(GOLDEN, "actions_cfg4.npz"))
+    check_actions(af(g["points"]), g["act_finder"])
