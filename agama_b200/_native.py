@@ -38,6 +38,7 @@ SIGNATURES = {
     "agama_actionFinderBracketSamples": (ctypes.c_int, [VP, ctypes.c_long, D, F, F, F]),
     "agama_actionFinderTrainBrackets": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_int, ctypes.c_int,
                                                        ctypes.c_float, ctypes.c_ulonglong, F, F]),
+    "agama_actionFinderPredictBrackets": (ctypes.c_int, [VP, ctypes.c_long, F, F]),
     "agama_actionFinderUseBrackets": (ctypes.c_int, [VP, ctypes.c_int]),
     "agama_actionFinderBracketStats": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     "agama_mlpCreate": (VP, [ctypes.c_ulonglong]),

@@ -95,6 +95,13 @@ class ActionFinder:
                                                             int(seed), ptr(hist, _native.F), ptr(w, _native.F)))
         return hist, w
 
+    def predict_brackets(self, features):
+        """the trained network's predictions (n x 3) for inputs as returned by bracket_samples"""
+        f = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 6)
+        y = np.empty((len(f), 3), dtype=np.float32)
+        check(_native.lib().agama_actionFinderPredictBrackets(self._h, len(f), ptr(f, _native.F), ptr(y, _native.F)))
+        return y
+
     def use_brackets(self, on=True):
         check(_native.lib().agama_actionFinderUseBrackets(self._h, 1 if on else 0))
 

@@ -590,6 +590,23 @@ extern "C" int agama_actionFinderTrainBrackets(agama_ActionFinder* a, long n, co
     });
 }
 
+extern "C" int agama_actionFinderPredictBrackets(const agama_ActionFinder* a, long n, const float* features,
+    float* prediction)
+{
+    return guarded([&] {
+        if(!a || n < 0 || (n > 0 && (!features || !prediction)))
+            throw std::invalid_argument("actionFinderPredictBrackets: invalid arguments");
+        if(!a->af->brackets) throw std::invalid_argument("actionFinderPredictBrackets: no bracket predictor trained");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(a->af->pot->device));
+        DevBuf<float> f(6 * n), y(3 * n);
+        AGB_CUDA(cudaMemcpy(f.ptr, features, sizeof(float) * 6 * n, cudaMemcpyHostToDevice));
+        a->af->brackets->predict(n, f.ptr, y.ptr, 0);
+        AGB_CUDA(cudaMemcpy(prediction, y.ptr, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+        a->af->brackets->checkError();
+    });
+}
+
 extern "C" int agama_actionFinderUseBrackets(agama_ActionFinder* a, int on)
 {
     return guarded([&] {

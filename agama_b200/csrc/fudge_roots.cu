@@ -25,18 +25,20 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
     (nu_max - |nu|)/(D2 - |nu|), (lambda_min - D2)/(lambda - D2), (lambda - D2)/(lambda_max - D2),
     all in [0, 1]) a search first runs
     on the predicted bracket (t -+ width, inside the plain bracket) with the plain bracket's
-    tolerance; when that bracket holds no sign change the plain search takes over.  stats (may be
-    null) accumulates {searches, narrowed, fallbacks, iterations}. */
+    tolerance; when that bracket holds no sign change the plain search takes over, and a lambda_max
+    found on a predicted bracket is accepted only if F is still negative half-way (in the scaled
+    variable) from it to infinity.  stats (may be null) accumulates {searches, narrowed,
+    fallbacks, iterations}. */
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
     FudgeRecord* __restrict__ rec, int* __restrict__ iters, unsigned long long* __restrict__ counter,
     const float* __restrict__ pred, const BracketWidths widths, unsigned long long* __restrict__ stats)
 {
     const long total = 3 * n;
     const unsigned lane = threadIdx.x & 31;
-    bool busy = false, drained = false, narrow = false;
+    bool busy = false, drained = false, narrow = false, verifying = false;
     long point = 0;
     int kind = 0;
-    double x = 0, u0 = 0, plainLo = 0, plainHi = 0, tol = 0;
+    double x = 0, u0 = 0, plainLo = 0, plainHi = 0, tol = 0, verified = 0;
     unsigned long long nSearch = 0, nNarrow = 0, nFallback = 0, nIter = 0;
     FudgeFunction fnc;
     RootSearch s;
@@ -112,12 +114,31 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
         if(busy) {
             double fx, dx;
             limitRootEval(fnc, kind, u0, x, &fx, &dx);
-            if(s.feed(fx, dx, &x)) {
+            if(verifying) {
+                // lambda_max from a predicted bracket: F must stay negative half-way (in the
+                // scaled variable) from the root to infinity; otherwise F has more roots beyond
+                // and the plain search, which may end on any of them, decides
+                verifying = false;
+                nIter++;
+                if(fx < 0) {
+                    busy = false;
+                    rec[point].lambdaMax = unscaleSemiInf(u0, verified, nullptr);
+                    if(iters) atomicAdd(iters + point, s.iter + 1);
+                } else {
+                    narrow = false;
+                    nFallback++;
+                    x = s.startAbs(plainLo, plainHi, tol);
+                }
+            } else if(s.feed(fx, dx, &x)) {
                 nIter += s.iter;
                 if(narrow && !isFinite(s.result)) {     // the predicted bracket missed: plain search
                     narrow = false;
                     nFallback++;
                     x = s.startAbs(plainLo, plainHi, tol);
+                } else if(narrow && kind == ROOT_LAMBDA_MAX) {
+                    verifying = true;
+                    verified = s.result;
+                    x = 0.5 * (s.result + 1);
                 } else {
                     busy = false;
                     FudgeRecord& r = rec[point];

@@ -27,8 +27,10 @@ constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + H * NIN, OFF_W2 = OFF_B1 + H, OFF_B2
     NPARAM = OFF_B4 + NOUT;
 static_assert(NPARAM == MLP_NUM_PARAMS, "parameter layout");
 
-__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
-__device__ __forceinline__ float dsilu(float z) { const float s = 1.f / (1.f + __expf(-z)); return s * (1.f + z * (1.f - s)); }
+/// SiLU z sigma(z) and its derivative, with the fast exponential and division of the special
+/// function unit (relative error ~1e-6: far below the BF16 rounding of the activations)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) { const float s = __fdividef(1.f, 1.f + __expf(-z)); return s * (1.f + z * (1.f - s)); }
 
 // ---------------------------------------------------------------- elementwise training kernels
 
@@ -226,15 +228,18 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
     extern __shared__ unsigned char smemRaw[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmemBase;
-    __shared__ float sW1[H * NIN], sB1[H], sB2[H], sB3[H], sW4[NOUT * H], sB4[NOUT], sScale[2 * NIN + 2 * NOUT];
+    __shared__ __align__(16) float sW1T[NIN][H];            // layer-1 weights, transposed
+    __shared__ __align__(16) float sW4T[H][4];               // layer-4 weights [unit][output], padded
+    __shared__ __align__(16) float sB1[H], sB2[H], sB3[H];
+    __shared__ float sB4[NOUT], sScale[2 * NIN + 2 * NOUT];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
     unsigned char* tW2 = base;
     unsigned char* tW3 = base + H * H * 2;
     unsigned char* tA = base + 2 * H * H * 2;
     const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
 
-    for(int k = tid; k < H * NIN; k += 128) sW1[k] = p[OFF_W1 + k];
-    for(int k = tid; k < NOUT * H; k += 128) sW4[k] = p[OFF_W4 + k];
+    for(int k = tid; k < H * NIN; k += 128) sW1T[k % NIN][k / NIN] = p[OFF_W1 + k];
+    for(int k = tid; k < H * 4; k += 128) sW4T[k / 4][k % 4] = k % 4 < NOUT ? p[OFF_W4 + (k % 4) * H + k / 4] : 0.f;
     for(int k = tid; k < H; k += 128) { sB1[k] = p[OFF_B1 + k]; sB2[k] = p[OFF_B2 + k]; sB3[k] = p[OFF_B3 + k]; }
     if(tid < NOUT) sB4[tid] = p[OFF_B4 + tid];
     if(tid < 2 * NIN + 2 * NOUT) sScale[tid] = scale[tid];
@@ -259,11 +264,16 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
 
     // write this thread's 128 activations (row tid of the tile) as BF16 in the canonical layout
     auto storeRow = [&](const float* h, int c0) {
-        // h holds 32 values for columns c0..c0+31: four 16-byte vectors
+        // h holds 32 values for columns c0..c0+31: four 16-byte vectors of 8 BF16
+#pragma unroll
         for(int q = 0; q < 4; q++) {
-            __align__(16) __nv_bfloat16 v[8];
-            for(int e = 0; e < 8; e++) v[e] = __float2bfloat16_rn(h[q * 8 + e]);
-            *reinterpret_cast<uint4*>(tA + umma::tileOffset(tid, c0 + q * 8, H)) = *reinterpret_cast<const uint4*>(v);
+            uint4 v;
+            __nv_bfloat162 p2[4];
+#pragma unroll
+            for(int e = 0; e < 4; e++) p2[e] = __floats2bfloat162_rn(h[q * 8 + 2 * e], h[q * 8 + 2 * e + 1]);
+            v.x = *reinterpret_cast<uint32_t*>(&p2[0]); v.y = *reinterpret_cast<uint32_t*>(&p2[1]);
+            v.z = *reinterpret_cast<uint32_t*>(&p2[2]); v.w = *reinterpret_cast<uint32_t*>(&p2[3]);
+            *reinterpret_cast<uint4*>(tA + umma::tileOffset(tid, c0 + q * 8, H)) = v;
         }
     };
     auto runLayer = [&](unsigned char* tW) {
@@ -290,10 +300,15 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
         for(int k = 0; k < NIN; k++) x[k] = valid ? (xin[i * NIN + k] - sScale[k]) / sScale[NIN + k] : 0.f;
         for(int c0 = 0; c0 < H; c0 += 32) {
             float h[32];
-            for(int c = 0; c < 32; c++) {
-                float s = sB1[c0 + c];
-                for(int k = 0; k < NIN; k++) s += x[k] * sW1[(c0 + c) * NIN + k];
-                h[c] = silu(s);
+#pragma unroll
+            for(int c = 0; c < 32; c += 4) {
+                float4 acc = *reinterpret_cast<const float4*>(&sB1[c0 + c]);
+#pragma unroll
+                for(int k = 0; k < NIN; k++) {
+                    const float4 w = *reinterpret_cast<const float4*>(&sW1T[k][c0 + c]);
+                    acc.x += x[k] * w.x; acc.y += x[k] * w.y; acc.z += x[k] * w.z; acc.w += x[k] * w.w;
+                }
+                h[c] = silu(acc.x); h[c + 1] = silu(acc.y); h[c + 2] = silu(acc.z); h[c + 3] = silu(acc.w);
             }
             storeRow(h, c0);
         }
@@ -302,7 +317,12 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
         for(int c0 = 0; c0 < H; c0 += 32) {
             float h[32];
             umma::tmemLoad32(tmemRow + c0, h);
-            for(int c = 0; c < 32; c++) h[c] = silu(h[c] + sB2[c0 + c]);
+#pragma unroll
+            for(int c = 0; c < 32; c += 4) {
+                const float4 b = *reinterpret_cast<const float4*>(&sB2[c0 + c]);
+                h[c] = silu(h[c] + b.x); h[c + 1] = silu(h[c + 1] + b.y);
+                h[c + 2] = silu(h[c + 2] + b.z); h[c + 3] = silu(h[c + 3] + b.w);
+            }
             storeRow(h, c0);
         }
         umma::fenceBeforeSync();
@@ -313,9 +333,11 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
         for(int c0 = 0; c0 < H; c0 += 32) {
             float h[32];
             umma::tmemLoad32(tmemRow + c0, h);
+#pragma unroll
             for(int c = 0; c < 32; c++) {
                 const float a = silu(h[c] + sB3[c0 + c]);
-                for(int j = 0; j < NOUT; j++) y[j] += a * sW4[j * H + c0 + c];
+                const float4 w = *reinterpret_cast<const float4*>(&sW4T[c0 + c][0]);
+                y[0] += a * w.x; y[1] += a * w.y; y[2] += a * w.z;
             }
         }
         if(valid)

@@ -265,6 +265,92 @@ def run_engine_secondary(dev, flush, dist, cpu):
     return out
 
 
+def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
+    """the actions with learned root brackets (BF16 tensor-core network choosing the brackets of
+    the FP64 searches) beside the plain FP64 form, config 2 (same 1e6 particles as the headline)
+    and config 4 (1e7 particles of the config-1 distribution in the config-1 potential made
+    axisymmetric, network trained on 2e6 of the finder's own searches)"""
+    import torch
+    import agama_b200
+    from agama_b200 import workloads
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, warmup=3, steps=5):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        t = float(np.mean(ms))
+        if dist:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    def rel_err(J, Jref):
+        J, Jref = J.cpu().numpy(), Jref.cpu().numpy()
+        ok = np.isfinite(Jref).all(1)
+        tot = np.abs(Jref[ok]).sum(1, keepdims=True)
+        e = np.abs(J[ok] - Jref[ok]) / np.maximum(np.abs(Jref[ok]), 1e-3 * tot)
+        return float(np.max(e)), float(np.quantile(e, 0.999))
+
+    out = []
+    vc2 = workloads.vcirc_from_force(lambda x: af2.potential.force(x))
+    train2 = workloads.disk_particles(1000000, vc2, seed=33)
+    t0 = time.perf_counter()
+    af2.train_brackets(train2, epochs=20, batch=2048, lr=2e-3, seed=1)
+    ttrain2 = time.perf_counter() - t0
+    cases = [("config 2: 1e6 disk particles (the headline set)", af2, dpts2, J2plain, ttrain2, 1000000)]
+    pot4 = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg4.coef"))
+    af4 = agama_b200.ActionFinder(pot4)
+    pos = workloads.dehnen_positions(2000000, 1.0, q=(0.8, 0.6), seed=workloads.SEEDS["particles4"])
+    train4 = workloads.orbit_ics(pos, pot4.potential, seed=workloads.SEEDS["particles4"] + 1000)
+    t0 = time.perf_counter()
+    af4.train_brackets(train4, epochs=20, batch=2048, lr=2e-3, seed=1)
+    ttrain4 = time.perf_counter() - t0
+    pos = workloads.dehnen_positions(10000000, 1.0, q=(0.8, 0.6), seed=workloads.SEEDS["particles4"] + 1)
+    ev4 = workloads.orbit_ics(pos, pot4.potential, seed=workloads.SEEDS["particles4"] + 2000)
+    d4 = torch.tensor(ev4, device=dev)
+    del pos, ev4
+    af4.use_brackets(False)
+    J4plain = af4(d4)
+    cases.append(("config 4: 1e7 particles of the config-1 distribution, config-1 potential made axisymmetric "
+                  "(lmax 6, 50 nodes)", af4, d4, J4plain, ttrain4, 2000000))
+    for name, af, d, Jplain, ttrain, ntrain in cases:
+        n = d.shape[0]
+        af.use_brackets(False)
+        tp = timed(lambda: af(d))
+        af.bracket_stats(reset=True)
+        af(d)
+        plain = af.bracket_stats(reset=True)
+        af.use_brackets(True)
+        tl = timed(lambda: af(d))
+        af.bracket_stats(reset=True)
+        J = af(d)
+        learned = af.bracket_stats(reset=True)
+        emax, e999 = rel_err(J, Jplain)
+        out.append({"metric": "actions/s", "mode": "learned root brackets (BF16 tcgen05 network + FP64 searches)",
+                    "value": n / (tl / 1000), "unit": "actions/s", "ms_per_step": tl, "config": name,
+                    "plain_fp64": {"value": n / (tp / 1000), "ms_per_step": tp},
+                    "speedup_vs_plain": tp / tl,
+                    "max_rel_err_vs_plain": emax, "rel_err_vs_plain_q999": e999,
+                    "narrowed_searches": learned["narrowed"] / max(1, learned["searches"]),
+                    "fallback_rate": learned["fallbacks"] / max(1, learned["narrowed"]),
+                    "root_iterations_vs_plain": learned["iterations"] / max(1, plain["iterations"]),
+                    "training": {"samples": ntrain, "epochs": 20, "seconds": ttrain},
+                    "steps": 5, "warmup": 3, "gpu_launches_per_step": 4})
+        af.use_brackets(False)
+    return out
+
+
 def reference_secondary(pts1, ic1, T1, ic3, T3):
     """the reference's own CPU code on bounded samples of the secondary workloads, all host cores"""
     try:
@@ -392,6 +478,8 @@ def run_engine(args):
             "cpu_baseline": None if args.no_baseline else cpu_baseline_line(pts),
         }
     secondary = None if args.no_secondary else run_engine_secondary(dev, flush, dist, rank == 0 and not args.no_baseline)
+    if not args.no_secondary:
+        secondary += run_bracket_modes(dev, flush, dist, af, dpts, act.clone())
     if rank == 0:
         if secondary is not None:
             line["secondary"] = secondary

@@ -218,6 +218,9 @@ int agama_actionFinderBracketSamples(const agama_ActionFinder* actionFinder, lon
     float* features, float* target, float* mask);
 int agama_actionFinderTrainBrackets(agama_ActionFinder* actionFinder, long n, const double* posvel, int epochs,
     int batch, float lr, unsigned long long seed, float* lossHistory, float* widths);
+/* the trained network's predictions (n x 3, in the target units above) for given inputs (n x 6) */
+int agama_actionFinderPredictBrackets(const agama_ActionFinder* actionFinder, long n, const float* features,
+    float* prediction);
 int agama_actionFinderUseBrackets(agama_ActionFinder* actionFinder, int on);
 int agama_actionFinderBracketStats(agama_ActionFinder* actionFinder, long long* stats, int reset);
 
