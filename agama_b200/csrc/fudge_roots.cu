@@ -25,10 +25,10 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
     (nu_max - |nu|)/(D2 - |nu|), (lambda_min - D2)/(lambda - D2), (lambda - D2)/(lambda_max - D2),
     all in [0, 1]) a search first runs
     on the predicted bracket (t -+ width, inside the plain bracket) with the plain bracket's
-    tolerance; when that bracket holds no sign change the plain search takes over, and a lambda_max
-    found on a predicted bracket is accepted only if F is still negative half-way (in the scaled
-    variable) from it to infinity.  stats (may be null) accumulates {searches, narrowed,
-    fallbacks, iterations}. */
+    tolerance; when that bracket holds no sign change the plain search takes over, and a root found
+    on a predicted bracket is accepted only if F is negative half-way from it to the plain end
+    where F is negative (one more evaluation).  stats (may be null) accumulates {searches,
+    narrowed, fallbacks, iterations}. */
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
     FudgeRecord* __restrict__ rec, int* __restrict__ iters, unsigned long long* __restrict__ counter,
     const float* __restrict__ pred, const BracketWidths widths, unsigned long long* __restrict__ stats)
@@ -68,11 +68,12 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         tol = fabs(plainLo - plainHi) * FUDGE_ACCURACY_RANGE;
                         double lo = plainLo, hi = plainHi;
                         narrow = false;
-                        // points predicted near the focal line (nu_max bracket reaching D2, or the
-                        // lambda_min bracket reaching D2) keep the plain searches for all limits:
+                        // points predicted near the focal line (nu_max or lambda_min within two
+                        // bracket half-widths of D2) keep the plain searches for all limits:
                         // there the GL action integrals resolve the integrands poorly and depend
                         // on the limits to the last bits of the plain searches
-                        const bool nearFocal = pred && (pred[3 * i] + widths.w[0] >= 1 || pred[3 * i + 1] - widths.w[1] <= 0);
+                        const bool nearFocal = pred && (pred[3 * i] + 2 * widths.w[0] >= 1 ||
+                                                        pred[3 * i + 1] - 2 * widths.w[1] <= 0);
                         if(pred && !nearFocal) {
                             const double tp = pred[3 * i + k], w = widths.w[k];
                             double nlo, nhi;
@@ -115,14 +116,19 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
             double fx, dx;
             limitRootEval(fnc, kind, u0, x, &fx, &dx);
             if(verifying) {
-                // lambda_max from a predicted bracket: F must stay negative half-way (in the
-                // scaled variable) from the root to infinity; otherwise F has more roots beyond
-                // and the plain search, which may end on any of them, decides
+                // a root from a predicted bracket: F must have the sign of the plain bracket's
+                // end half-way between the root and that end (lambda_max: towards infinity in the
+                // scaled variable; lambda_min: towards D2; nu_max: towards D2), where it is
+                // negative; otherwise F has more roots there and the plain search, which may end
+                // on any of them, decides
                 verifying = false;
                 nIter++;
                 if(fx < 0) {
                     busy = false;
-                    rec[point].lambdaMax = unscaleSemiInf(u0, verified, nullptr);
+                    FudgeRecord& r = rec[point];
+                    if(kind == ROOT_NU_MAX) r.nuMax = verified;
+                    else if(kind == ROOT_LAMBDA_MIN) r.lambdaMin = verified;
+                    else r.lambdaMax = unscaleSemiInf(u0, verified, nullptr);
                     if(iters) atomicAdd(iters + point, s.iter + 1);
                 } else {
                     narrow = false;
@@ -135,10 +141,10 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                     narrow = false;
                     nFallback++;
                     x = s.startAbs(plainLo, plainHi, tol);
-                } else if(narrow && kind == ROOT_LAMBDA_MAX) {
+                } else if(narrow) {
                     verifying = true;
                     verified = s.result;
-                    x = 0.5 * (s.result + 1);
+                    x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? plainLo : plainHi));
                 } else {
                     busy = false;
                     FudgeRecord& r = rec[point];
