@@ -26,6 +26,12 @@ SIGNATURES = {
     "agama_inspectMultipoleFile": (ctypes.c_int, [ctypes.c_char_p, I, I, I, I, I]),
     "agama_evalPotentialMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
     "agama_evalPotentialManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
+    "agama_setOrbitLanesPerOrbit": (ctypes.c_int, [ctypes.c_int]),
+    "agama_integrateOrbitsTrajectoryManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
+                                                                 ctypes.c_double, ctypes.c_long, ctypes.c_int, VP, VP,
+                                                                 VP, VP, VP]),
+    "agama_integrateOrbitsTrajectoryMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
+                                                           ctypes.c_long, ctypes.c_int, D, D, L, I]),
     "agama_integrateOrbitsMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_long, D, L, I]),
     "agama_integrateOrbitsManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,

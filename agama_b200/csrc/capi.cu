@@ -186,6 +186,15 @@ OrbitParams makeOrbitParams(double Omega, double accuracy, long maxNumSteps)
 }
 }  // namespace
 
+extern "C" int agama_setOrbitLanesPerOrbit(int lanes)
+{
+    return guarded([&] {
+        if(!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8))
+            throw std::invalid_argument("setOrbitLanesPerOrbit: lanes must be 0 (autotuned), 1, 2, 4 or 8");
+        setOrbitLanes(lanes);
+    });
+}
+
 extern "C" int agama_integrateOrbitsManyDevice(const agama_Potential* p, long n, const double* ic,
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, long* numRejected, int* status, int useQueue, void* stream)
@@ -201,6 +210,50 @@ extern "C" int agama_integrateOrbitsManyDevice(const agama_Potential* p, long n,
         if(useQueue) AGB_CUDA(cudaMallocAsync(&queue, sizeof(unsigned long long), s));
         launchOrbits(p->pot->view, P, n, ic, T, finalState, numSteps, numRejected, status, queue, s);
         if(queue) AGB_CUDA(cudaFreeAsync(queue, s));
+    });
+}
+
+extern "C" int agama_integrateOrbitsTrajectoryManyDevice(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, int trajSize, double* traj,
+    double* finalState, long* numSteps, int* status, void* stream)
+{
+    return guarded([&] {
+        if(!p || n < 0 || trajSize < 2 || (n > 0 && (!ic || !T || !traj || !finalState)))
+            throw std::invalid_argument("integrateOrbitsTrajectoryManyDevice: invalid arguments (trajSize >= 2)");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        OrbitParams P = makeOrbitParams(Omega, accuracy, maxNumSteps);
+        P.trajSize = trajSize;
+        P.traj = traj;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        Scratch q(sizeof(unsigned long long), s);
+        launchOrbits(p->pot->view, P, n, ic, T, finalState, numSteps, nullptr, status,
+            static_cast<unsigned long long*>(q.ptr), s);
+    });
+}
+
+extern "C" int agama_integrateOrbitsTrajectoryMany(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, int trajSize, double* traj,
+    double* finalState, long* numSteps, int* status)
+{
+    return guarded([&] {
+        if(!p || n < 0 || trajSize < 2 || (n > 0 && (!ic || !T || !traj)))
+            throw std::invalid_argument("integrateOrbitsTrajectoryMany: invalid arguments (trajSize >= 2)");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        DevBuf<double> dic(6 * n), dT(n), dout(6 * n), dtraj(static_cast<size_t>(n) * trajSize * 6);
+        DevBuf<long> dsteps(n);
+        DevBuf<int> dstat(n);
+        AGB_CUDA(cudaMemcpy(dic.ptr, ic, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
+        AGB_CUDA(cudaMemcpy(dT.ptr, T, n * sizeof(double), cudaMemcpyHostToDevice));
+        if(agama_integrateOrbitsTrajectoryManyDevice(p, n, dic.ptr, dT.ptr, Omega, accuracy, maxNumSteps, trajSize,
+                dtraj.ptr, dout.ptr, dsteps.ptr, dstat.ptr, nullptr) != 0)
+            throw std::runtime_error(lastError());
+        AGB_CUDA(cudaMemcpy(traj, dtraj.ptr, static_cast<size_t>(n) * trajSize * 6 * sizeof(double),
+            cudaMemcpyDeviceToHost));
+        if(finalState) AGB_CUDA(cudaMemcpy(finalState, dout.ptr, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        if(numSteps) AGB_CUDA(cudaMemcpy(numSteps, dsteps.ptr, n * sizeof(long), cudaMemcpyDeviceToHost));
+        if(status) AGB_CUDA(cudaMemcpy(status, dstat.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
     });
 }
 

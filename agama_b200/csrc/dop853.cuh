@@ -11,6 +11,8 @@ struct OrbitParams {
     double accRel;       ///< relative accuracy (DOP853 "accuracy")
     double accAbs;       ///< absolute accuracy (0 in the reference's orbit integrator)
     long   maxSteps;     ///< maximum number of accepted steps per orbit
+    int    trajSize = 0; ///< samples per orbit at regular times 0 .. T (0: final point only)
+    double* traj = nullptr;   ///< n x trajSize x 6 samples (rotating frame), NaN where none
 };
 
 /// per-orbit outcome codes
@@ -76,15 +78,17 @@ constexpr double fdec = 0.333, finc = 6.0, safe = 0.9;   // step-size control
 
 /** Right-hand side of the orbit ODE in the inertial frame with the potential rotating at
     Omega: dx/dt = v, dv/dt = -R(-Omega t) grad Phi(R(Omega t) x); optionally the accuracy factor
-    min(1, |E| / max(|Phi|, K)).  Reference OrbitIntegrator<Car>::eval, src/orbit.cpp:183-208. */
-template<int NQ, int KIND>
+    min(1, |E| / max(|Phi|, K)).  Reference OrbitIntegrator<Car>::eval, src/orbit.cpp:183-208.
+    G > 1: called together by a group of G lanes with the same point, which share the spline
+    evaluations (the multi-harmonic evaluator kind only). */
+template<int NQ, int KIND, int G = 1>
 __device__ __noinline__ void orbitRHS(const MultipoleView& M, double Omega, double time,
     const double* xv, double* dxdt, double* accFac)
 {
     double ca = 1, sa = 0;
     if(Omega != 0) sincos(Omega * time, &sa, &ca);
     double Epot, g[3], h[6];
-    evalMultipoleCar<NQ, KIND>(M, xv[0] * ca + xv[1] * sa, xv[1] * ca - xv[0] * sa, xv[2], &Epot, g, h);
+    evalMultipoleCar<NQ, KIND, G>(M, xv[0] * ca + xv[1] * sa, xv[1] * ca - xv[0] * sa, xv[2], &Epot, g, h);
     dxdt[0] = xv[3];
     dxdt[1] = xv[4];
     dxdt[2] = xv[5];

@@ -385,15 +385,41 @@ __device__ void evalInterp2d(const MultipoleView& M, double R, double z, double 
     }
 }
 
+/// sum of v over the G consecutive lanes of this lane's group, in a fixed lane order, so that
+/// every lane of the group gets the same bits
+template<int G>
+__device__ __forceinline__ double groupSum(double v, unsigned mask)
+{
+    double s = __shfl_sync(mask, v, 0, G);
+#pragma unroll
+    for(int j = 1; j < G; j++) s += __shfl_sync(mask, v, j, G);
+    return s;
+}
+
+/// the lanes of this lane's group of G consecutive lanes
+template<int G>
+__device__ __forceinline__ unsigned groupMask()
+{
+    if(G >= 32) return 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    return ((1u << G) - 1) << (lane & ~(G - 1));
+}
+
 /** The same 2-D spline evaluation with the harmonics held in registers: at most MAXS non-empty
     azimuthal harmonics, listed in M.fastM / M.fastSlot with m = 0 first and the others in
     ascending m (the order in which the reference sums them), so every array index is a
     compile-time constant after unrolling and nothing goes to local memory.  cos/sin(|m| phi)
-    come from the same multiple-angle recurrence as trigMultiAngle. */
-template<int NQ, int MAXS>
+    come from the same multiple-angle recurrence as trigMultiAngle.
+    G > 1: the evaluation is shared by a group of G consecutive lanes that evaluate the same
+    point: lane j of the group evaluates the harmonics s = j, j + G, ..., the m = 0 terms are
+    broadcast from lane 0 and the Fourier sums are added over the group in a fixed order (every
+    lane returns the same bits; the sums are ordered by lane, not by m). */
+template<int NQ, int MAXS, int G = 1>
 __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
+    const int gl = G > 1 ? static_cast<int>(threadIdx.x % G) : 0;
+    const unsigned gmask = G > 1 ? groupMask<G>() : 0u;
     const double r = sqrt(R * R + z * z), logr = log(r), rpRinv = 1. / (r + fabs(R));
     const double tau = R == 0 ? signOf(z) : z * rpRinv;
     const int xi = binSearch(logr, M.lnr, M.nr), yi = binSearch(tau, M.tau, M.nt);
@@ -404,10 +430,19 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
     double P[MAXS], Dr[MAXS], Dt[MAXS], Drr[MAXS], Drt[MAXS], Dtt[MAXS];
 #pragma unroll
     for(int s = 0; s < MAXS; s++) {
-        if(s < M.nFast) {
+        P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = 0;
+        if(s < M.nFast && s % G == gl) {
             spline2dCell<NQ>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
                 &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
             if(!inside) P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = NAN;
+        }
+    }
+    if(G > 1) {     // every lane needs the m = 0 harmonic (log scaling, Fourier sum)
+        P[0] = __shfl_sync(gmask, P[0], 0, G);
+        if(NQ >= 3) { Dr[0] = __shfl_sync(gmask, Dr[0], 0, G); Dt[0] = __shfl_sync(gmask, Dt[0], 0, G); }
+        if(NQ == 6) {
+            Drr[0] = __shfl_sync(gmask, Drr[0], 0, G); Drt[0] = __shfl_sync(gmask, Drt[0], 0, G);
+            Dtt[0] = __shfl_sync(gmask, Dtt[0], 0, G);
         }
     }
     if(M.logScaling) {
@@ -426,7 +461,7 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
         }
 #pragma unroll
         for(int s = 1; s < MAXS; s++) {
-            if(s < M.nFast) {
+            if(s < M.nFast && s % G == gl) {
                 if(NQ == 6) {
                     Drr[s] = Drr[s] * P[0] + P[s] * Drr[0] + 2 * Dr[s] * Dr[0];
                     Dtt[s] = Dtt[s] * P[0] + P[s] * Dtt[0] + 2 * Dt[s] * Dt[0];
@@ -441,10 +476,15 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
         }
     }
     // Fourier synthesis in the reference's order: m = 0, then the others by ascending m
+    // (G > 1: each lane sums its own harmonics, lane 0 starting from m = 0; then the group sum)
     SphDerivs gs; SphHess hs;
-    *pot = P[0];
-    if(NQ >= 3) { gs.dr = Dr[0]; gs.dt = Dt[0]; gs.dphi = 0; }
-    if(NQ == 6) { hs.dr2 = Drr[0]; hs.drdt = Drt[0]; hs.dt2 = Dtt[0]; hs.drdphi = hs.dtdphi = hs.dphi2 = 0; }
+    const bool own0 = gl == 0;
+    *pot = own0 ? P[0] : 0;
+    if(NQ >= 3) { gs.dr = own0 ? Dr[0] : 0; gs.dt = own0 ? Dt[0] : 0; gs.dphi = 0; }
+    if(NQ == 6) {
+        hs.dr2 = own0 ? Drr[0] : 0; hs.drdt = own0 ? Drt[0] : 0; hs.dt2 = own0 ? Dtt[0] : 0;
+        hs.drdphi = hs.dtdphi = hs.dphi2 = 0;
+    }
     if(MAXS > 1 && M.nFast > 1) {
         double cm[MAXS], sm[MAXS];
         double s1, c1, sh, ch;
@@ -465,7 +505,7 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
         }
 #pragma unroll
         for(int s = 1; s < MAXS; s++) {
-            if(s < M.nFast) {
+            if(s < M.nFast && s % G == gl) {
                 const int m = M.fastM[s];
                 const double tr = m > 0 ? cm[s] : sm[s];
                 const double dtr = m > 0 ? -m * sm[s] : -m * cm[s];
@@ -485,6 +525,15 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
                     hs.dphi2 += P[s] * d2tr;
                 }
             }
+        }
+    }
+    if(G > 1) {
+        *pot = groupSum<G>(*pot, gmask);
+        if(NQ >= 3) { gs.dr = groupSum<G>(gs.dr, gmask); gs.dt = groupSum<G>(gs.dt, gmask); gs.dphi = groupSum<G>(gs.dphi, gmask); }
+        if(NQ == 6) {
+            hs.dr2 = groupSum<G>(hs.dr2, gmask); hs.drdt = groupSum<G>(hs.drdt, gmask); hs.dt2 = groupSum<G>(hs.dt2, gmask);
+            hs.drdphi = groupSum<G>(hs.drdphi, gmask); hs.dtdphi = groupSum<G>(hs.dtdphi, gmask);
+            hs.dphi2 = groupSum<G>(hs.dphi2, gmask);
         }
     }
     if(NQ == 1) return;
@@ -521,10 +570,11 @@ enum EvalKind {
     asymptote by radius (reference src/potential_multipole.cpp:1538-1548).
     NQ = 1 (value), 3 (+ gradient) or 6 (+ Hessian); KIND selects the spline evaluator
     (the host picks the instantiation that matches the potential). */
-template<int NQ, int KIND = EVAL_GENERAL>
+template<int NQ, int KIND = EVAL_GENERAL, int G = 1>
 __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
+    static_assert(G == 1 || KIND == EVAL_FAST, "the group-shared evaluation is that of the multi-harmonic kind");
     const double rsq = R * R + z * z;
     if(rsq < M.rInnerSq)
         evalPowerLaw<NQ>(M.inner, R, z, phi, pot, g, h);
@@ -534,7 +584,7 @@ __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double 
         if(KIND == EVAL_AXI)
             evalInterp2dFast<NQ, 1>(M, R, z, phi, pot, g, h);
         else if(KIND == EVAL_FAST)
-            evalInterp2dFast<NQ, FAST_MAX_HARMONICS>(M, R, z, phi, pot, g, h);
+            evalInterp2dFast<NQ, FAST_MAX_HARMONICS, G>(M, R, z, phi, pot, g, h);
         else
             evalInterp2d<NQ>(M, R, z, phi, pot, g, h);
     } else
@@ -560,7 +610,7 @@ inline int evalKindOf(const MultipoleView& M)
 /** Evaluation at a Cartesian point with gradient (and Hessian xx,yy,zz,xy,yz,zx) in Cartesian
     coordinates: Car -> Cyl -> evaluate -> back (reference coord::evalAndConvert,
     src/coord.h:831-856, with the Car<->Cyl derivatives of src/coord.cpp:94-123, 608-719). */
-template<int NQ, int KIND = EVAL_GENERAL>
+template<int NQ, int KIND = EVAL_GENERAL, int G = 1>
 __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double x, double y, double z,
     double* pot, double* grad, double* hess)
 {
@@ -576,7 +626,7 @@ __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double 
         phi = atan2(y, x);
     }
     CylDerivs g; CylHess h;
-    evalMultipoleCyl<NQ, KIND>(M, R, z, phi, pot, &g, &h);
+    evalMultipoleCyl<NQ, KIND, G>(M, R, z, phi, pot, &g, &h);
     if(NQ >= 3) {
         grad[0] = g.dR * dRdx + g.dphi * dphidx;
         grad[1] = g.dR * dRdy + g.dphi * dphidy;

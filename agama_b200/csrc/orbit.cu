@@ -8,8 +8,12 @@
 // atomic counter) by a grid sized to the GPU, which balances orbits of very different length.
 #include "runtime.h"
 #include "dop853.cuh"
+#include "host_pipeline.h"
+#include <atomic>
 #include <map>
 #include <mutex>
+#include <tuple>
+#include <algorithm>
 
 namespace agb {
 
@@ -74,6 +78,58 @@ __host__ __device__ constexpr StageTable makeStageTable()
 }
 __constant__ StageTable STAGE_TABLE = makeStageTable();
 
+/** Trajectory samples inside one accepted step [t, t + h] at the regular times k T/(trajSize-1)
+    (RuntimeTrajectory::processTimestep, src/orbit.cpp:15-47: sample range with the 10 eps
+    round-off allowance, offsets clipped into the step) from the 7th-order dense output of the step
+    (OdeStepperDOP853::getSol and its coefficients, src/math_ode.cpp:381-426), rotated to the frame of
+    the potential at each sample time (OrbitIntegrator<Car>::getSolNative, src/orbit.cpp:119-133). */
+__device__ void sampleStep(const OrbitParams& P, long i, double tEnd, double sign, double t, double h,
+    const double* x, const double* xt, const double* k1, const double* k13, const StageStore& S)
+{
+    using namespace dp853;
+    const double dt = fabs(tEnd) / (P.trajSize - 1), tend = t + h;
+    const double roundoff = 10 * DBL_EPSILON * fmax(fabs(tend), fabs(t));
+    long iout = static_cast<long>(ceil(sign * t / dt));
+    long iend = static_cast<long>((sign * tend + roundoff) / dt);
+    if(iend > P.trajSize - 1) iend = P.trajSize - 1;
+    for(; iout <= iend; iout++) {
+        const double timeout = sign * dt * iout;
+        const double offset = clip(sign * (timeout - t), 0.0, sign * h) * sign;
+        double v[6];
+        if(offset == h) {
+            for(int c = 0; c < 6; c++) v[c] = xt[c];
+        } else if(offset == 0) {
+            for(int c = 0; c < 6; c++) v[c] = x[c];
+        } else {
+            const double p = offset / h, q = 1.0 - p;
+            for(int c = 0; c < 6; c++) {
+                const double k6 = S.at(4, c), k7 = S.at(5, c), k8 = S.at(6, c), k9 = S.at(7, c), k10 = S.at(8, c),
+                    k11 = S.at(0, c), k12 = S.at(1, c);
+                const double xd = xt[c] - x[c], xc = h * k1[c] - xd;
+                const double r4 = xd - h * k13[c] - xc;
+                const double r5 = h * (d41 * k1[c] + d46 * k6 + d47 * k7 + d48 * k8 + d49 * k9 + d410 * k10 +
+                                       d411 * k11 + d412 * k12 + d413 * k13[c]);
+                const double r6 = h * (d51 * k1[c] + d56 * k6 + d57 * k7 + d58 * k8 + d59 * k9 + d510 * k10 +
+                                       d511 * k11 + d512 * k12 + d513 * k13[c]);
+                const double r7 = h * (d61 * k1[c] + d66 * k6 + d67 * k7 + d68 * k8 + d69 * k9 + d610 * k10 +
+                                       d611 * k11 + d612 * k12 + d613 * k13[c]);
+                const double r8 = h * (d71 * k1[c] + d76 * k6 + d77 * k7 + d78 * k8 + d79 * k9 + d710 * k10 +
+                                       d711 * k11);
+                v[c] = x[c] + p * (xd + q * (xc + p * (r4 + q * (r5 + p * (r6 + q * (r7 + p * r8))))));
+            }
+        }
+        double ca = 1, sa = 0;
+        if(P.Omega != 0) sincos(P.Omega * (t + offset), &sa, &ca);
+        double* o = P.traj + (i * P.trajSize + iout) * 6;
+        o[0] = v[0] * ca + v[1] * sa;
+        o[1] = v[1] * ca - v[0] * sa;
+        o[2] = v[2];
+        o[3] = v[3] * ca + v[4] * sa;
+        o[4] = v[4] * ca - v[3] * sa;
+        o[5] = v[5];
+    }
+}
+
 /// phases of the per-lane integration state machine
 enum { PH_FETCH, PH_INIT1, PH_INIT2, PH_INIT3, PH_STAGE, PH_FINISH };
 
@@ -87,13 +143,19 @@ enum { PH_FETCH, PH_INIT1, PH_INIT2, PH_INIT3, PH_STAGE, PH_FINISH };
     min(finc, safe / err^(1/8)), rejection with the nbad counter; the final point is rotated
     to the frame of the potential at time tb + hLast (RuntimeTrajectory semantics).
     queue != nullptr: lanes take orbits from the work counter until it passes n; otherwise lane
-    i integrates orbit i only. */
-template<int KIND>
+    i integrates orbit i only.
+    G > 1: a group of G consecutive lanes integrates one orbit: every lane of the group runs the
+    same state machine on the same data (the group's sums are bit-identical in all its lanes, so
+    its control flow never splits) and the lanes share the spline evaluations of each right-hand
+    side; lane 0 of the group takes the orbits from the counter and writes the results. */
+template<int KIND, int G>
 __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constant__ MultipoleView M, const OrbitParams P,
     long n, const double* __restrict__ ic, const double* __restrict__ T, double* __restrict__ out,
     long* __restrict__ nsteps, long* __restrict__ nrej, int* __restrict__ status,
     unsigned long long* queue)
 {
+    const int gl = threadIdx.x % G;
+    const unsigned gmask = groupMask<G>();
     using namespace dp853;
     extern __shared__ double smem[];
     __shared__ StageTable tab;
@@ -103,7 +165,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
     const StageStore S{ smem + threadIdx.x, static_cast<int>(blockDim.x) };
     const double Om = P.Omega;
 
-    long i = queue ? -1 : blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    long i = queue ? -1 : (blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x) / G;
     if(!queue && i >= n) return;
     int phase = queue ? PH_FETCH : PH_INIT1;
     double x[6], k1[6], xt[6], k1b[6];
@@ -129,7 +191,9 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
 
     while(true) {
         if(phase == PH_FETCH) {
-            i = static_cast<long>(atomicAdd(queue, 1ull));
+            long v = 0;
+            if(gl == 0) v = static_cast<long>(atomicAdd(queue, 1ull));
+            i = G > 1 ? static_cast<long>(__shfl_sync(gmask, static_cast<unsigned long long>(v), 0, G)) : v;
             if(i >= n) break;
             phase = PH_INIT1;
         }
@@ -138,19 +202,31 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
             tEnd = T[i];
             t = 0; tb = 0; hLast = 0; steps = 0; rejects = 0; st = ORBIT_OK; accFac = 1;
             sign = tEnd >= 0 ? 1 : -1;
+            if(P.traj && gl == 0) {
+                // no sample yet; an orbit that is not integrated gets its start as sample 0 (and, for
+                // T = 0, as sample 1 too: the reference's zero sampling interval records the start
+                // and the end of its single zero step)
+                double* o = P.traj + i * P.trajSize * 6;
+                for(int k = 0; k < P.trajSize * 6; k++) o[k] = NAN;
+                if(tEnd == 0 || !isFinite(tEnd))
+                    for(int k = 0; k < (tEnd == 0 ? 2 : 1) && k < P.trajSize; k++)
+                        for(int c = 0; c < 6; c++) o[6 * k + c] = x[c];
+            }
         }
         if(phase == PH_FINISH) {
-            double ca = 1, sa = 0;
-            if(Om != 0) sincos(Om * (hLast + tb), &sa, &ca);
-            out[6 * i + 0] = x[0] * ca + x[1] * sa;
-            out[6 * i + 1] = x[1] * ca - x[0] * sa;
-            out[6 * i + 2] = x[2];
-            out[6 * i + 3] = x[3] * ca + x[4] * sa;
-            out[6 * i + 4] = x[4] * ca - x[3] * sa;
-            out[6 * i + 5] = x[5];
-            if(nsteps) nsteps[i] = steps;
-            if(nrej) nrej[i] = rejects;
-            if(status) status[i] = st;
+            if(gl == 0) {
+                double ca = 1, sa = 0;
+                if(Om != 0) sincos(Om * (hLast + tb), &sa, &ca);
+                out[6 * i + 0] = x[0] * ca + x[1] * sa;
+                out[6 * i + 1] = x[1] * ca - x[0] * sa;
+                out[6 * i + 2] = x[2];
+                out[6 * i + 3] = x[3] * ca + x[4] * sa;
+                out[6 * i + 4] = x[4] * ca - x[3] * sa;
+                out[6 * i + 5] = x[5];
+                if(nsteps) nsteps[i] = steps;
+                if(nrej) nrej[i] = rejects;
+                if(status) status[i] = st;
+            }
             if(!queue) break;
             phase = PH_FETCH;
             continue;
@@ -181,7 +257,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
         // ---- the one evaluation site
         const bool wantAcc = phase == PH_INIT1 || (phase == PH_STAGE && row == NUM_ROWS - 1);
         double k[6], af = 1;
-        orbitRHS<3, KIND>(M, Om, tt, xt, k, wantAcc ? &af : nullptr);
+        orbitRHS<3, KIND, G>(M, Om, tt, xt, k, wantAcc ? &af : nullptr);
         // ---- use the result
         if(phase == PH_INIT1) {
             for(int c = 0; c < 6; c++) k1[c] = k[c];
@@ -244,6 +320,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
                     continue;
                 }
             }
+            if(P.traj && gl == 0) sampleStep(P, i, tEnd, sign, t, h, x, xt, k1, k, S);
             for(int c = 0; c < 6; c++) { x[c] = xt[c]; k1[c] = k[c]; }
             tb = t;
             hLast = h;
@@ -262,15 +339,31 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
 
 size_t orbitSharedBytes(int block) { return sizeof(double) * NUM_STAGE_VECTORS * 6 * block; }
 
-void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream)
+namespace {
+
+using OrbitKernel = void (*)(const MultipoleView, const OrbitParams, long, const double*, const double*, double*,
+    long*, long*, int*, unsigned long long*);
+
+OrbitKernel orbitKernel(int kind, int lanes)
 {
-    if(n <= 0) return;
+    if(kind == EVAL_FAST) {
+        switch(lanes) {
+            case 2: return dop853Kernel<EVAL_FAST, 2>;
+            case 4: return dop853Kernel<EVAL_FAST, 4>;
+            case 8: return dop853Kernel<EVAL_FAST, 8>;
+            default: return dop853Kernel<EVAL_FAST, 1>;
+        }
+    }
+    return kind == EVAL_AXI ? dop853Kernel<EVAL_AXI, 1> : dop853Kernel<EVAL_GENERAL, 1>;
+}
+
+void launchOrbitKernel(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, int lanes, cudaStream_t stream)
+{
     const int block = ORBIT_BLOCK;
     const size_t shmem = orbitSharedBytes(block);
-    const int kind = evalKindOf(M);
-    auto kernel = kind == EVAL_AXI ? dop853Kernel<EVAL_AXI> : kind == EVAL_FAST ? dop853Kernel<EVAL_FAST>
-                                                                              : dop853Kernel<EVAL_GENERAL>;
+    const OrbitKernel kernel = orbitKernel(evalKindOf(M), lanes);
+    const long threads = n * lanes;
     long grid;
     if(queue) {
         int dev, sms, perSM = 0;
@@ -278,14 +371,91 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
         AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, block, shmem));
         grid = static_cast<long>(sms) * (perSM > 0 ? perSM : 1);
-        const long needed = (n + block - 1) / block;
+        const long needed = (threads + block - 1) / block;
         if(grid > needed) grid = needed;
         AGB_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), stream));
     } else {
-        grid = (n + block - 1) / block;
+        grid = (threads + block - 1) / block;
     }
     kernel<<<grid, block, shmem, stream>>>(M, P, n, ic, T, out, nsteps, nrej, status, queue);
     AGB_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Lanes per orbit: chosen by a timing trial on the caller's own orbits, once per device,
+// potential and batch-size class (powers of two), then cached.
+
+namespace {
+
+std::mutex g_laneMutex;
+std::map<std::tuple<int, const void*, int>, int> g_laneChoice;
+std::atomic<int> g_laneSetting{ 0 };
+constexpr int TRIAL_ORBITS = 32768, TRIAL_STEPS = 24;
+
+/// time each candidate on the first orbits of the batch, each integrated for TRIAL_STEPS steps
+int tuneLanes(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    cudaStream_t stream)
+{
+    const long m = std::min<long>(n, TRIAL_ORBITS);
+    OrbitParams Pt = P;
+    Pt.maxSteps = TRIAL_STEPS;
+    Scratch scratch(m * 6 * sizeof(double) + 256, stream);
+    double* out = static_cast<double*>(scratch.ptr);
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(out + 6 * m);
+    cudaEvent_t a, b;
+    AGB_CUDA(cudaEventCreate(&a));
+    AGB_CUDA(cudaEventCreate(&b));
+    int best = 1;
+    float bestMs = INFINITY;
+    const int candidates[] = { 1, 1, 2, 4, 8 };          // the first run also absorbs one-time set-up
+    for(int c = 0; c < 5; c++) {
+        AGB_CUDA(cudaEventRecord(a, stream));
+        launchOrbitKernel(M, Pt, m, ic, T, out, nullptr, nullptr, nullptr, counter, candidates[c], stream);
+        AGB_CUDA(cudaEventRecord(b, stream));
+        AGB_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        AGB_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if(c > 0 && ms < bestMs) { bestMs = ms; best = candidates[c]; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return best;
+}
+
+}  // namespace
+
+void setOrbitLanes(int lanes) { g_laneSetting = lanes; }
+
+int orbitLanesFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    cudaStream_t stream)
+{
+    if(evalKindOf(M) != EVAL_FAST) return 1;
+    const int fixed = g_laneSetting;
+    if(fixed == 1 || fixed == 2 || fixed == 4 || fixed == 8) return fixed;
+    int dev;
+    AGB_CUDA(cudaGetDevice(&dev));
+    int bucket = 0;
+    while((1L << bucket) < n) bucket++;
+    const auto key = std::make_tuple(dev, static_cast<const void*>(M.spl2d), bucket);
+    {
+        std::lock_guard<std::mutex> lock(g_laneMutex);
+        auto it = g_laneChoice.find(key);
+        if(it != g_laneChoice.end()) return it->second;
+    }
+    const int lanes = tuneLanes(M, P, n, ic, T, stream);
+    std::lock_guard<std::mutex> lock(g_laneMutex);
+    g_laneChoice[key] = lanes;
+    return lanes;
+}
+
+void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes)
+{
+    if(n <= 0) return;
+    if(lanes <= 0) lanes = orbitLanesFor(M, P, n, ic, T, stream);
+    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, queue, lanes, stream);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -333,8 +503,9 @@ void launchOrbitsNoAlloc(const MultipoleView& M, const OrbitParams& P, long n, c
         } else
             base = it->second;
     }
-    // launchOrbits clears the counter (cudaMemsetAsync on the stream) before the kernel runs
-    launchOrbits(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, stream);
+    // launchOrbits clears the counter (cudaMemsetAsync on the stream) before the kernel runs;
+    // one lane per orbit (the lane autotuner's trial would allocate scratch)
+    launchOrbits(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, stream, 1);
 }
 
 }  // namespace agb

@@ -81,7 +81,9 @@ void launchEvalPotential(const MultipoleView& M, long n, const double* pos, doub
     double* grad, double* hess, cudaStream_t stream);
 /// DOP853 batch; queue != nullptr selects the persistent work-queue mapping (8-byte counter)
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream);
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes = 0);
+/// lanes per orbit for all later batches: 1, 2, 4, 8, or 0 (default) for the autotuner
+void setOrbitLanes(int lanes);
 
 /// the same work-queue batch with its counter in the library's static device array (slot 0..31),
 /// allocating nothing

@@ -12,6 +12,20 @@ from . import _native
 from ._native import check, ptr
 
 
+def trajectory(potential, ic, time, trajsize, Omega=0.0, accuracy=1e-8, maxNumSteps=0):
+    """Orbits sampled at trajsize regular times from 0 to time (per orbit), as the reference's
+    orbit(..., trajsize=N): returns (times n x N, trajectories n x N x 6); numpy in, numpy out."""
+    x = np.ascontiguousarray(ic, dtype=np.float64).reshape(-1, 6)
+    n = len(x)
+    T = np.ascontiguousarray(np.broadcast_to(np.asarray(time, dtype=np.float64), (n,)))
+    traj = np.empty((n, int(trajsize), 6))
+    check(_native.lib().agama_integrateOrbitsTrajectoryMany(
+        potential.handle, n, ptr(x), ptr(T), float(Omega), float(accuracy), int(maxNumSteps), int(trajsize),
+        ptr(traj), None, None, None))
+    times = T[:, None] * np.linspace(0, 1, int(trajsize))[None, :]
+    return times, traj
+
+
 def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=True, info=False):
     """Integrate orbits; returns the final phase-space points (n x 6), and with info=True also
     a dict with the accepted step counts, rejected attempts and statuses
@@ -51,3 +65,8 @@ def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=Tr
     if single:
         out = out[0]
     return (out, dict(steps=steps, status=st)) if info else out
+
+
+def set_orbit_lanes(lanes=0):
+    """lanes of a warp integrating one orbit together: 1, 2, 4, 8, or 0 (autotuned, the default)"""
+    check(_native.lib().agama_setOrbitLanesPerOrbit(int(lanes)))

@@ -84,6 +84,28 @@ int agama_integrateOrbitsMany(const agama_Potential* potential, long n, const do
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, int* status);
 
+/* Lanes of a warp that integrate one orbit together (no reference counterpart): 1, 2, 4 or 8
+   (the lanes share the spline evaluations of potentials with up to 8 azimuthal harmonics; other
+   potentials use 1), or 0 (default) to let the library choose: a timing trial on the batch's
+   first orbits, once per device, potential and batch-size class, then cached.  The trial runs on
+   the caller's stream and waits for it, so the first call of a class should not be made during
+   stream capture.  Applies to the orbit entry points below except the allocation-free one. */
+int agama_setOrbitLanesPerOrbit(int lanes);
+
+/* Orbits with their trajectories sampled at trajSize (>= 2) regular times t_k = k T/(trajSize-1)
+   of each orbit (the reference's RuntimeTrajectory with sampling interval T/(trajSize-1), as
+   its Python orbit(trajsize=...), src/orbit.cpp:15-47: 7th-order dense output of the DOP853 steps,
+   src/math_ode.cpp:381-426); traj is n x trajSize x 6 in the frame rotating with Omega, NaN where
+   an orbit produced no sample (stopped early); T = 0 gives the start as samples 0 and 1.
+   Device-pointer and host-buffer variants; finalState, numSteps, status as for
+   agama_integrateOrbitsMany (in the host variant finalState may be NULL). */
+int agama_integrateOrbitsTrajectoryManyDevice(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, int trajSize, double* traj,
+    double* finalState, long* numSteps, int* status, void* stream);
+int agama_integrateOrbitsTrajectoryMany(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, int trajSize, double* traj,
+    double* finalState, long* numSteps, int* status);
+
 /* The same on device buffers (numSteps, numRejected, status may be NULL; numRejected counts
    rejected step attempts).  useQueue != 0 drains the batch from a device work queue with a
    grid sized to the GPU (for batches of very uneven integration times). */

@@ -46,6 +46,8 @@ def lib():
         L.ref_eval_cyl_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, _D, _D]
         L.ref_orbits_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_long, _D, _L, _I, ctypes.c_int]
+        L.ref_orbits_traj_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_long, ctypes.c_int, _D, ctypes.c_int]
         L.ref_orbits_evals.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_long, _LL, ctypes.c_int]
         L.ref_actions_fd_many.argtypes = [ctypes.c_void_p, ctypes.c_long, _D, _D, _D, _LL, ctypes.c_int]
@@ -118,6 +120,16 @@ class Potential:
         _check(lib().ref_orbits_many(self.h, n, _p(ic), _p(T), Omega, accuracy, maxSteps,
                                      _p(final), _p(nsteps, _L), _p(status, _I), nthreads))
         return final, nsteps, status
+
+    def orbits_traj(self, ic, T, trajsize, Omega=0.0, accuracy=1e-8, maxSteps=0, nthreads=0):
+        """trajectories at trajsize regular times from 0 to T (n x trajsize x 6)"""
+        ic = np.ascontiguousarray(ic, dtype=np.float64).reshape(-1, 6)
+        n = len(ic)
+        T = np.ascontiguousarray(np.broadcast_to(np.asarray(T, dtype=np.float64), (n,)))
+        out = np.empty((n, trajsize, 6))
+        _check(lib().ref_orbits_traj_many(self.h, n, _p(ic), _p(T), Omega, accuracy, maxSteps, int(trajsize),
+                                          _p(out), nthreads))
+        return out
 
     def orbit_evals(self, ic, T, Omega=0.0, accuracy=1e-8, maxSteps=0, nthreads=0):
         """potential evaluations spent on each orbit"""

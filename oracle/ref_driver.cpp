@@ -183,6 +183,37 @@ int ref_orbits_many(void* handle, long n, const double* ic, const double* T, dou
     return 0;
 }
 
+/// trajectories sampled at trajSize regular times 0, T/(trajSize-1), ..., T (the reference's
+/// RuntimeTrajectory with samplingInterval = T/(trajSize-1), as its Python orbit(trajsize=...));
+/// traj: n x trajSize x 6, NaN where the orbit produced no sample
+int ref_orbits_traj_many(void* handle, long n, const double* ic, const double* T, double Omega,
+    double accuracy, long maxSteps, int trajSize, double* traj, int nthreads)
+{
+    const potential::BasePotential& pot = *static_cast<PotHandle*>(handle)->pot;
+    setThreads(nthreads);
+    orbit::OrbitIntParams params(accuracy, maxSteps > 0 ? (size_t)maxSteps : (size_t)1e8);
+    std::string err;
+#pragma omp parallel for schedule(dynamic, 1)
+    for(long i = 0; i < n; i++) {
+        try {
+            for(long k = 0; k < (long)trajSize * 6; k++) traj[i * trajSize * 6 + k] = NAN;
+            orbit::Trajectory tr;
+            orbit::OrbitIntegrator<coord::Car> orbint(pot, Omega, params);
+            orbint.addRuntimeFnc(orbit::PtrRuntimeFnc(
+                new orbit::RuntimeTrajectory(orbint, fabs(T[i]) / (trajSize - 1), tr)));
+            orbint.init(coord::PosVelCar(ic + 6*i));
+            orbint.run(T[i]);
+            for(size_t k = 0; k < tr.size() && (long)k < trajSize; k++)
+                tr[k].first.unpack_to(traj + (i * trajSize + k) * 6);
+        } catch(std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if(!err.empty()) { g_error = err; return -1; }
+    return 0;
+}
+
 /// the number of potential evaluations each orbit of ref_orbits_many costs (counting wrapper)
 int ref_orbits_evals(void* handle, long n, const double* ic, const double* T, double Omega,
     double accuracy, long maxSteps, long long* nevals, int nthreads)

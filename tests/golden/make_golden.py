@@ -134,9 +134,10 @@ def make_orbit_vectors():
     final, steps, status = pot.orbits(ic, T, Omega=0.0, accuracy=1e-8)
     fin10, steps10, st10 = pot.orbits(ic[:4], T[:4], Omega=0.0, accuracy=1e-8, maxSteps=10)
     regular = regular_flags(pot, ic, T, 0.0)
+    traj = pot.orbits_traj(ic, T, 11, Omega=0.0, accuracy=1e-8)
     np.savez_compressed(os.path.join(HERE, "orbits_cfg1.npz"), ic=ic, T=T, Omega=0.0, accuracy=1e-8,
                         final=final, steps=steps, status=status, regular=regular,
-                        final_maxsteps10=fin10, steps_maxsteps10=steps10, status_maxsteps10=st10)
+                        final_maxsteps10=fin10, steps_maxsteps10=steps10, status_maxsteps10=st10, traj11=traj)
     print("cfg1 orbits", len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max())
     # config 3: rotating frame Omega = 0.05, uneven times 10^U[1, 1.5] T_circ
     coef = coef_path("cfg3")
@@ -149,8 +150,9 @@ def make_orbit_vectors():
     T = tcirc(coef, E) * 10 ** rng.uniform(1, 1.5, size=n)
     final, steps, status = pot.orbits(ic, T, Omega=0.05, accuracy=1e-8)
     regular = regular_flags(pot, ic, T, 0.05)
+    traj = pot.orbits_traj(ic, T, 11, Omega=0.05, accuracy=1e-8)
     np.savez_compressed(os.path.join(HERE, "orbits_cfg3.npz"), ic=ic, T=T, Omega=0.05, accuracy=1e-8,
-                        final=final, steps=steps, status=status, regular=regular)
+                        final=final, steps=steps, status=status, regular=regular, traj11=traj)
     print("cfg3 orbits", len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max())
 
 

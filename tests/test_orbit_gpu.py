@@ -29,9 +29,11 @@ def rel_vec(a, b):
 
 
 @pytest.mark.parametrize("cfg", ["cfg1", "cfg3"])
-@pytest.mark.parametrize("queue", [True, False])
-def test_orbit_parity(cfg, queue):
+@pytest.mark.parametrize("queue,lanes", [(True, 0), (False, 1), (True, 1), (True, 2), (True, 4), (True, 8), (False, 4)])
+def test_orbit_parity(cfg, queue, lanes):
+    """lanes: lanes of a warp per orbit (0: the autotuner's choice)"""
     import agama_b200
+    agama_b200.set_orbit_lanes(lanes)
     g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % cfg))
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
     Omega = float(g["Omega"])
@@ -50,6 +52,7 @@ def test_orbit_parity(cfg, queue):
     drift_ref = np.abs(jacobi_energy(pot, g["final"], Omega) / E0 - 1)
     ok = g["status"] == 0
     assert np.all(drift[ok] <= np.maximum(10 * drift_ref[ok], 1e-9)), (drift[ok].max(), drift_ref[ok].max())
+    agama_b200.set_orbit_lanes(0)
 
 
 def test_orbit_edge_cases():
@@ -83,3 +86,26 @@ def test_orbit_device_pointers():
     torch.cuda.synchronize()
     host = agama_b200.orbit(pot, g["ic"], g["T"])
     assert np.array_equal(out.cpu().numpy(), host)
+
+
+@pytest.mark.parametrize("cfg", ["cfg1", "cfg3"])
+def test_trajectory_samples(cfg):
+    """samples at 11 regular times from the dense output of the steps against the reference's
+    RuntimeTrajectory: regular orbits to 1e-7 (positions and velocities), NaN pattern identical
+    (the zero-time orbit: its start as samples 0 and 1), the last sample the final point"""
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % cfg))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    Omega = float(g["Omega"])
+    times, traj = agama_b200.trajectory(pot, g["ic"], g["T"], 11, Omega=Omega, accuracy=float(g["accuracy"]))
+    ref = g["traj11"]
+    assert np.array_equal(np.isnan(traj), np.isnan(ref))
+    reg = g["regular"] & (g["status"] == 0)
+    for k in range(11):
+        ok = reg & np.all(np.isfinite(ref[:, k]), axis=1)
+        epos = rel_vec(traj[ok, k, :3], ref[ok, k, :3])
+        evel = rel_vec(traj[ok, k, 3:], ref[ok, k, 3:])
+        assert epos.max(initial=0) <= 1e-7 and evel.max(initial=0) <= 1e-7, (k, epos.max(), evel.max())
+    final = agama_b200.orbit(pot, g["ic"], g["T"], Omega=Omega, accuracy=float(g["accuracy"]))
+    fin = g["T"] != 0
+    assert np.allclose(traj[fin, -1], final[fin], rtol=1e-12, atol=1e-12 * np.max(np.abs(final[fin])))
