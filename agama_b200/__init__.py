@@ -157,5 +157,5 @@ class Potential:
 
 
 from .actions import ActionFinder, actions  # noqa: E402,F401
-from .orbit import orbit, set_orbit_lanes, trajectory  # noqa: E402,F401
+from .orbit import orbit, set_orbit_lanes, trajectory, OrbitGraph  # noqa: E402,F401
 from .mlp import BracketNet  # noqa: E402,F401

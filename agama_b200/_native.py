@@ -32,6 +32,11 @@ SIGNATURES = {
                                                                  VP, VP, VP]),
     "agama_integrateOrbitsTrajectoryMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
                                                            ctypes.c_long, ctypes.c_int, D, D, L, I]),
+    "agama_orbitGraphCreate": (VP, [VP, ctypes.c_long, VP, VP, ctypes.c_double, ctypes.c_double, ctypes.c_long,
+                                    VP, VP, VP, VP]),
+    "agama_orbitGraphLaunch": (ctypes.c_int, [VP, VP]),
+    "agama_orbitGraphLanes": (ctypes.c_int, [VP]),
+    "agama_orbitGraphDelete": (None, [VP]),
     "agama_integrateOrbitsMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_long, D, L, I]),
     "agama_integrateOrbitsManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,

@@ -257,6 +257,67 @@ extern "C" int agama_integrateOrbitsTrajectoryMany(const agama_Potential* p, lon
     });
 }
 
+// ---- orbit batches captured once in a CUDA graph and replayed
+
+struct agama_OrbitGraph {
+    int device = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    DevBuf<unsigned long long> queue;
+    int lanes = 1;
+    ~agama_OrbitGraph() {
+        if(exec) cudaGraphExecDestroy(exec);
+        if(graph) cudaGraphDestroy(graph);
+    }
+};
+
+extern "C" agama_OrbitGraph* agama_orbitGraphCreate(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState, long* numSteps,
+    long* numRejected, int* status)
+{
+    try {
+        if(!p || n <= 0 || !ic || !T || !finalState) throw std::invalid_argument("orbitGraphCreate: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const OrbitParams P = makeOrbitParams(Omega, accuracy, maxNumSteps);
+        agama_OrbitGraph* g = new agama_OrbitGraph;
+        try {
+            g->device = p->pot->device;
+            g->queue.alloc(1);
+            cudaStream_t s;
+            AGB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            // the lanes per orbit are settled (autotuner trial) before the capture begins
+            g->lanes = orbitLanesFor(p->pot->view, P, n, ic, T, s);
+            AGB_CUDA(cudaStreamSynchronize(s));
+            AGB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            launchOrbits(p->pot->view, P, n, ic, T, finalState, numSteps, numRejected, status, g->queue.ptr, s,
+                g->lanes);
+            AGB_CUDA(cudaStreamEndCapture(s, &g->graph));
+            AGB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
+            AGB_CUDA(cudaStreamDestroy(s));
+        } catch(...) {
+            delete g;
+            throw;
+        }
+        return g;
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+extern "C" int agama_orbitGraphLaunch(agama_OrbitGraph* g, void* stream)
+{
+    return guarded([&] {
+        if(!g) throw std::invalid_argument("orbitGraphLaunch: null graph");
+        AGB_CUDA(cudaSetDevice(g->device));
+        AGB_CUDA(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+    });
+}
+
+extern "C" int agama_orbitGraphLanes(const agama_OrbitGraph* g) { return g ? g->lanes : 0; }
+
+extern "C" void agama_orbitGraphDelete(agama_OrbitGraph* g) { delete g; }
+
 extern "C" int agama_integrateOrbitsMany(const agama_Potential* p, long n, const double* ic,
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, int* status)

@@ -84,6 +84,9 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
     double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes = 0);
 /// lanes per orbit for all later batches: 1, 2, 4, 8, or 0 (default) for the autotuner
 void setOrbitLanes(int lanes);
+/// the lanes per orbit a batch will use (runs the autotuner's trial on the stream if needed)
+int orbitLanesFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    cudaStream_t stream);
 
 /// the same work-queue batch with its counter in the library's static device array (slot 0..31),
 /// allocating nothing

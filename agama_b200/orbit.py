@@ -70,3 +70,42 @@ def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=Tr
 def set_orbit_lanes(lanes=0):
     """lanes of a warp integrating one orbit together: 1, 2, 4, 8, or 0 (autotuned, the default)"""
     check(_native.lib().agama_setOrbitLanesPerOrbit(int(lanes)))
+
+
+class OrbitGraph:
+    """an orbit batch over CUDA tensors captured once in a CUDA graph; launch() replays it on the
+    current stream (with final is ic, every launch continues the orbits for another T)"""
+
+    def __init__(self, potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, final=None):
+        import torch
+        from . import _dev_ptr
+        self.potential = potential
+        self.ic = ic
+        n = ic.shape[0]
+        self.T = time if hasattr(time, "data_ptr") else torch.full((n,), float(time), dtype=torch.float64,
+                                                                    device=ic.device)
+        self.final = torch.empty_like(ic) if final is None else final
+        self.steps = torch.empty(n, dtype=torch.int64, device=ic.device)
+        self.rejected = torch.empty(n, dtype=torch.int64, device=ic.device)
+        self.status = torch.empty(n, dtype=torch.int32, device=ic.device)
+        h = _native.lib().agama_orbitGraphCreate(potential.handle, n, _dev_ptr(ic), _dev_ptr(self.T), float(Omega),
+                                                 float(accuracy), int(maxNumSteps), _dev_ptr(self.final),
+                                                 _dev_ptr(self.steps), _dev_ptr(self.rejected), _dev_ptr(self.status))
+        if not h:
+            raise RuntimeError("agama_b200: " + _native.error())
+        self._h = ctypes.c_void_p(h)
+
+    @property
+    def lanes(self):
+        return _native.lib().agama_orbitGraphLanes(self._h)
+
+    def launch(self):
+        from . import _current_stream
+        check(_native.lib().agama_orbitGraphLaunch(self._h, _current_stream()))
+        return self.final
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _native._lib is not None:
+            _native._lib.agama_orbitGraphDelete(h)
+            self._h = None

@@ -253,12 +253,16 @@ def run_engine_secondary(dev, flush, dist, cpu):
             ("config 3: %d of the 1e5 orbits (10-1000 T_circ, Omega 0.05), DOP853 1e-8, at most %d steps per orbit"
              % (ORBIT3_ORBITS, ORBIT3_MAX_STEPS), pot3, ic3, T3, 0.05, ORBIT3_MAX_STEPS, 1, 2)):
         dic, dT = torch.tensor(ic, device=dev), torch.tensor(T, device=dev)
-        t, r = timed(lambda: agama_b200.orbit(pot, dic, dT, Omega=Om, maxNumSteps=mx, info=True), warm, steps)
-        info = r[1]
-        nst, nrej = int(info["steps"].sum().item()), int(info["rejected"].sum().item())
+        # the batch is captured once in a CUDA graph (work-counter reset + persistent kernel, lanes
+        # per orbit chosen by the autotuner before the capture) and replayed every step
+        graph = agama_b200.OrbitGraph(pot, dic, dT, Omega=Om, maxNumSteps=mx)
+        t, _ = timed(graph.launch, warm, steps)
+        nst, nrej = int(graph.steps.sum().item()), int(graph.rejected.sum().item())
         out.append({"metric": "orbit-steps/s", "value": nst / (t / 1000), "unit": "accepted DOP853 steps/s",
                     "ms_per_step": t, "config": name, "steps": steps, "warmup": warm, "accepted_steps": nst,
-                    "rejected_attempts": nrej, "gpu_launches_per_step": 1})
+                    "rejected_attempts": nrej, "gpu_launches_per_step": 1, "launch": "CUDA graph",
+                    "lanes_per_orbit": graph.lanes})
+        del graph
     if cpu:
         for line, base in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3)):
             line["cpu_baseline"] = base

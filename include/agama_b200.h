@@ -92,6 +92,20 @@ int agama_integrateOrbitsMany(const agama_Potential* potential, long n, const do
    stream capture.  Applies to the orbit entry points below except the allocation-free one. */
 int agama_setOrbitLanesPerOrbit(int lanes);
 
+/* An orbit batch captured once in a CUDA graph (no reference counterpart): the work-counter reset
+   and the persistent DOP853 kernel over the given device buffers, with the lanes per orbit settled
+   (autotuner trial) before the capture.  Each agama_orbitGraphLaunch replays the batch on the
+   stream, reading the current contents of ic and T: with finalState == ic every launch continues
+   the orbits for another T (each orbit reads its start before writing its end).  The buffers
+   must stay valid while the graph exists. */
+typedef struct agama_OrbitGraph agama_OrbitGraph;
+agama_OrbitGraph* agama_orbitGraphCreate(const agama_Potential* potential, long n, const double* ic, const double* T,
+    double Omega, double accuracy, long maxNumSteps, double* finalState, long* numSteps, long* numRejected,
+    int* status);
+int agama_orbitGraphLaunch(agama_OrbitGraph* graph, void* stream);
+int agama_orbitGraphLanes(const agama_OrbitGraph* graph);
+void agama_orbitGraphDelete(agama_OrbitGraph* graph);
+
 /* Orbits with their trajectories sampled at trajSize (>= 2) regular times t_k = k T/(trajSize-1)
    of each orbit (the reference's RuntimeTrajectory with sampling interval T/(trajSize-1), as
    its Python orbit(trajsize=...), src/orbit.cpp:15-47: 7th-order dense output of the DOP853 steps,

@@ -109,3 +109,30 @@ def test_trajectory_samples(cfg):
     final = agama_b200.orbit(pot, g["ic"], g["T"], Omega=Omega, accuracy=float(g["accuracy"]))
     fin = g["T"] != 0
     assert np.allclose(traj[fin, -1], final[fin], rtol=1e-12, atol=1e-12 * np.max(np.abs(final[fin])))
+
+
+def test_orbit_graph_replays_and_continues():
+    """a captured orbit batch: one launch equals the direct call bit for bit; with the end points
+    written over the starts, two launches of T continue the orbits: bit for bit the same as two
+    direct calls, the second started from the end of the first (a restart, as the reference's
+    integrator started again from a point)"""
+    import torch
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "orbits_cfg1.npz"))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+    ok = g["T"] > 0
+    ic = torch.tensor(g["ic"][ok], device="cuda")
+    T = torch.tensor(g["T"][ok], device="cuda")
+    direct = agama_b200.orbit(pot, ic, T)
+    graph = agama_b200.OrbitGraph(pot, ic, T)
+    assert graph.lanes in (1, 2, 4, 8)
+    once = graph.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(once, direct)
+    x = ic.clone()
+    seg = agama_b200.OrbitGraph(pot, x, T, final=x)
+    seg.launch()
+    seg.launch()
+    twice = agama_b200.orbit(pot, agama_b200.orbit(pot, ic, T), T)
+    torch.cuda.synchronize()
+    assert torch.equal(x, twice)
