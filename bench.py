@@ -158,11 +158,15 @@ def run_reference_secondary():
 
         def force(self, x):
             return -self.p.eval(x)[1]
+    from agama_b200 import workloads
     _, pts1, ic1, T1, _, ic3, T3 = secondary_workloads(RefPot, lambda c: os.path.join(GOLDEN, c + ".coef"))
+    p5 = RefPot(os.path.join(GOLDEN, "cfg5.coef"))
+    ic5, T5 = workloads.orbit_workload(5, p5.potential, p5.force, 1000)
     names = [("force evals/s", "config 1 forces"), ("orbit-steps/s", "config 1 orbits"),
-             ("orbit-steps/s", "config 3 orbits, at most %d steps per orbit" % ORBIT3_MAX_STEPS)]
+             ("orbit-steps/s", "config 3 orbits, at most %d steps per orbit" % ORBIT3_MAX_STEPS),
+             ("orbit-steps/s", "config 5 orbits"), ("actions/s", "config 5 actions of the final snapshot")]
     return [dict(metric=m, value=b and b["value"], unit=b and b.get("unit"), config=c, cpu_baseline=b)
-            for (m, c), b in zip(names, reference_secondary(pts1, ic1, T1, ic3, T3))]
+            for (m, c), b in zip(names, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5))]
 
 
 def cpu_baseline_line(pts):
@@ -197,6 +201,9 @@ def cpu_baseline_line(pts):
 #                     steps per orbit, hours of integration on either arm   -> orbit-steps/s
 ORBIT3_ORBITS = 20000
 ORBIT3_MAX_STEPS = 5000
+#   config 5:         5e4 of the 1e6 orbits (100 T_circ each) in the Spheroid + disk Multipole
+#                     (lmax 12, 80 nodes), then the actions of their final snapshot
+ORBIT5_ORBITS = 50000
 
 
 def secondary_workloads(potential_cls, coef):
@@ -263,8 +270,27 @@ def run_engine_secondary(dev, flush, dist, cpu):
                     "rejected_attempts": nrej, "gpu_launches_per_step": 1, "launch": "CUDA graph",
                     "lanes_per_orbit": graph.lanes})
         del graph
+    # config 5: orbits, then the actions of the final snapshot
+    from agama_b200 import workloads
+    pot5 = Pot(os.path.join(GOLDEN, "cfg5.coef"))
+    ic5, T5 = workloads.orbit_workload(5, pot5.potential, pot5.force, ORBIT5_ORBITS)
+    dic5, dT5 = torch.tensor(ic5, device=dev), torch.tensor(T5, device=dev)
+    graph5 = agama_b200.OrbitGraph(pot5, dic5, dT5)
+    t5, _ = timed(graph5.launch, 1, 1)
+    nst5 = int(graph5.steps.sum().item())
+    af5 = agama_b200.ActionFinder(pot5)
+    snap = graph5.final.clone()
+    ta, _ = timed(lambda: af5(snap), 3, 5)
+    out.append({"metric": "orbit-steps/s", "value": nst5 / (t5 / 1000), "unit": "accepted DOP853 steps/s",
+                "ms_per_step": t5, "config": "config 5: %d of the 1e6 orbits x 100 T_circ, Spheroid + disk Multipole "
+                "lmax 12 / 80 nodes, DOP853 1e-8" % ORBIT5_ORBITS, "steps": 1, "warmup": 1, "accepted_steps": nst5,
+                "gpu_launches_per_step": 1, "launch": "CUDA graph", "lanes_per_orbit": graph5.lanes})
+    out.append({"metric": "actions/s", "value": ORBIT5_ORBITS / (ta / 1000), "unit": "actions/s", "ms_per_step": ta,
+                "config": "config 5: actions of the final snapshot of those orbits (action finder, FP64)",
+                "steps": 5, "warmup": 3, "gpu_launches_per_step": 3})
+    del graph5
     if cpu:
-        for line, base in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3)):
+        for line, base in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5)):
             line["cpu_baseline"] = base
     return out
 
@@ -355,12 +381,12 @@ def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
     return out
 
 
-def reference_secondary(pts1, ic1, T1, ic3, T3):
+def reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5):
     """the reference's own CPU code on bounded samples of the secondary workloads, all host cores"""
     try:
         from oracle import ref
         if not ref.available():
-            return [None, None, None]
+            return [None] * 5
         cores = os.cpu_count()
         p1 = ref.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
         p3 = ref.Potential(file=os.path.join(GOLDEN, "cfg3.coef"))
@@ -379,9 +405,21 @@ def reference_secondary(pts1, ic1, T1, ic3, T3):
             dt = time.perf_counter() - t0
             res.append({"value": float(steps.sum()) / dt, "unit": "accepted DOP853 steps/s", "cores": cores,
                         "kind": "reference", "sample": "first %d orbits of the %s workload, OpenMP dynamic 1" % (n, what)})
+        p5 = ref.Potential(file=os.path.join(GOLDEN, "cfg5.coef"))
+        t0 = time.perf_counter()
+        fin5, steps5, _ = p5.orbits(ic5[:200], T5[:200], nthreads=cores)
+        dt = time.perf_counter() - t0
+        res.append({"value": float(steps5.sum()) / dt, "unit": "accepted DOP853 steps/s", "cores": cores,
+                    "kind": "reference", "sample": "first 200 orbits of the config 5 workload, OpenMP dynamic 1"})
+        af5 = ref.ActionFinder(p5)
+        t0 = time.perf_counter()
+        af5.actions(fin5, nthreads=cores)
+        dt = time.perf_counter() - t0
+        res.append({"value": len(fin5) / dt, "unit": "actions/s", "cores": cores, "kind": "reference",
+                    "sample": "actions of those 200 final points, reference ActionFinderAxisymFudge, OpenMP"})
         return res
     except Exception as e:   # the baseline is reported, never required
-        return [{"value": None, "kind": "reference", "sample": "failed: %s" % e}] * 3
+        return [{"value": None, "kind": "reference", "sample": "failed: %s" % e}] * 5
 
 
 def run_engine(args):
