@@ -482,8 +482,9 @@ def run_engine(args):
 
     # ---- end to end through the public API, pinned host buffers
     hp = torch.from_numpy(pts).pin_memory().numpy()
-    for _ in range(2):      # warm-up at full size: the output's page-locked block, the pool's chunk scratch
-        af(hp)
+    out = None
+    for _ in range(3):      # warm-up at full size: the outputs' page-locked blocks (the previous result
+        out = af(hp)        # is alive during the next call, as in the timed loop), the pool's chunk scratch
     e2e_times = []
     for k in range(max(2, min(args.steps, 5))):
         torch.cuda.synchronize()
