@@ -157,5 +157,6 @@ class Potential:
 
 
 from .actions import ActionFinder, actions  # noqa: E402,F401
-from .orbit import orbit, set_orbit_lanes, trajectory, OrbitGraph  # noqa: E402,F401
+from .orbit import (orbit, set_orbit_lanes, set_orbit_precision, jacobi_energy_error,  # noqa: E402,F401
+                    trajectory, OrbitGraph)
 from .mlp import BracketNet  # noqa: E402,F401

@@ -27,6 +27,7 @@ SIGNATURES = {
     "agama_evalPotentialMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
     "agama_evalPotentialManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
     "agama_setOrbitLanesPerOrbit": (ctypes.c_int, [ctypes.c_int]),
+    "agama_setOrbitPrecision": (ctypes.c_int, [ctypes.c_int]),
     "agama_integrateOrbitsTrajectoryManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
                                                                  ctypes.c_double, ctypes.c_long, ctypes.c_int, VP, VP,
                                                                  VP, VP, VP]),

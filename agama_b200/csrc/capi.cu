@@ -195,6 +195,14 @@ extern "C" int agama_setOrbitLanesPerOrbit(int lanes)
     });
 }
 
+extern "C" int agama_setOrbitPrecision(int mixed)
+{
+    return guarded([&] {
+        if(mixed != 0 && mixed != 1) throw std::invalid_argument("setOrbitPrecision: mixed must be 0 or 1");
+        setOrbitMixedPrecision(mixed != 0);
+    });
+}
+
 extern "C" int agama_integrateOrbitsManyDevice(const agama_Potential* p, long n, const double* ic,
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, long* numRejected, int* status, int useQueue, void* stream)

@@ -73,10 +73,10 @@ AGB_HD int binSearch(double x, const double* arr, int size)
     "defects" (mismatch of f, f', f'' at xh), each multiplied by a fixed basis polynomial in t.
     Same interpolant and special case x == xh as evalQuinticSplines, reference
     src/math_spline.cpp:654-731. */
-template<int K>
-AGB_HD void quinticSegment(double x, double xl, double xh,
-    const double* fl, const double* fh, const double* f1l, const double* f1h,
-    const double* f2l, const double* f2h, double* f, double* df, double* d2f)
+template<int K, typename T = double>
+AGB_HD void quinticSegment(T x, T xl, T xh,
+    const T* fl, const T* fh, const T* f1l, const T* f1h,
+    const T* f2l, const T* f2h, T* f, T* df, T* d2f)
 {
     if(x == xh) {   // exactly at the right node: return the node values without round-off
 #pragma unroll
@@ -87,24 +87,24 @@ AGB_HD void quinticSegment(double x, double xl, double xh,
         }
         return;
     }
-    const double dx = x - xl, hdx2 = 0.5 * dx * dx, h = xh - xl, hi = 1 / h, h2 = h * h;
-    const double t = dx * hi, t2 = t * t, t3 = t * t2, omt = t * (1 - t);
+    const T dx = x - xl, hdx2 = T(0.5) * dx * dx, h = xh - xl, hi = 1 / h, h2 = h * h;
+    const T t = dx * hi, t2 = t * t, t3 = t * t2, omt = t * (1 - t);
     // basis polynomials for the three defects and their first two derivatives
-    const double bf   = t3 * (10 - t * (15 - 6 * t));
-    const double b1   = t3 * (1 - t * 0.5) * h;
-    const double b2   = t3 * (1 - t * (1.25 - 0.5 * t)) * h2;
-    const double cx   = 30 * omt * hi;
-    const double bfp  = cx * omt;
-    const double b1p  = t2 * (3 - t * 2);
-    const double b2p  = t2 * (3 - t * (5 - 2.5 * t)) * h;
-    const double bfpp = cx * hi * (2 - 4 * t);
-    const double b1pp = cx * 0.2;
-    const double b2pp = t * (6 - t * (15 - 10 * t));
+    const T bf   = t3 * (10 - t * (15 - 6 * t));
+    const T b1   = t3 * (1 - t * T(0.5)) * h;
+    const T b2   = t3 * (1 - t * (T(1.25) - T(0.5) * t)) * h2;
+    const T cx   = 30 * omt * hi;
+    const T bfp  = cx * omt;
+    const T b1p  = t2 * (3 - t * 2);
+    const T b2p  = t2 * (3 - t * (5 - T(2.5) * t)) * h;
+    const T bfpp = cx * hi * (2 - 4 * t);
+    const T b1pp = cx * T(0.2);
+    const T b2pp = t * (6 - t * (15 - 10 * t));
 #pragma unroll
     for(int k = 0; k < K; k++) {
-        const double d0 = fh[k]  - fl[k]  - 0.5 * h * (f1h[k] + f1l[k]);
-        const double d1 = f1h[k] - f1l[k] - 0.5 * h * (f2h[k] + f2l[k]);
-        const double d2 = f2h[k] - f2l[k];
+        const T d0 = fh[k]  - fl[k]  - T(0.5) * h * (f1h[k] + f1l[k]);
+        const T d1 = f1h[k] - f1l[k] - T(0.5) * h * (f2h[k] + f2l[k]);
+        const T d2 = f2h[k] - f2l[k];
         if(f)   f[k]   = fl[k] + bf * d0 + dx * f1l[k] + b1 * d1 + hdx2 * f2l[k] + b2 * d2;
         if(df)  df[k]  = bfp * d0 + f1l[k] + b1p * d1 + dx * f2l[k] + b2p * d2;
         if(d2f) d2f[k] = bfpp * d0 + b1pp * d1 + f2l[k] + b2pp * d2;

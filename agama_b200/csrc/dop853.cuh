@@ -81,14 +81,14 @@ constexpr double fdec = 0.333, finc = 6.0, safe = 0.9;   // step-size control
     min(1, |E| / max(|Phi|, K)).  Reference OrbitIntegrator<Car>::eval, src/orbit.cpp:183-208.
     G > 1: called together by a group of G lanes with the same point, which share the spline
     evaluations (the multi-harmonic evaluator kind only). */
-template<int NQ, int KIND, int G = 1>
+template<int NQ, int KIND, int G = 1, bool MIXED = false>
 __device__ __noinline__ void orbitRHS(const MultipoleView& M, double Omega, double time,
     const double* xv, double* dxdt, double* accFac)
 {
     double ca = 1, sa = 0;
     if(Omega != 0) sincos(Omega * time, &sa, &ca);
     double Epot, g[3], h[6];
-    evalMultipoleCar<NQ, KIND, G>(M, xv[0] * ca + xv[1] * sa, xv[1] * ca - xv[0] * sa, xv[2], &Epot, g, h);
+    evalMultipoleCar<NQ, KIND, G, MIXED>(M, xv[0] * ca + xv[1] * sa, xv[1] * ca - xv[0] * sa, xv[2], &Epot, g, h);
     dxdt[0] = xv[3];
     dxdt[1] = xv[4];
     dxdt[2] = xv[5];

@@ -50,6 +50,7 @@ struct MultipoleView {
     int nt; const double* tau;   // angular grid in tau (2-D case)
     int splSlot[2 * LMAX_MAX + 1];  // slot of the 2-D spline for m (index m+mmax), -1 if empty
     const double* spl2d;  // [slot][nr][nt][NODE_STRIDE]: f fx fy fxx fxy fyy fxxy fxyy fxxyy pad
+    const float* spl2d32; // the same table rounded to FP32 (mixed-precision evaluation of m != 0)
     const double* spl1d;  // [c][nr][3]: f f' f''  (1-D case; all (lmax+1)^2 coefficients)
     int logScaling;
     double invPhi0;

@@ -294,9 +294,53 @@ __device__ __forceinline__ void spline2dCell(const double* tab, int nt, int xi, 
     quinticSegment<1>(x, xl, xh, &F[0], &F[1], &F[2], &F[3], &F[4], &F[5], z, zx, zxx);
     *z += off;
     if(NQ >= 3)
-        quinticSegment<1>(x, xl, xh, &dF[0], &dF[1], &dF[2], &dF[3], &dF[4], &dF[5], zy, zxy, nullptr);
+        quinticSegment<1, double>(x, xl, xh, &dF[0], &dF[1], &dF[2], &dF[3], &dF[4], &dF[5], zy, zxy, nullptr);
     if(NQ == 6)
-        quinticSegment<1>(x, xl, xh, &d2F[0], &d2F[1], &d2F[2], &d2F[3], &d2F[4], &d2F[5], zyy, nullptr, nullptr);
+        quinticSegment<1, double>(x, xl, xh, &d2F[0], &d2F[1], &d2F[2], &d2F[3], &d2F[4], &d2F[5], zyy, nullptr, nullptr);
+}
+
+/** The same cell in FP32 (the mixed-precision evaluation of the m != 0 harmonics): node values
+    from the FP32 copy of the table, local coordinates x - xl, y - yl formed in FP64 and rounded,
+    so that the interpolation keeps FP32 precision relative to the cell size; results in FP64. */
+template<int NQ>
+__device__ __forceinline__ void spline2dCell32(const float* tab, int nt, int xi, int yi,
+    double x, double xl, double xh, double y, double yl, double yh,
+    double* z, double* zx, double* zy, double* zxx, double* zxy, double* zyy)
+{
+    const float* nll = tab + (static_cast<size_t>(xi) * nt + yi) * NODE_STRIDE;
+    const float* nlu = nll + NODE_STRIDE;
+    const float* nul = nll + static_cast<size_t>(nt) * NODE_STRIDE;
+    const float* nuu = nul + NODE_STRIDE;
+    float ll[10], lu[10], ul[10], uu[10];
+#pragma unroll
+    for(int q = 0; q < 5; q++) {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(nll) + q), b = __ldg(reinterpret_cast<const float2*>(nlu) + q),
+            c = __ldg(reinterpret_cast<const float2*>(nul) + q), d = __ldg(reinterpret_cast<const float2*>(nuu) + q);
+        ll[2 * q] = a.x; ll[2 * q + 1] = a.y; lu[2 * q] = b.x; lu[2 * q + 1] = b.y;
+        ul[2 * q] = c.x; ul[2 * q + 1] = c.y; uu[2 * q] = d.x; uu[2 * q + 1] = d.y;
+    }
+    const float hx = static_cast<float>(xh - xl), hy = static_cast<float>(yh - yl);
+    const float lx = x == xh ? hx : static_cast<float>(x - xl), ly = y == yh ? hy : static_cast<float>(y - yl);
+    const float off = x == xh ? (y == yh ? uu[0] : ul[0]) : (y == yh ? lu[0] : ll[0]);
+    const float fl[6]  = { ll[0] - off, ul[0] - off, ll[1], ul[1], ll[3], ul[3] };
+    const float fu[6]  = { lu[0] - off, uu[0] - off, lu[1], uu[1], lu[3], uu[3] };
+    const float f1l[6] = { ll[2], ul[2], ll[4], ul[4], ll[6], ul[6] };
+    const float f1u[6] = { lu[2], uu[2], lu[4], uu[4], lu[6], uu[6] };
+    const float f2l[6] = { ll[5], ul[5], ll[7], ul[7], ll[8], ul[8] };
+    const float f2u[6] = { lu[5], uu[5], lu[7], uu[7], lu[8], uu[8] };
+    float F[6], dF[6], d2F[6], v, vx, vxx, vy, vxy, vyy;
+    quinticSegment<6, float>(ly, 0.f, hy, fl, fu, f1l, f1u, f2l, f2u, F, NQ >= 3 ? dF : nullptr, NQ == 6 ? d2F : nullptr);
+    quinticSegment<1, float>(lx, 0.f, hx, &F[0], &F[1], &F[2], &F[3], &F[4], &F[5], &v, &vx, &vxx);
+    *z = static_cast<double>(v) + static_cast<double>(off);
+    *zx = vx; *zxx = vxx;
+    if(NQ >= 3) {
+        quinticSegment<1, float>(lx, 0.f, hx, &dF[0], &dF[1], &dF[2], &dF[3], &dF[4], &dF[5], &vy, &vxy, nullptr);
+        *zy = vy; *zxy = vxy;
+    }
+    if(NQ == 6) {
+        quinticSegment<1, float>(lx, 0.f, hx, &d2F[0], &d2F[1], &d2F[2], &d2F[3], &d2F[4], &d2F[5], &vyy, nullptr, nullptr);
+        *zyy = vyy;
+    }
 }
 
 /** 2-D splines per azimuthal harmonic; reference MultipoleInterp2d::evalCyl,
@@ -410,11 +454,12 @@ __device__ __forceinline__ unsigned groupMask()
     ascending m (the order in which the reference sums them), so every array index is a
     compile-time constant after unrolling and nothing goes to local memory.  cos/sin(|m| phi)
     come from the same multiple-angle recurrence as trigMultiAngle.
+    MIXED: the m != 0 harmonics from the FP32 table in FP32 arithmetic (their sum in FP64).
     G > 1: the evaluation is shared by a group of G consecutive lanes that evaluate the same
     point: lane j of the group evaluates the harmonics s = j, j + G, ..., the m = 0 terms are
     broadcast from lane 0 and the Fourier sums are added over the group in a fixed order (every
     lane returns the same bits; the sums are ordered by lane, not by m). */
-template<int NQ, int MAXS, int G = 1>
+template<int NQ, int MAXS, int G = 1, bool MIXED = false>
 __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
@@ -432,8 +477,12 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
     for(int s = 0; s < MAXS; s++) {
         P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = 0;
         if(s < M.nFast && s % G == gl) {
-            spline2dCell<NQ>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
-                &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
+            if(MIXED && s > 0)      // m != 0 (angular) harmonics in FP32, the radial m = 0 one in FP64
+                spline2dCell32<NQ>(M.spl2d32 + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
+                    &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
+            else
+                spline2dCell<NQ>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
+                    &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
             if(!inside) P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = NAN;
         }
     }
@@ -570,7 +619,7 @@ enum EvalKind {
     asymptote by radius (reference src/potential_multipole.cpp:1538-1548).
     NQ = 1 (value), 3 (+ gradient) or 6 (+ Hessian); KIND selects the spline evaluator
     (the host picks the instantiation that matches the potential). */
-template<int NQ, int KIND = EVAL_GENERAL, int G = 1>
+template<int NQ, int KIND = EVAL_GENERAL, int G = 1, bool MIXED = false>
 __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
@@ -584,7 +633,7 @@ __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double 
         if(KIND == EVAL_AXI)
             evalInterp2dFast<NQ, 1>(M, R, z, phi, pot, g, h);
         else if(KIND == EVAL_FAST)
-            evalInterp2dFast<NQ, FAST_MAX_HARMONICS, G>(M, R, z, phi, pot, g, h);
+            evalInterp2dFast<NQ, FAST_MAX_HARMONICS, G, MIXED>(M, R, z, phi, pot, g, h);
         else
             evalInterp2d<NQ>(M, R, z, phi, pot, g, h);
     } else
@@ -610,7 +659,7 @@ inline int evalKindOf(const MultipoleView& M)
 /** Evaluation at a Cartesian point with gradient (and Hessian xx,yy,zz,xy,yz,zx) in Cartesian
     coordinates: Car -> Cyl -> evaluate -> back (reference coord::evalAndConvert,
     src/coord.h:831-856, with the Car<->Cyl derivatives of src/coord.cpp:94-123, 608-719). */
-template<int NQ, int KIND = EVAL_GENERAL, int G = 1>
+template<int NQ, int KIND = EVAL_GENERAL, int G = 1, bool MIXED = false>
 __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double x, double y, double z,
     double* pot, double* grad, double* hess)
 {
@@ -626,7 +675,7 @@ __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double 
         phi = atan2(y, x);
     }
     CylDerivs g; CylHess h;
-    evalMultipoleCyl<NQ, KIND, G>(M, R, z, phi, pot, &g, &h);
+    evalMultipoleCyl<NQ, KIND, G, MIXED>(M, R, z, phi, pot, &g, &h);
     if(NQ >= 3) {
         grad[0] = g.dR * dRdx + g.dphi * dphidx;
         grad[1] = g.dR * dRdy + g.dphi * dphidy;

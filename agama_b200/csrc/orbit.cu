@@ -147,8 +147,10 @@ enum { PH_FETCH, PH_INIT1, PH_INIT2, PH_INIT3, PH_STAGE, PH_FINISH };
     G > 1: a group of G consecutive lanes integrates one orbit: every lane of the group runs the
     same state machine on the same data (the group's sums are bit-identical in all its lanes, so
     its control flow never splits) and the lanes share the spline evaluations of each right-hand
-    side; lane 0 of the group takes the orbits from the counter and writes the results. */
-template<int KIND, int G>
+    side; lane 0 of the group takes the orbits from the counter and writes the results.
+    MIXED: the forces of the multi-harmonic kind with the m != 0 harmonics in FP32 (the radial m = 0
+    part, the Fourier sums, the state, the stages and the error norm stay FP64). */
+template<int KIND, int G, bool MIXED>
 __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constant__ MultipoleView M, const OrbitParams P,
     long n, const double* __restrict__ ic, const double* __restrict__ T, double* __restrict__ out,
     long* __restrict__ nsteps, long* __restrict__ nrej, int* __restrict__ status,
@@ -257,7 +259,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
         // ---- the one evaluation site
         const bool wantAcc = phase == PH_INIT1 || (phase == PH_STAGE && row == NUM_ROWS - 1);
         double k[6], af = 1;
-        orbitRHS<3, KIND, G>(M, Om, tt, xt, k, wantAcc ? &af : nullptr);
+        orbitRHS<3, KIND, G, MIXED>(M, Om, tt, xt, k, wantAcc ? &af : nullptr);
         // ---- use the result
         if(phase == PH_INIT1) {
             for(int c = 0; c < 6; c++) k1[c] = k[c];
@@ -344,25 +346,32 @@ namespace {
 using OrbitKernel = void (*)(const MultipoleView, const OrbitParams, long, const double*, const double*, double*,
     long*, long*, int*, unsigned long long*);
 
-OrbitKernel orbitKernel(int kind, int lanes)
+OrbitKernel orbitKernel(int kind, int lanes, bool mixed)
 {
     if(kind == EVAL_FAST) {
+        if(mixed) return dop853Kernel<EVAL_FAST, 1, true>;
         switch(lanes) {
-            case 2: return dop853Kernel<EVAL_FAST, 2>;
-            case 4: return dop853Kernel<EVAL_FAST, 4>;
-            case 8: return dop853Kernel<EVAL_FAST, 8>;
-            default: return dop853Kernel<EVAL_FAST, 1>;
+            case 2: return dop853Kernel<EVAL_FAST, 2, false>;
+            case 4: return dop853Kernel<EVAL_FAST, 4, false>;
+            case 8: return dop853Kernel<EVAL_FAST, 8, false>;
+            default: return dop853Kernel<EVAL_FAST, 1, false>;
         }
     }
-    return kind == EVAL_AXI ? dop853Kernel<EVAL_AXI, 1> : dop853Kernel<EVAL_GENERAL, 1>;
+    return kind == EVAL_AXI ? dop853Kernel<EVAL_AXI, 1, false> : dop853Kernel<EVAL_GENERAL, 1, false>;
 }
 
+/// FP32 non-axisymmetric harmonics in later batches (multi-harmonic potentials only; off by default)
+std::atomic<int> g_mixedSetting{ 0 };
+
 void launchOrbitKernel(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, int lanes, cudaStream_t stream)
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, int lanes, bool mixed,
+    cudaStream_t stream)
 {
     const int block = ORBIT_BLOCK;
     const size_t shmem = orbitSharedBytes(block);
-    const OrbitKernel kernel = orbitKernel(evalKindOf(M), lanes);
+    mixed = mixed && evalKindOf(M) == EVAL_FAST;
+    if(mixed) lanes = 1;
+    const OrbitKernel kernel = orbitKernel(evalKindOf(M), lanes, mixed);
     const long threads = n * lanes;
     long grid;
     if(queue) {
@@ -412,7 +421,7 @@ int tuneLanes(const MultipoleView& M, const OrbitParams& P, long n, const double
     const int candidates[] = { 1, 1, 2, 4, 8 };          // the first run also absorbs one-time set-up
     for(int c = 0; c < 5; c++) {
         AGB_CUDA(cudaEventRecord(a, stream));
-        launchOrbitKernel(M, Pt, m, ic, T, out, nullptr, nullptr, nullptr, counter, candidates[c], stream);
+        launchOrbitKernel(M, Pt, m, ic, T, out, nullptr, nullptr, nullptr, counter, candidates[c], false, stream);
         AGB_CUDA(cudaEventRecord(b, stream));
         AGB_CUDA(cudaEventSynchronize(b));
         float ms = 0;
@@ -427,11 +436,12 @@ int tuneLanes(const MultipoleView& M, const OrbitParams& P, long n, const double
 }  // namespace
 
 void setOrbitLanes(int lanes) { g_laneSetting = lanes; }
+void setOrbitMixedPrecision(bool mixed) { g_mixedSetting = mixed ? 1 : 0; }
 
 int orbitLanesFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     cudaStream_t stream)
 {
-    if(evalKindOf(M) != EVAL_FAST) return 1;
+    if(evalKindOf(M) != EVAL_FAST || g_mixedSetting) return 1;
     const int fixed = g_laneSetting;
     if(fixed == 1 || fixed == 2 || fixed == 4 || fixed == 8) return fixed;
     int dev;
@@ -455,7 +465,7 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
 {
     if(n <= 0) return;
     if(lanes <= 0) lanes = orbitLanesFor(M, P, n, ic, T, stream);
-    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, queue, lanes, stream);
+    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, queue, lanes, g_mixedSetting != 0, stream);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -503,9 +513,10 @@ void launchOrbitsNoAlloc(const MultipoleView& M, const OrbitParams& P, long n, c
         } else
             base = it->second;
     }
-    // launchOrbits clears the counter (cudaMemsetAsync on the stream) before the kernel runs;
-    // one lane per orbit (the lane autotuner's trial would allocate scratch)
-    launchOrbits(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, stream, 1);
+    // the launch clears the counter (cudaMemsetAsync on the stream) before the kernel runs;
+    // one lane per orbit (the lane autotuner's trial would allocate scratch), always FP64
+    if(n <= 0) return;
+    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, 1, false, stream);
 }
 
 }  // namespace agb

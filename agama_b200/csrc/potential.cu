@@ -64,6 +64,7 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
         P->lnr.upload(H.lnr);
         P->tau.upload(H.tau);
         P->spl2d.upload(H.spl2d);
+        P->spl2d32.upload(std::vector<float>(H.spl2d.begin(), H.spl2d.end()));
         P->spl1d.upload(H.spl1d);
         P->innerS.upload(H.inner.S); P->innerU.upload(H.inner.U); P->innerW.upload(H.inner.W);
         P->outerS.upload(H.outer.S); P->outerU.upload(H.outer.U); P->outerW.upload(H.outer.W);
@@ -80,6 +81,7 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
         V.tau = P->tau.ptr;
         for(int i = 0; i < 2 * LMAX_MAX + 1; i++) V.splSlot[i] = H.splSlot[i];
         V.spl2d = P->spl2d.ptr;
+        V.spl2d32 = P->spl2d32.ptr;
         V.spl1d = P->spl1d.ptr;
         V.logScaling = H.logScaling;
         V.invPhi0 = H.invPhi0;

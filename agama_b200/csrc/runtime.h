@@ -47,6 +47,7 @@ struct DevicePotential {
     int device = 0;
     MultipoleHost host;
     DevBuf<double> lnr, tau, spl2d, spl1d, innerS, innerU, innerW, outerS, outerU, outerW;
+    DevBuf<float> spl2d32;
     MultipoleView view;
     /// the axisymmetric (m = 0) part, used by the action finder (same as the full potential
     /// when the potential is axisymmetric)
@@ -84,6 +85,9 @@ void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const do
     double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes = 0);
 /// lanes per orbit for all later batches: 1, 2, 4, 8, or 0 (default) for the autotuner
 void setOrbitLanes(int lanes);
+/// mixed precision for later batches in multi-harmonic potentials: the m != 0 harmonics of the
+/// force from an FP32 copy of the spline table (one lane per orbit); false (default) = all FP64
+void setOrbitMixedPrecision(bool mixed);
 /// the lanes per orbit a batch will use (runs the autotuner's trial on the stream if needed)
 int orbitLanesFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     cudaStream_t stream);

@@ -67,6 +67,24 @@ def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=Tr
     return (out, dict(steps=steps, status=st)) if info else out
 
 
+def set_orbit_precision(mixed=False):
+    """mixed=True: later orbit batches in multi-harmonic potentials evaluate the m != 0 harmonics
+    of the force in FP32 (radial m = 0 part, azimuthal sums, state, stages and error norm in FP64);
+    False (the default): everything in FP64.  jacobi_energy_error() states the error per orbit."""
+    check(_native.lib().agama_setOrbitPrecision(1 if mixed else 0))
+
+
+def jacobi_energy_error(potential, ic, final, Omega=0.0):
+    """relative change |E_J(final) / E_J(ic) - 1| of the Jacobi energy
+    E_J = Phi + v^2/2 - Omega (x v_y - y v_x) of each orbit, Phi evaluated in FP64: the per-orbit
+    error statement of an integration (the integrator's own truncation error plus, in mixed
+    precision, the effect of the FP32 harmonics); numpy or CUDA tensors in, the same out."""
+    def ej(w):
+        phi = potential.potential(w[:, :3])
+        return phi + 0.5 * (w[:, 3:] ** 2).sum(1) - Omega * (w[:, 0] * w[:, 4] - w[:, 1] * w[:, 3])
+    return abs(ej(final) / ej(ic) - 1)
+
+
 def set_orbit_lanes(lanes=0):
     """lanes of a warp integrating one orbit together: 1, 2, 4, 8, or 0 (autotuned, the default)"""
     check(_native.lib().agama_setOrbitLanesPerOrbit(int(lanes)))

@@ -249,7 +249,7 @@ def run_engine_secondary(dev, flush, dist, cpu):
             t = float(tt.item())
         return t, r
 
-    out = []
+    out, mixed_lines = [], []
     d1 = torch.tensor(pts1, device=dev)
     t, _ = timed(lambda: pot1.eval(d1, pot=True, acc=True), 3, 10)
     out.append({"metric": "force evals/s", "value": len(pts1) / (t / 1000), "unit": "evals/s", "ms_per_step": t,
@@ -269,6 +269,7 @@ def run_engine_secondary(dev, flush, dist, cpu):
                     "ms_per_step": t, "config": name, "steps": steps, "warmup": warm, "accepted_steps": nst,
                     "rejected_attempts": nrej, "gpu_launches_per_step": 1, "launch": "CUDA graph",
                     "lanes_per_orbit": graph.lanes})
+        mixed_lines.append(mixed_orbit_entry(agama_b200, timed, pot, dic, dT, Om, mx, warm, steps, name, graph, t))
         del graph
     # config 5: orbits, then the actions of the final snapshot
     from agama_b200 import workloads
@@ -292,7 +293,36 @@ def run_engine_secondary(dev, flush, dist, cpu):
     if cpu:
         for line, base in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5)):
             line["cpu_baseline"] = base
-    return out
+    return out + mixed_lines
+
+
+def mixed_orbit_entry(agama_b200, timed, pot, dic, dT, Om, mx, warm, steps, name, graph64, t64):
+    """the same orbit batch with the m != 0 harmonics of the force in FP32, with the error of
+    every orbit stated: its Jacobi-energy error and its deviation from the FP64 batch"""
+    import torch
+    agama_b200.set_orbit_precision(True)
+    try:
+        graph = agama_b200.OrbitGraph(pot, dic, dT, Omega=Om, maxNumSteps=mx)
+    finally:
+        agama_b200.set_orbit_precision(False)
+    t, _ = timed(graph.launch, warm, steps)
+    nst = int(graph.steps.sum().item())
+    ok = ((graph.status == 0) & (graph64.status == 0)).cpu().numpy()
+    f32, f64 = graph.final.cpu().numpy()[ok], graph64.final.cpu().numpy()[ok]
+    ic = dic.cpu().numpy()[ok]
+    dev = np.linalg.norm(f32[:, :3] - f64[:, :3], axis=1) / np.linalg.norm(f64[:, :3], axis=1)
+    e32 = agama_b200.jacobi_energy_error(pot, ic, f32, Om)
+    e64 = agama_b200.jacobi_energy_error(pot, ic, f64, Om)
+    q = lambda a: {"median": float(np.median(a)), "p90": float(np.quantile(a, 0.9)), "max": float(a.max())}
+    line = {"metric": "orbit-steps/s", "value": nst / (t / 1000), "unit": "accepted DOP853 steps/s",
+            "ms_per_step": t, "config": name + "; mixed precision (m != 0 harmonics in FP32)", "steps": steps,
+            "warmup": warm, "accepted_steps": nst, "gpu_launches_per_step": 1, "launch": "CUDA graph",
+            "lanes_per_orbit": graph.lanes, "fp64_ms_per_step": t64,
+            "error_per_orbit": {"jacobi_energy_rel_mixed": q(e32), "jacobi_energy_rel_fp64": q(e64),
+                                "position_rel_vs_fp64": q(dev), "orbits": int(ok.sum())}}
+    del graph
+    torch.cuda.synchronize()
+    return line
 
 
 def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):

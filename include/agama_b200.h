@@ -92,6 +92,16 @@ int agama_integrateOrbitsMany(const agama_Potential* potential, long n, const do
    stream capture.  Applies to the orbit entry points below except the allocation-free one. */
 int agama_setOrbitLanesPerOrbit(int lanes);
 
+/* Mixed precision for orbit batches (no reference counterpart): 1 evaluates the non-axisymmetric
+   (m != 0) harmonics of multi-harmonic Multipole potentials from an FP32 copy of the spline table,
+   with the radial m = 0 part, the azimuthal sums, the integrator state, its stages and its error
+   norm in FP64; 0 (default) is all FP64.  Forces then differ from FP64 by about 1e-7 of the
+   non-axisymmetric part, and final states of regular orbits by the growth of that over the
+   integration (the Python orbit_precision_error helper measures it per orbit).  One lane per orbit
+   in mixed mode; other potentials and the allocation-free entry point stay FP64.  Applies to
+   batches launched or captured afterwards. */
+int agama_setOrbitPrecision(int mixed);
+
 /* An orbit batch captured once in a CUDA graph (no reference counterpart): the work-counter reset
    and the persistent DOP853 kernel over the given device buffers, with the lanes per orbit settled
    (autotuner trial) before the capture.  Each agama_orbitGraphLaunch replays the batch on the
