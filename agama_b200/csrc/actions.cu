@@ -77,12 +77,13 @@ constexpr long POINTS_PER_PASS = 1L << 20;     // records of one pass: 128 MB of
 /// from the finder's table; otherwise fd[i], or fd0 if fd is null), integrals of motion, the
 /// limits that need no root search and the brackets of those that do -> one record per point.
 /// Jphi (and NaN Jr, Jz of points without actions) are written directly.  Optional outputs:
-/// Delta used, root-finder iterations (zeroed here, counted by phase 2).
+/// Delta used, root-finder iterations (zeroed here, counted by phase 2).  ends[i]: F and F' at the
+/// record's lambdaPos, for the root searches.
 template<bool FINDER>
 __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __grid_constant__ MultipoleView M,
     const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd,
     double fd0, FudgeRecord* __restrict__ rec, double* __restrict__ act, double* __restrict__ fdOut,
-    int* __restrict__ iters, float* __restrict__ features)
+    int* __restrict__ iters, float* __restrict__ features, double2* __restrict__ ends)
 {
     const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
     if(i >= n) return;
@@ -94,9 +95,10 @@ __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __g
     evalMultipoleCylCall<1, EVAL_AXI>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
     const double delta = FINDER ? finderFocalDistance(F, pc, Phi) : (fd ? fd[i] : fd0);
     FudgeRecord r;
-    double a[3];
-    fudgePrepare(M, pc, Phi, delta, r, a);
+    double a[3], endF[2] = { 0, 0 };
+    fudgePrepare(M, pc, Phi, delta, r, a, endF);
     rec[i] = r;
+    ends[i] = make_double2(endF[0], endF[1]);
     act[3 * i + 2] = a[2];
     if(!r.valid) { act[3 * i] = a[0]; act[3 * i + 1] = a[1]; }
     if(fdOut) fdOut[i] = delta;
@@ -129,12 +131,13 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
     const bool predict = bp && bp->net;
     // records, two work counters, the actions of a pass when the caller wants none, and the
     // predictor's inputs and outputs
-    const size_t recBytes = pass * sizeof(FudgeRecord) + 256;
+    const size_t recBytes = pass * (sizeof(FudgeRecord) + sizeof(double2)) + 256;
     const size_t actBytes = act ? 0 : pass * 3 * sizeof(double);
     const size_t featBytes = (predict ? pass * 9 * sizeof(float) : 0) + 256;
     Scratch scratch(recBytes + actBytes + featBytes, stream);
     FudgeRecord* rec = static_cast<FudgeRecord*>(scratch.ptr);
-    unsigned long long* counter = reinterpret_cast<unsigned long long*>(rec + pass);
+    double2* ends = reinterpret_cast<double2*>(rec + pass);
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(ends + pass);
     double* actTmp = reinterpret_cast<double*>(static_cast<char*>(scratch.ptr) + recBytes);
     float* feat = predict ? reinterpret_cast<float*>(static_cast<char*>(scratch.ptr) + recBytes + actBytes) : nullptr;
     float* pred = predict ? feat + pass * 6 : nullptr;
@@ -148,10 +151,10 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
         float* f = samples ? samples->features + 6 * first : feat;
         fudgePrepareKernel<FINDER><<<(count + PREPARE_BLOCK - 1) / PREPARE_BLOCK, PREPARE_BLOCK, 0, stream>>>(
             M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, a,
-            fdOut ? fdOut + first : nullptr, it, f);
+            fdOut ? fdOut + first : nullptr, it, f, ends);
         AGB_CUDA(cudaGetLastError());
         if(predict) bp->net->predict(count, feat, pred, stream);
-        launchFudgeRoots(M, count, rec, it, counter, pred, widths, bp ? bp->stats : nullptr, stream);
+        launchFudgeRoots(M, count, rec, ends, it, counter, pred, widths, bp ? bp->stats : nullptr, stream);
         if(samples)
             launchBracketTargets(count, rec, samples->target + 3 * first, samples->mask + 3 * first, stream);
         else if(angles)

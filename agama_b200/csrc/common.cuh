@@ -297,7 +297,8 @@ AGB_HD double findRoot(const F& fnc, double xlower, double xupper, double reltol
 struct RootSearch {
     double a, b, c, fa, fb, fc, da, db, dc, d, e, abstol;
     double result;
-    int iter, phase;     // phase 0: wants f(xlower), 1: f(xupper), 2: f(next iterate)
+    int iter, phase;     // phase 0: wants f(xlower), 1: f(xupper), 2: f(next iterate),
+                         // 3: f(xlower) with f(xupper) already known
 
     AGB_HD double start(double xlower, double xupper, double reltol)
     {
@@ -314,6 +315,26 @@ struct RootSearch {
         return a;
     }
 
+    /// the same search with f, f' at the upper end already known (so the first point to evaluate
+    /// is the lower end, returned)
+    AGB_HD double startKnownUpper(double xlower, double xupper, double tol, double fupper, double dupper)
+    {
+        startAbs(xlower, xupper, tol);
+        fb = fupper; db = dupper;
+        phase = 3;
+        return a;
+    }
+
+    /// the same search with f, f' at both ends already known: true when it has finished at once
+    /// (result set), otherwise *xnext is the first point to evaluate
+    AGB_HD bool startKnownEnds(double xlower, double xupper, double tol, double flower, double dlower,
+        double fupper, double dupper, double* xnext)
+    {
+        startAbs(xlower, xupper, tol);
+        fa = flower; da = dlower; fb = fupper; db = dupper;
+        return begin(xnext);
+    }
+
     /// take f and f' at the requested point; true when the search has finished (result set),
     /// otherwise *xnext is the next point to evaluate
     AGB_HD bool feed(double fx, double dx, double* xnext)
@@ -326,15 +347,11 @@ struct RootSearch {
         }
         if(phase == 1) {
             fb = fx; db = dx;
-            if((fa < 0 && fb < 0) || (fa > 0 && fb > 0) || !isFinite(fa + fb)) { result = NAN; return true; }
-            if(fa == 0) { result = fb == 0 ? 0.5 * (a + b) : a; return true; }
-            if(fb == 0) { result = b; return true; }
-            c = a; fc = fa; dc = da; d = b - c; e = b - c;
-            if(fabs(fc) < fabs(fb)) {
-                a = b; b = c; c = a;  fa = fb; fb = fc; fc = fa;  da = db; db = dc; dc = da;
-            }
-            phase = 2;
-            return propose(xnext);
+            return begin(xnext);
+        }
+        if(phase == 3) {
+            fa = fx; da = dx;
+            return begin(xnext);
         }
         fb = fx; db = dx;
         if(!isFinite(fb)) { result = NAN; return true; }
@@ -356,6 +373,20 @@ struct RootSearch {
         const bool inside = (off > 0 && off < c - b) || (off < 0 && off > c - b);
         if(inside && fabs(off) < abstol) { result = b + off; return true; }
         if(iter >= ROOT_MAXITER) { result = b; return true; }
+        return propose(xnext);
+    }
+
+    /// both end values known: the bracket checks and the first iterate
+    AGB_HD bool begin(double* xnext)
+    {
+        if((fa < 0 && fb < 0) || (fa > 0 && fb > 0) || !isFinite(fa + fb)) { result = NAN; return true; }
+        if(fa == 0) { result = fb == 0 ? 0.5 * (a + b) : a; return true; }
+        if(fb == 0) { result = b; return true; }
+        c = a; fc = fa; dc = da; d = b - c; e = b - c;
+        if(fabs(fc) < fabs(fb)) {
+            a = b; b = c; c = a;  fa = fb; fb = fc; fc = fa;  da = db; db = dc; dc = da;
+        }
+        phase = 2;
         return propose(xnext);
     }
 

@@ -203,8 +203,10 @@ __device__ __forceinline__ void loadFudgeFunction(const MultipoleView& M, const 
 
 /** Integration limits of the lambda and nu motions (findIntegrationLimitsAxisym,
     src/actions_staeckel.cpp:360-483), part 1: every decision up to the three root searches, whose
-    brackets go into the record; limits that need no root are stored directly (NaN otherwise). */
-static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& rec)
+    brackets go into the record; limits that need no root are stored directly (NaN otherwise).
+    endF (may be null) receives F and F' at lambda_pos, the end that the brackets of lambda_min and
+    lambda_max share, which the root searches then take instead of evaluating it again. */
+static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& rec, double* endF = nullptr)
 {
     const double delta = fnc.D2;
     const double f_zero = fnc.value(0);
@@ -227,7 +229,7 @@ static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& r
         if(f_zero > 0) roots |= ROOT_NU_MAX;           // falls back to |nu| if no root is found
         else nu_max = fabs(fnc.nu);
     }
-    double lambda_pos = fnc.lambda;
+    double lambda_pos = fnc.lambda, f_pos = f_lambda, df_pos = df_lambda;
     const double dxToRoot = -f_lambda / df_lambda;
     if(f_lambda <= 0 || fabs(dxToRoot) < fnc.lambda * FUDGE_MINIMUM_RANGE) {
         if(df_lambda >= 0) lambda_min = fnc.lambda;
@@ -241,6 +243,7 @@ static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& r
         lambda_pos += fmax(dxToRoot, safeOffset) * (df_lambda >= 0 ? 1 : -1);
         double f_lp, df_lp, d2f_lp;
         fnc.eval<true, true>(lambda_pos, &f_lp, &df_lp, &d2f_lp);
+        f_pos = f_lp; df_pos = df_lp;
         nearShell |= d2f_lp < 0 &&
             pow2(df_lp) - 2 * f_lp * d2f_lp - pow2(fnc.lambda * FUDGE_MINIMUM_RANGE * d2f_lp) < 0;
         if(nearShell || f_lp < 0)
@@ -251,6 +254,7 @@ static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& r
     rec.nuMax = nu_max; rec.lambdaMin = lambda_min; rec.lambdaMax = lambda_max;
     rec.nuUpper = nu_upper; rec.lambdaLower = lambda_lower; rec.lambdaPos = lambda_pos;
     rec.roots = roots;
+    if(endF) { endF[0] = f_pos; endF[1] = df_pos; }
 }
 
 struct FudgeLimits { double lambda_min, lambda_max, nu_max; int order; };
@@ -294,9 +298,9 @@ static __device__ double fudgeMomentumNode(const FudgeFunction& fnc, double lo, 
     Phi is the potential at the point.  Writes Jphi into act[2]; for a point without actions
     (unbound, or lambda = nu = Delta^2) also NaN into act[0..1] and marks the record invalid.
     Otherwise the record holds the integrals of motion (findIntegralsOfMotionAxisymFudge,
-    :176-195) and the limits and root brackets of fudgeLimitsSetup. */
+    :176-195) and the limits and root brackets of fudgeLimitsSetup (endF: as there). */
 static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, double Phi, double fd,
-    FudgeRecord& rec, double* act)
+    FudgeRecord& rec, double* act, double* endF = nullptr)
 {
     const double R = pc[0], z = pc[1], phi = pc[2], vR = pc[3], vz = pc[4], vphi = pc[5];
     if(fd <= 0) fd = fmax(R, 1.) * 1e-4;
@@ -337,7 +341,7 @@ static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, do
     if(!isFinite(fnc.E + fnc.I3 + fnc.Lz) || fnc.E >= 0) { act[0] = act[1] = NAN; return; }
     rec.lambda = fnc.lambda; rec.nu = fnc.nu; rec.D2 = D2; rec.E = fnc.E; rec.Lz = Lz; rec.I3 = fnc.I3;
     rec.flambda = fnc.flambda; rec.fnu = fnc.fnu; rec.phi = phi;
-    fudgeLimitsSetup(fnc, rec);
+    fudgeLimitsSetup(fnc, rec, endF);
     // velocities in prolate spheroidal coordinates (src/coord.cpp:317-322, :525-531)
     const double lambdadot = R * 2 * lambda / sqD * vR + z * 2 * lmd / sqD * vz;
     const double nudot = R * 2 * -absnu / sqD * signz * vR + z * 2 * dmn / sqD * signz * vz;

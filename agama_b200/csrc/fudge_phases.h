@@ -16,9 +16,12 @@ struct BracketWidths { float w[3]; };
 /// phase 2: the root searches of the integration limits, drained by a persistent grid from a
 /// device work counter (8 bytes, zeroed here on the stream); with pred (n x 3 predictions) the
 /// searches start on the predicted brackets; stats (4 counters, may be null) accumulates
-/// searches, narrowed searches, fallbacks to the plain bracket and iterations
-void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, unsigned long long* counter,
-    const float* pred, const BracketWidths& widths, unsigned long long* stats, cudaStream_t stream);
+/// searches, narrowed searches, fallbacks to the plain bracket and iterations; ends (may be null):
+/// F and F' at each record's lambdaPos, which the plain searches of lambda_min and lambda_max take
+/// instead of evaluating that end again
+void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const double2* ends, int* iters,
+    unsigned long long* counter, const float* pred, const BracketWidths& widths, unsigned long long* stats,
+    cudaStream_t stream);
 
 /// training targets of the bracket predictor from records whose plain searches are done
 void launchBracketTargets(long n, const FudgeRecord* rec, float* target, float* mask, cudaStream_t stream);

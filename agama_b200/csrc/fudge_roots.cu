@@ -30,8 +30,9 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
     where F is negative (one more evaluation).  stats (may be null) accumulates {searches,
     narrowed, fallbacks, iterations}. */
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
-    FudgeRecord* __restrict__ rec, int* __restrict__ iters, unsigned long long* __restrict__ counter,
-    const float* __restrict__ pred, const BracketWidths widths, unsigned long long* __restrict__ stats)
+    FudgeRecord* __restrict__ rec, const double2* __restrict__ ends, int* __restrict__ iters,
+    unsigned long long* __restrict__ counter, const float* __restrict__ pred, const BracketWidths widths,
+    unsigned long long* __restrict__ stats)
 {
     const long total = 3 * n;
     const unsigned lane = threadIdx.x & 31;
@@ -103,10 +104,26 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                                 lo = nlo; hi = nhi; narrow = true;
                             }
                         }
-                        x = s.startAbs(lo, hi, tol);
                         nSearch++;
                         nNarrow += narrow;
                         busy = true;
+                        if(narrow || !ends || kind == ROOT_NU_MAX)
+                            x = s.startAbs(lo, hi, tol);
+                        else {
+                            // the plain brackets of lambda_min and lambda_max share the end lambda_pos,
+                            // where phase 1 has F and F' already; the far end of lambda_max (s = 1,
+                            // lambda = inf) needs no evaluation either (limitRootEval's values there)
+                            const double2 e = ends[i];
+                            if(kind == ROOT_LAMBDA_MIN)
+                                x = s.startKnownUpper(lo, hi, tol, e.x, e.y);
+                            else {
+                                const double fa = e.x / pow2(u0), da = (e.y - 2 * e.x / u0) / pow2(u0) * u0;
+                                if(s.startKnownEnds(lo, hi, tol, fa, da, fnc.E, NAN, &x)) {
+                                    busy = false;       // no sign change or a root at an end
+                                    rec[i].lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
+                                }
+                            }
+                        }
                     }
                 }
             }
@@ -207,13 +224,14 @@ int rootGridSize()
 
 }  // namespace
 
-void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, int* iters, unsigned long long* counter,
-    const float* pred, const BracketWidths& widths, unsigned long long* stats, cudaStream_t stream)
+void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const double2* ends, int* iters,
+    unsigned long long* counter, const float* pred, const BracketWidths& widths, unsigned long long* stats,
+    cudaStream_t stream)
 {
     if(n <= 0) return;
     AGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
     const long grid = std::min<long>(rootGridSize(), (3 * n + ROOT_BLOCK - 1) / ROOT_BLOCK);
-    fudgeRootKernel<<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, iters, counter, pred, widths, stats);
+    fudgeRootKernel<<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, pred, widths, stats);
     AGB_CUDA(cudaGetLastError());
 }
 
