@@ -216,14 +216,30 @@ __global__ void gatherKernel(int B, int ncol, const int* __restrict__ idx, const
 constexpr int INF_SMEM = 3 * H * H * 2 + 2048;         // W2, W3, activation tile (BF16) + alignment
 constexpr long INF_MAX_POLLS = 1L << 22;
 
-/** Forward pass of 128 points per CTA iteration, persistent over tiles: thread t owns point t of
-    the tile; layer 1 on the FP32 pipe, the two 128 x 128 layers as tcgen05 MMAs (A = the tile's
-    BF16 activations, B = the BF16 weights, both staged once / per layer in shared memory in the
-    canonical K-major layout, accumulator in 128 tensor-memory columns), SiLU epilogues from
-    tensor-memory loads, layer 4 fused into the last epilogue. */
-__global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __restrict__ xin, float* __restrict__ yout,
-    const float* __restrict__ p, const __nv_bfloat16* __restrict__ w2, const __nv_bfloat16* __restrict__ w3,
-    const float* __restrict__ scale, int* __restrict__ error)
+/// SiLU of the inference kernel: z sigmoid(z) = z/2 (1 + tanh(z/2)) with the single-instruction
+/// hardware tanh approximation (relative error ~2^-11, below the BF16 rounding that follows)
+__device__ __forceinline__ float siluFast(float z)
+{
+    const float hz = 0.5f * z;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(hz));
+    return fmaf(hz, t, hz);
+}
+
+// threads per point (row of a tile): 1, 2 or 4; on B200, 1e6 points took 0.214, 0.218, 0.236 ms
+constexpr int INF_ROW_THREADS = 1;
+constexpr int INF_THREADS = 128 * INF_ROW_THREADS, INF_COLS = H / INF_ROW_THREADS;
+
+/** Forward pass of 128 points per CTA iteration, persistent over tiles, INF_ROW_THREADS threads
+    per point: thread t owns row t % 128 of the tile and the INF_COLS columns starting at
+    INF_COLS (t / 128) (the tensor-memory rows of a warp are those of its warp index modulo 4).  Layer 1 on the FP32 pipe, the
+    two 128 x 128 layers as tcgen05 MMAs (A = the tile's BF16 activations, B = the BF16 weights,
+    both staged in shared memory in the canonical K-major layout, accumulator in 128 tensor-memory
+    columns), SiLU epilogues from tensor-memory loads, layer 4 fused into the last epilogue (the
+    threads of a row add their partial outputs through shared memory). */
+__global__ void __launch_bounds__(INF_THREADS, 2) mlpInferKernel(long n, const float* __restrict__ xin,
+    float* __restrict__ yout, const float* __restrict__ p, const __nv_bfloat16* __restrict__ w2,
+    const __nv_bfloat16* __restrict__ w3, const float* __restrict__ scale, int* __restrict__ error)
 {
     extern __shared__ unsigned char smemRaw[];
     __shared__ uint64_t mbar;
@@ -232,19 +248,21 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
     __shared__ __align__(16) float sW4T[H][4];               // layer-4 weights [unit][output], padded
     __shared__ __align__(16) float sB1[H], sB2[H], sB3[H];
     __shared__ float sB4[NOUT], sScale[2 * NIN + 2 * NOUT];
+    __shared__ float sPart[INF_ROW_THREADS > 1 ? INF_ROW_THREADS - 1 : 1][NOUT][128];  // partial layer-4 sums
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
     unsigned char* tW2 = base;
     unsigned char* tW3 = base + H * H * 2;
     unsigned char* tA = base + 2 * H * H * 2;
-    const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+    const int tid = threadIdx.x, warp = tid / 32, row = tid % 128, half = tid / 128;   // half: the row's column block
+    const int cBegin = half * INF_COLS;
 
-    for(int k = tid; k < H * NIN; k += 128) sW1T[k % NIN][k / NIN] = p[OFF_W1 + k];
-    for(int k = tid; k < H * 4; k += 128) sW4T[k / 4][k % 4] = k % 4 < NOUT ? p[OFF_W4 + (k % 4) * H + k / 4] : 0.f;
-    for(int k = tid; k < H; k += 128) { sB1[k] = p[OFF_B1 + k]; sB2[k] = p[OFF_B2 + k]; sB3[k] = p[OFF_B3 + k]; }
+    for(int k = tid; k < H * NIN; k += INF_THREADS) sW1T[k % NIN][k / NIN] = p[OFF_W1 + k];
+    for(int k = tid; k < H * 4; k += INF_THREADS) sW4T[k / 4][k % 4] = k % 4 < NOUT ? p[OFF_W4 + (k % 4) * H + k / 4] : 0.f;
+    for(int k = tid; k < H; k += INF_THREADS) { sB1[k] = p[OFF_B1 + k]; sB2[k] = p[OFF_B2 + k]; sB3[k] = p[OFF_B3 + k]; }
     if(tid < NOUT) sB4[tid] = p[OFF_B4 + tid];
     if(tid < 2 * NIN + 2 * NOUT) sScale[tid] = scale[tid];
     // weights into the canonical layout: row o (output unit) = MMA "B" row, K = input unit
-    for(int v = tid; v < H * H / 8; v += 128) {
+    for(int v = tid; v < H * H / 8; v += INF_THREADS) {
         const int r = v / (H / 8), kc = v % (H / 8);
         const uint32_t off = umma::tileOffset(r, kc * 8, H);
         *reinterpret_cast<uint4*>(tW2 + off) = *reinterpret_cast<const uint4*>(w2 + r * H + kc * 8);
@@ -256,15 +274,14 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
     __syncthreads();
     umma::fenceAfterSync();
     const uint32_t tmem = tmemBase;
-    const uint32_t tmemRow = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t tmemRow = tmem + (static_cast<uint32_t>((warp % 4) * 32) << 16);
     constexpr uint32_t idesc = umma::instrDescBf16(128, H);
     constexpr uint32_t SBO = H / 8 * umma::CORE_BYTES;
     uint32_t parity = 0;
     bool ok = true;
 
-    // write this thread's 128 activations (row tid of the tile) as BF16 in the canonical layout
+    // write 32 activations of this thread's row (columns c0..c0+31) as BF16 in the canonical layout
     auto storeRow = [&](const float* h, int c0) {
-        // h holds 32 values for columns c0..c0+31: four 16-byte vectors of 8 BF16
 #pragma unroll
         for(int q = 0; q < 4; q++) {
             uint4 v;
@@ -273,7 +290,7 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
             for(int e = 0; e < 4; e++) p2[e] = __floats2bfloat162_rn(h[q * 8 + 2 * e], h[q * 8 + 2 * e + 1]);
             v.x = *reinterpret_cast<uint32_t*>(&p2[0]); v.y = *reinterpret_cast<uint32_t*>(&p2[1]);
             v.z = *reinterpret_cast<uint32_t*>(&p2[2]); v.w = *reinterpret_cast<uint32_t*>(&p2[3]);
-            *reinterpret_cast<uint4*>(tA + umma::tileOffset(tid, c0 + q * 8, H)) = v;
+            *reinterpret_cast<uint4*>(tA + umma::tileOffset(row, c0 + q * 8, H)) = v;
         }
     };
     auto runLayer = [&](unsigned char* tW) {
@@ -294,11 +311,11 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
 
     const long tiles = (n + 127) / 128;
     for(long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-        const long i = tile * 128 + tid;
+        const long i = tile * 128 + row;
         const bool valid = i < n;
         float x[NIN];
         for(int k = 0; k < NIN; k++) x[k] = valid ? (xin[i * NIN + k] - sScale[k]) / sScale[NIN + k] : 0.f;
-        for(int c0 = 0; c0 < H; c0 += 32) {
+        for(int c0 = cBegin; c0 < cBegin + INF_COLS; c0 += 32) {
             float h[32];
 #pragma unroll
             for(int c = 0; c < 32; c += 4) {
@@ -308,20 +325,20 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
                     const float4 w = *reinterpret_cast<const float4*>(&sW1T[k][c0 + c]);
                     acc.x += x[k] * w.x; acc.y += x[k] * w.y; acc.z += x[k] * w.z; acc.w += x[k] * w.w;
                 }
-                h[c] = silu(acc.x); h[c + 1] = silu(acc.y); h[c + 2] = silu(acc.z); h[c + 3] = silu(acc.w);
+                h[c] = siluFast(acc.x); h[c + 1] = siluFast(acc.y); h[c + 2] = siluFast(acc.z); h[c + 3] = siluFast(acc.w);
             }
             storeRow(h, c0);
         }
         runLayer(tW2);
         if(!ok) break;
-        for(int c0 = 0; c0 < H; c0 += 32) {
+        for(int c0 = cBegin; c0 < cBegin + INF_COLS; c0 += 32) {
             float h[32];
             umma::tmemLoad32(tmemRow + c0, h);
 #pragma unroll
             for(int c = 0; c < 32; c += 4) {
                 const float4 b = *reinterpret_cast<const float4*>(&sB2[c0 + c]);
-                h[c] = silu(h[c] + b.x); h[c + 1] = silu(h[c + 1] + b.y);
-                h[c + 2] = silu(h[c + 2] + b.z); h[c + 3] = silu(h[c + 3] + b.w);
+                h[c] = siluFast(h[c] + b.x); h[c + 1] = siluFast(h[c + 1] + b.y);
+                h[c + 2] = siluFast(h[c + 2] + b.z); h[c + 3] = siluFast(h[c + 3] + b.w);
             }
             storeRow(h, c0);
         }
@@ -329,21 +346,27 @@ __global__ void __launch_bounds__(128) mlpInferKernel(long n, const float* __res
         runLayer(tW3);
         if(!ok) break;
         float y[NOUT];
-        for(int j = 0; j < NOUT; j++) y[j] = sB4[j];
-        for(int c0 = 0; c0 < H; c0 += 32) {
+        for(int j = 0; j < NOUT; j++) y[j] = half == 0 ? sB4[j] : 0.f;
+        for(int c0 = cBegin; c0 < cBegin + INF_COLS; c0 += 32) {
             float h[32];
             umma::tmemLoad32(tmemRow + c0, h);
 #pragma unroll
             for(int c = 0; c < 32; c++) {
-                const float a = silu(h[c] + sB3[c0 + c]);
+                const float a = siluFast(h[c] + sB3[c0 + c]);
                 const float4 w = *reinterpret_cast<const float4*>(&sW4T[c0 + c][0]);
                 y[0] += a * w.x; y[1] += a * w.y; y[2] += a * w.z;
             }
         }
-        if(valid)
-            for(int j = 0; j < NOUT; j++) yout[i * NOUT + j] = y[j] * sScale[2 * NIN + NOUT + j] + sScale[2 * NIN + j];
+        if(half > 0)
+            for(int j = 0; j < NOUT; j++) sPart[half - 1][j][row] = y[j];
         umma::fenceBeforeSync();
-        __syncthreads();        // the tile's activations are rewritten by the next iteration
+        __syncthreads();        // the partial sums are in place; the tile's activations may be rewritten
+        if(half == 0 && valid)
+            for(int j = 0; j < NOUT; j++) {
+                float v = y[j];
+                for(int q = 0; q < INF_ROW_THREADS - 1; q++) v += sPart[q][j][row];
+                yout[i * NOUT + j] = v * sScale[2 * NIN + NOUT + j] + sScale[2 * NIN + j];
+            }
     }
     if(!ok && tid == 0) atomicExch(error, 1);
     umma::fenceBeforeSync();
@@ -555,7 +578,7 @@ void Mlp::predict(long n, const float* x, float* y, cudaStream_t s) const
     AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const long tiles = (n + 127) / 128;
     const int grid = static_cast<int>(std::min<long>(tiles, 2L * sms));
-    mlpInferKernel<<<grid, 128, INF_SMEM, s>>>(n, x, y, params.ptr, reinterpret_cast<const __nv_bfloat16*>(w2.ptr),
+    mlpInferKernel<<<grid, INF_THREADS, INF_SMEM, s>>>(n, x, y, params.ptr, reinterpret_cast<const __nv_bfloat16*>(w2.ptr),
         reinterpret_cast<const __nv_bfloat16*>(w3.ptr), scaling.ptr, error.ptr);
     AGB_CUDA(cudaGetLastError());
 }
