@@ -78,12 +78,12 @@ constexpr long POINTS_PER_PASS = 1L << 20;     // records of one pass: 128 MB of
 /// limits that need no root search and the brackets of those that do -> one record per point.
 /// Jphi (and NaN Jr, Jz of points without actions) are written directly.  Optional outputs:
 /// Delta used, root-finder iterations (zeroed here, counted by phase 2).  ends[i]: F and F' at the
-/// record's lambdaPos, for the root searches.
+/// ends of the record's plain root brackets, for the root searches.
 template<bool FINDER>
 __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __grid_constant__ MultipoleView M,
     const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd,
     double fd0, FudgeRecord* __restrict__ rec, double* __restrict__ act, double* __restrict__ fdOut,
-    int* __restrict__ iters, float* __restrict__ features, double2* __restrict__ ends)
+    int* __restrict__ iters, float* __restrict__ features, FudgeEnds* __restrict__ ends)
 {
     const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
     if(i >= n) return;
@@ -95,10 +95,11 @@ __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __g
     evalMultipoleCylCall<1, EVAL_AXI>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
     const double delta = FINDER ? finderFocalDistance(F, pc, Phi) : (fd ? fd[i] : fd0);
     FudgeRecord r;
-    double a[3], endF[2] = { 0, 0 };
-    fudgePrepare(M, pc, Phi, delta, r, a, endF);
+    double a[3];
+    FudgeEnds e;
+    fudgePrepare(M, pc, Phi, delta, r, a, &e);
     rec[i] = r;
-    ends[i] = make_double2(endF[0], endF[1]);
+    if(r.valid) ends[i] = e;
     act[3 * i + 2] = a[2];
     if(!r.valid) { act[3 * i] = a[0]; act[3 * i + 1] = a[1]; }
     if(fdOut) fdOut[i] = delta;
@@ -131,12 +132,12 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
     const bool predict = bp && bp->net;
     // records, two work counters, the actions of a pass when the caller wants none, and the
     // predictor's inputs and outputs
-    const size_t recBytes = pass * (sizeof(FudgeRecord) + sizeof(double2)) + 256;
+    const size_t recBytes = pass * (sizeof(FudgeRecord) + sizeof(FudgeEnds)) + 256;
     const size_t actBytes = act ? 0 : pass * 3 * sizeof(double);
     const size_t featBytes = (predict ? pass * 9 * sizeof(float) : 0) + 256;
     Scratch scratch(recBytes + actBytes + featBytes, stream);
     FudgeRecord* rec = static_cast<FudgeRecord*>(scratch.ptr);
-    double2* ends = reinterpret_cast<double2*>(rec + pass);
+    FudgeEnds* ends = reinterpret_cast<FudgeEnds*>(rec + pass);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(ends + pass);
     double* actTmp = reinterpret_cast<double*>(static_cast<char*>(scratch.ptr) + recBytes);
     float* feat = predict ? reinterpret_cast<float*>(static_cast<char*>(scratch.ptr) + recBytes + actBytes) : nullptr;

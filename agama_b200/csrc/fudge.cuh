@@ -172,6 +172,12 @@ static_assert(sizeof(FudgeRecord) == 128, "FudgeRecord is one 128-byte line");
 
 enum { ROOT_NU_MAX = 1, ROOT_LAMBDA_MIN = 2, ROOT_LAMBDA_MAX = 4 };
 
+/// F and F' at the ends of the plain root brackets that phase 1 evaluates once for the searches of
+/// phase 2: lambda_pos (shared by the lambda_min and lambda_max brackets), Delta^2 (the upper end
+/// of the nu_max bracket and the lower end of the lambda_min one) and |nu| (the lower end of the
+/// nu_max bracket); NaN where not evaluated
+struct FudgeEnds { double fPos, dfPos, fD2, dfD2, fNu, dfNu; };
+
 /** The root functions of the three integration limits behind one evaluation site (kind
     ROOT_NU_MAX, ROOT_LAMBDA_MIN: F(tau) and F'(tau); ROOT_LAMBDA_MAX: F(tau)/tau^2 on
     [u0, inf) mapped to s in [0, 1] by the semi-infinite scaling, AxisymScaledForRootfinder inside
@@ -204,9 +210,10 @@ __device__ __forceinline__ void loadFudgeFunction(const MultipoleView& M, const 
 /** Integration limits of the lambda and nu motions (findIntegrationLimitsAxisym,
     src/actions_staeckel.cpp:360-483), part 1: every decision up to the three root searches, whose
     brackets go into the record; limits that need no root are stored directly (NaN otherwise).
-    endF (may be null) receives F and F' at lambda_pos, the end that the brackets of lambda_min and
-    lambda_max share, which the root searches then take instead of evaluating it again. */
-static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& rec, double* endF = nullptr)
+    ends (may be null) receives F and F' at the ends of the plain brackets (FudgeEnds), which the
+    root searches then take instead of evaluating them: at lambda_pos from the evaluation above,
+    at Delta^2 and |nu| from the same evaluation of F as the searches would make. */
+static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& rec, FudgeEnds* ends = nullptr)
 {
     const double delta = fnc.D2;
     const double f_zero = fnc.value(0);
@@ -254,7 +261,14 @@ static __device__ void fudgeLimitsSetup(const FudgeFunction& fnc, FudgeRecord& r
     rec.nuMax = nu_max; rec.lambdaMin = lambda_min; rec.lambdaMax = lambda_max;
     rec.nuUpper = nu_upper; rec.lambdaLower = lambda_lower; rec.lambdaPos = lambda_pos;
     rec.roots = roots;
-    if(endF) { endF[0] = f_pos; endF[1] = df_pos; }
+    if(ends) {
+        ends->fPos = f_pos; ends->dfPos = df_pos;
+        ends->fD2 = ends->dfD2 = ends->fNu = ends->dfNu = NAN;
+        if(((roots & ROOT_NU_MAX) && nu_upper == delta) || ((roots & ROOT_LAMBDA_MIN) && lambda_lower == delta))
+            fnc.eval<true, false>(delta, &ends->fD2, &ends->dfD2, nullptr);
+        if(roots & ROOT_NU_MAX)
+            fnc.eval<true, false>(fabs(fnc.nu), &ends->fNu, &ends->dfNu, nullptr);
+    }
 }
 
 struct FudgeLimits { double lambda_min, lambda_max, nu_max; int order; };
@@ -298,9 +312,9 @@ static __device__ double fudgeMomentumNode(const FudgeFunction& fnc, double lo, 
     Phi is the potential at the point.  Writes Jphi into act[2]; for a point without actions
     (unbound, or lambda = nu = Delta^2) also NaN into act[0..1] and marks the record invalid.
     Otherwise the record holds the integrals of motion (findIntegralsOfMotionAxisymFudge,
-    :176-195) and the limits and root brackets of fudgeLimitsSetup (endF: as there). */
+    :176-195) and the limits and root brackets of fudgeLimitsSetup (ends: as there). */
 static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, double Phi, double fd,
-    FudgeRecord& rec, double* act, double* endF = nullptr)
+    FudgeRecord& rec, double* act, FudgeEnds* ends = nullptr)
 {
     const double R = pc[0], z = pc[1], phi = pc[2], vR = pc[3], vz = pc[4], vphi = pc[5];
     if(fd <= 0) fd = fmax(R, 1.) * 1e-4;
@@ -341,7 +355,7 @@ static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, do
     if(!isFinite(fnc.E + fnc.I3 + fnc.Lz) || fnc.E >= 0) { act[0] = act[1] = NAN; return; }
     rec.lambda = fnc.lambda; rec.nu = fnc.nu; rec.D2 = D2; rec.E = fnc.E; rec.Lz = Lz; rec.I3 = fnc.I3;
     rec.flambda = fnc.flambda; rec.fnu = fnc.fnu; rec.phi = phi;
-    fudgeLimitsSetup(fnc, rec, endF);
+    fudgeLimitsSetup(fnc, rec, ends);
     // velocities in prolate spheroidal coordinates (src/coord.cpp:317-322, :525-531)
     const double lambdadot = R * 2 * lambda / sqD * vR + z * 2 * lmd / sqD * vz;
     const double nudot = R * 2 * -absnu / sqD * signz * vR + z * 2 * dmn / sqD * signz * vz;

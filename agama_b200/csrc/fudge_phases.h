@@ -8,6 +8,7 @@
 namespace agb {
 
 struct FudgeRecord;
+struct FudgeEnds;
 
 /// half-widths of the predicted brackets, in units of the predicted fractions (order of the ROOT_*
 /// kinds: nu_max, lambda_min, lambda_max)
@@ -17,9 +18,9 @@ struct BracketWidths { float w[3]; };
 /// device work counter (8 bytes, zeroed here on the stream); with pred (n x 3 predictions) the
 /// searches start on the predicted brackets; stats (4 counters, may be null) accumulates
 /// searches, narrowed searches, fallbacks to the plain bracket and iterations; ends (may be null):
-/// F and F' at each record's lambdaPos, which the plain searches of lambda_min and lambda_max take
-/// instead of evaluating that end again
-void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const double2* ends, int* iters,
+/// F and F' at the ends of each record's plain brackets, which the plain searches take instead of
+/// evaluating them again
+void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const FudgeEnds* ends, int* iters,
     unsigned long long* counter, const float* pred, const BracketWidths& widths, unsigned long long* stats,
     cudaStream_t stream);
 

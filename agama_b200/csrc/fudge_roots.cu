@@ -15,6 +15,38 @@ namespace {
 constexpr int ROOT_BLOCK = 128;
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
+/// the limit found by a plain search (nu_max falls back to |nu| when the search found no root)
+__device__ __forceinline__ void storePlainLimit(FudgeRecord& r, int kind, const RootSearch& s, double u0, double nu)
+{
+    if(kind == ROOT_NU_MAX) r.nuMax = isFinite(s.result) ? s.result : fabs(nu);
+    else if(kind == ROOT_LAMBDA_MIN) r.lambdaMin = s.result;
+    else r.lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
+}
+
+/** Start a plain search on its bracket [lo, hi] with F and F' at the ends taken from phase 1
+    (e may be null: the ends are then evaluated by the search): lambda_pos (shared by the lambda
+    brackets), Delta^2 and |nu|; the far end of lambda_max (s = 1, lambda = inf) needs no
+    evaluation either (limitRootEval's values there).  True when the search has finished at once
+    (no sign change, or a root at an end); otherwise *x is the first point to evaluate. */
+__device__ __forceinline__ bool startPlain(RootSearch& s, int kind, const FudgeEnds* e, double lo, double hi,
+    double tol, double u0, double D2, double E, double* x)
+{
+    if(!e) { *x = s.startAbs(lo, hi, tol); return false; }
+    if(kind == ROOT_NU_MAX) {
+        if(hi == D2) return s.startKnownEnds(lo, hi, tol, e->fNu, e->dfNu, e->fD2, e->dfD2, x);
+        *x = s.startAbs(lo, hi, tol);
+        s.feed(e->fNu, e->dfNu, x);         // the lower end known; the upper one is evaluated next
+        return false;
+    }
+    if(kind == ROOT_LAMBDA_MIN) {
+        if(lo == D2) return s.startKnownEnds(lo, hi, tol, e->fD2, e->dfD2, e->fPos, e->dfPos, x);
+        *x = s.startKnownUpper(lo, hi, tol, e->fPos, e->dfPos);
+        return false;
+    }
+    const double fa = e->fPos / pow2(u0), da = (e->dfPos - 2 * e->fPos / u0) / pow2(u0) * u0;
+    return s.startKnownEnds(lo, hi, tol, fa, da, E, NAN, x);
+}
+
 /** Phase 2: every root search of the integration limits (task t = kind * n + i for the kinds
     nu_max, lambda_min, lambda_max of point i) drained from one work counter by a persistent grid.
     Each lane runs one search as a RootSearch state machine and takes the next task as soon as
@@ -30,7 +62,7 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
     where F is negative (one more evaluation).  stats (may be null) accumulates {searches,
     narrowed, fallbacks, iterations}. */
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
-    FudgeRecord* __restrict__ rec, const double2* __restrict__ ends, int* __restrict__ iters,
+    FudgeRecord* __restrict__ rec, const FudgeEnds* __restrict__ ends, int* __restrict__ iters,
     unsigned long long* __restrict__ counter, const float* __restrict__ pred, const BracketWidths widths,
     unsigned long long* __restrict__ stats)
 {
@@ -107,22 +139,12 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         nSearch++;
                         nNarrow += narrow;
                         busy = true;
-                        if(narrow || !ends || kind == ROOT_NU_MAX)
-                            x = s.startAbs(lo, hi, tol);
-                        else {
-                            // the plain brackets of lambda_min and lambda_max share the end lambda_pos,
-                            // where phase 1 has F and F' already; the far end of lambda_max (s = 1,
-                            // lambda = inf) needs no evaluation either (limitRootEval's values there)
-                            const double2 e = ends[i];
-                            if(kind == ROOT_LAMBDA_MIN)
-                                x = s.startKnownUpper(lo, hi, tol, e.x, e.y);
-                            else {
-                                const double fa = e.x / pow2(u0), da = (e.y - 2 * e.x / u0) / pow2(u0) * u0;
-                                if(s.startKnownEnds(lo, hi, tol, fa, da, fnc.E, NAN, &x)) {
-                                    busy = false;       // no sign change or a root at an end
-                                    rec[i].lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
-                                }
-                            }
+                        bool done = false;
+                        if(narrow) x = s.startAbs(lo, hi, tol);
+                        else done = startPlain(s, kind, ends ? ends + i : nullptr, lo, hi, tol, u0, r.D2, r.E, &x);
+                        if(done) {      // no sign change or a root at an end
+                            busy = false;
+                            storePlainLimit(rec[i], kind, s, u0, fnc.nu);
                         }
                     }
                 }
@@ -150,24 +172,27 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                 } else {
                     narrow = false;
                     nFallback++;
-                    x = s.startAbs(plainLo, plainHi, tol);
+                    if(startPlain(s, kind, ends ? ends + point : nullptr, plainLo, plainHi, tol, u0, fnc.D2, fnc.E, &x)) {
+                        busy = false;
+                        storePlainLimit(rec[point], kind, s, u0, fnc.nu);
+                    }
                 }
             } else if(s.feed(fx, dx, &x)) {
                 nIter += s.iter;
                 if(narrow && !isFinite(s.result)) {     // the predicted bracket missed: plain search
                     narrow = false;
                     nFallback++;
-                    x = s.startAbs(plainLo, plainHi, tol);
+                    if(startPlain(s, kind, ends ? ends + point : nullptr, plainLo, plainHi, tol, u0, fnc.D2, fnc.E, &x)) {
+                        busy = false;
+                        storePlainLimit(rec[point], kind, s, u0, fnc.nu);
+                    }
                 } else if(narrow) {
                     verifying = true;
                     verified = s.result;
                     x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? plainLo : plainHi));
                 } else {
                     busy = false;
-                    FudgeRecord& r = rec[point];
-                    if(kind == ROOT_NU_MAX) r.nuMax = isFinite(s.result) ? s.result : fabs(fnc.nu);
-                    else if(kind == ROOT_LAMBDA_MIN) r.lambdaMin = s.result;
-                    else r.lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
+                    storePlainLimit(rec[point], kind, s, u0, fnc.nu);
                     if(iters) atomicAdd(iters + point, s.iter);
                 }
             }
@@ -224,7 +249,7 @@ int rootGridSize()
 
 }  // namespace
 
-void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const double2* ends, int* iters,
+void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const FudgeEnds* ends, int* iters,
     unsigned long long* counter, const float* pred, const BracketWidths& widths, unsigned long long* stats,
     cudaStream_t stream)
 {
