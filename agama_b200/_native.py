@@ -47,6 +47,7 @@ SIGNATURES = {
                                                               ctypes.c_double, ctypes.c_long, VP, VP, VP, VP,
                                                               ctypes.c_int, VP]),
     "agama_measureFP64Throughput": (ctypes.c_int, [D]),
+    "agama_actionPhaseTiming": (ctypes.c_int, [ctypes.c_int, D, L]),
     "agama_actionFinderBracketSamples": (ctypes.c_int, [VP, ctypes.c_long, D, F, F, F]),
     "agama_actionFinderTrainBrackets": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_int, ctypes.c_int,
                                                        ctypes.c_float, ctypes.c_ulonglong, F, F]),

@@ -1,5 +1,8 @@
 // Staeckel-fudge action kernels, the device-resident action finder and their host launchers.
 #include "runtime.h"
+#include <array>
+#include <mutex>
+#include <vector>
 #include "fudge.cuh"
 #include "host_pipeline.h"
 #include "fudge_phases.h"
@@ -117,6 +120,27 @@ __global__ void __launch_bounds__(PREPARE_BLOCK, 3) fudgePrepareKernel(const __g
     }
 }
 
+/// Optional timing of the phases: while on, every pass records CUDA events on its stream before
+/// and after each phase (prepare, bracket inference, root searches, integrals); the durations are
+/// read and summed when the timing is switched off.
+struct PhaseTimer {
+    std::mutex mutex;
+    bool on = false;
+    std::vector<std::array<cudaEvent_t, 5>> passes;
+};
+PhaseTimer g_phaseTimer;
+
+/// events of one pass, or null when the timing is off
+std::array<cudaEvent_t, 5>* phaseEvents()
+{
+    std::lock_guard<std::mutex> lock(g_phaseTimer.mutex);
+    if(!g_phaseTimer.on) return nullptr;
+    std::array<cudaEvent_t, 5> ev;
+    for(auto& e : ev) AGB_CUDA(cudaEventCreate(&e));
+    g_phaseTimer.passes.push_back(ev);
+    return &g_phaseTimer.passes.back();
+}
+
 /// the three phases over passes of at most POINTS_PER_PASS points (bounded scratch); with ang or
 /// freq the last phase also computes angles / frequencies (act may then be null).  With a
 /// bracket predictor (bp), phase 1 also writes its inputs and the root searches start on its
@@ -147,6 +171,11 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
     if(predict) for(int k = 0; k < 3; k++) widths.w[k] = bp->widths[k];
     for(long first = 0; first < n; first += pass) {
         const long count = std::min(pass, n - first);
+        std::array<cudaEvent_t, 5> ev;
+        bool timed = false;
+        if(auto* e = phaseEvents()) { ev = *e; timed = true; }
+        auto mark = [&](int k) { if(timed) AGB_CUDA(cudaEventRecord(ev[k], stream)); };
+        mark(0);
         int* it = iters ? iters + first : nullptr;
         double* a = act ? act + 3 * first : actTmp;
         float* f = samples ? samples->features + 6 * first : feat;
@@ -154,8 +183,11 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
             M, F, count, posvel + 6 * first, fd ? fd + first : nullptr, fd0, rec, a,
             fdOut ? fdOut + first : nullptr, it, f, ends);
         AGB_CUDA(cudaGetLastError());
+        mark(1);
         if(predict) bp->net->predict(count, feat, pred, stream);
+        mark(2);
         launchFudgeRoots(M, count, rec, ends, it, counter, pred, widths, bp ? bp->stats : nullptr, stream);
+        mark(3);
         if(samples)
             launchBracketTargets(count, rec, samples->target + 3 * first, samples->mask + 3 * first, stream);
         else if(angles)
@@ -163,10 +195,33 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
                 freq ? freq + 3 * first : nullptr, stream);
         else
             launchFudgeIntegrals(M, gl, count, rec, a, counter + 1, stream);
+        mark(4);
     }
 }
 
 }  // namespace
+
+void setActionPhaseTiming(bool on, double* ms, long* passes)
+{
+    std::lock_guard<std::mutex> lock(g_phaseTimer.mutex);
+    if(!on) {
+        double sum[4] = { 0, 0, 0, 0 };
+        for(auto& ev : g_phaseTimer.passes) {
+            AGB_CUDA(cudaEventSynchronize(ev[4]));
+            for(int k = 0; k < 4; k++) {
+                float t = 0;
+                AGB_CUDA(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+                sum[k] += t;
+            }
+        }
+        if(ms) for(int k = 0; k < 4; k++) ms[k] = sum[k];
+        if(passes) *passes = static_cast<long>(g_phaseTimer.passes.size());
+    }
+    for(auto& ev : g_phaseTimer.passes)
+        for(auto& e : ev) cudaEventDestroy(e);
+    g_phaseTimer.passes.clear();
+    g_phaseTimer.on = on;
+}
 
 void launchActionsFixedDelta(const MultipoleView& M, long n, const double* posvel, const double* fd, double fd0,
     double* act, double* ang, double* freq, int* iters, cudaStream_t stream)

@@ -863,6 +863,11 @@ __global__ void fp64FmaProbe(double* out, int iters)
 }
 }  // namespace
 
+extern "C" int agama_actionPhaseTiming(int on, double* ms, long* passes)
+{
+    return guarded([&] { setActionPhaseTiming(on != 0, ms, passes); });
+}
+
 extern "C" int agama_measureFP64Throughput(double* tflops)
 {
     return guarded([&] {

@@ -83,6 +83,10 @@ void launchEvalPotential(const MultipoleView& M, long n, const double* pos, doub
 /// DOP853 batch; queue != nullptr selects the persistent work-queue mapping (8-byte counter)
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes = 0);
+/// phase timing of the action computation: on = true clears and starts recording; on = false
+/// stops and returns the summed device durations (ms) of prepare, bracket inference, root
+/// searches and integrals, and the number of passes timed
+void setActionPhaseTiming(bool on, double* ms, long* passes);
 /// lanes per orbit for all later batches: 1, 2, 4, 8, or 0 (default) for the autotuner
 void setOrbitLanes(int lanes);
 /// mixed precision for later batches in multi-harmonic potentials: the m != 0 harmonics of the

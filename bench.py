@@ -492,12 +492,17 @@ def run_engine(args):
     torch.cuda.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    import ctypes
+    _native.check(lib.agama_actionPhaseTiming(1, None, None))     # CUDA events around each phase
     for k in range(args.steps):
         flush.zero_()
         starts[k].record(stream)
         step()
         ends[k].record(stream)
     torch.cuda.synchronize()
+    phase_ms, phase_passes = (ctypes.c_double * 4)(), ctypes.c_long(0)
+    _native.check(lib.agama_actionPhaseTiming(0, phase_ms, ctypes.byref(phase_passes)))
+    phase_ms = [phase_ms[k] / args.steps for k in range(4)]
     if dist:
         dist.barrier()
     clocks = sampler.stop(physical_gpu_index(local)) if rank == 0 else None
@@ -528,13 +533,13 @@ def run_engine(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = n * world / (float(t.item()) / 1000)
     if rank == 0:
-        # ---- roofline of the action kernels (FP64-pipe bound): executed FP64 flops per action
-        # from an ncu capture of this workload; peak measured on this device
-        import ctypes
+        # ---- roofline (FP64-pipe bound): the dominant kernel (root searches), timed by CUDA events
+        # around it during the timed steps, and the whole three-kernel step; executed FP64 flops
+        # per action from an ncu capture of this workload; peak measured on this device
         pk = ctypes.c_double(0)
         _native.check(lib.agama_measureFP64Throughput(ctypes.byref(pk)))
-        flops_per_action = FLOPS_PER_ACTION_CFG2
-        achieved = flops_per_action * n / (ms_per_step / 1000) / 1e12
+        achieved = FLOPS_ROOT_PER_ACTION_CFG2 * n / (phase_ms[2] / 1000) / 1e12
+        step_achieved = FLOPS_PER_ACTION_CFG2 * n / (ms_per_step / 1000) / 1e12
         line = {
             "metric": METRIC, "value": value, "unit": "actions/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -544,10 +549,16 @@ def run_engine(args):
             "e2e": {"value": e2e_val, "unit": "actions/s", "h2d_bytes_per_step": int(pts.nbytes),
                     "d2h_bytes_per_step": int(n * 3 * 8)},
             "gpu_launches": ACTION_LAUNCHES_PER_STEP * args.steps,
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": pk.value, "unit": "TFLOP/s",
-                         "frac": achieved / pk.value if pk.value else None, "traffic": TRAFFIC_PER_LAUNCH_CFG2,
+            "roofline": {"bound": "fp64", "kernel": "fudgeRootKernel", "achieved": achieved, "peak": pk.value,
+                         "unit": "TFLOP/s", "frac": achieved / pk.value if pk.value else None,
+                         "traffic": TRAFFIC_ROOT_PER_LAUNCH_CFG2, "ms_per_launch": phase_ms[2],
+                         "flops_per_action": FLOPS_ROOT_PER_ACTION_CFG2,
                          "peak_source": "measured FP64 FMA throughput of this device (agama_measureFP64Throughput)",
-                         "flops_per_action": flops_per_action},
+                         "step": {"kernels": 3, "achieved": step_achieved,
+                                  "frac": step_achieved / pk.value if pk.value else None,
+                                  "flops_per_action": FLOPS_PER_ACTION_CFG2, "traffic": TRAFFIC_PER_STEP_CFG2,
+                                  "phase_ms": {"prepare": phase_ms[0], "roots": phase_ms[2],
+                                               "integrals": phase_ms[3]}}},
             "clocks": clocks,
             "cpu_baseline": None if args.no_baseline else cpu_baseline_line(pts),
         }
@@ -565,12 +576,14 @@ def run_engine(args):
 
 # kernels per action step: prepare, root searches, integrals
 ACTION_LAUNCHES_PER_STEP = 3
-# executed FP64 flops per action (dadd + dmul + 2 dfma summed over the five kernels, ncu, config-2
-# workload) and DRAM bytes of one step for 1e6 particles
-FLOPS_PER_ACTION_CFG2 = 26508.0
-# dram read + write of the three kernels of one 200 000-particle step (prepare 11.00 + 1.79 MB,
-# roots 25.76 + 22.79 MB, integrals 26.00 + 0.01 MB), scaled to 1e6 particles
-TRAFFIC_PER_LAUNCH_CFG2 = 5 * 87.35e6
+# executed FP64 flops per action (dadd + dmul + 2 dfma, ncu, config-2 workload, 200 000 particles):
+# prepare 3874, root searches 11014, integrals 9667
+FLOPS_ROOT_PER_ACTION_CFG2 = 11014.0
+FLOPS_PER_ACTION_CFG2 = 3874.0 + 11014.0 + 9667.0
+# dram read + write of one 200 000-particle step (prepare 11.11 + 4.57 MB, roots 39.04 + 82.31 MB,
+# integrals 26.00 + 0.00 MB), scaled to 1e6 particles (the traffic grows with the particles)
+TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 121.35e6
+TRAFFIC_PER_STEP_CFG2 = 5 * 163.03e6
 
 
 def ctypes_stream(stream):

@@ -311,6 +311,13 @@ int agama_mlpCheck(const agama_Mlp* net);
    of the FP64-bound kernels above. */
 int agama_measureFP64Throughput(double* tflops);
 
+/* Phase timing of the action computation (no reference counterpart): on = 1 clears and starts
+   recording CUDA events around the phases of every later action call (on the call's stream);
+   on = 0 stops, waits for the recorded events and returns in ms[4] the summed device durations of
+   the phases (prepare, bracket-network inference, root searches, integrals / angles) and in
+   *passes the number of passes timed (ms, passes may be null). */
+int agama_actionPhaseTiming(int on, double* ms, long* passes);
+
 #ifdef __cplusplus
 }
 #endif
