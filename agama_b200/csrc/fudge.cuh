@@ -103,8 +103,9 @@ struct FudgeFunction {
     double E, Lz, I3, flambda, fnu;
     int bad;                        // set when a coordinate conversion is invalid
 
-    /// F(tau) and optionally F', F'' (src/actions_staeckel.cpp:202-252)
-    template<bool DER, bool DER2>
+    /// F(tau) and optionally F', F'' (src/actions_staeckel.cpp:202-252); INL: the potential
+    /// evaluation inlined at this call site instead of the shared out-of-line copy
+    template<bool DER, bool DER2, bool INL = false>
     __device__ void eval(double tau, double* val, double* der, double* der2) const
     {
         double lam, n, mult, I;
@@ -121,7 +122,8 @@ struct FudgeFunction {
         const double z = sqrt(lam * absnu / D2) * sgn;
         double Phi;
         CylDerivs g; CylHess h;
-        if(DER2)     evalMultipoleCylCall<6, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
+        if(INL)      evalMultipoleCyl<DER2 ? 6 : DER ? 3 : 1, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
+        else if(DER2) evalMultipoleCylCall<6, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         else if(DER) evalMultipoleCylCall<3, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         else         evalMultipoleCylCall<1, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         const double tmd = tau - D2;
@@ -148,7 +150,7 @@ struct FudgeFunction {
             }
         }
     }
-    __device__ double value(double tau) const { double v; eval<false, false>(tau, &v, nullptr, nullptr); return v; }
+    __device__ double value(double tau) const { double v; eval<false, false, true>(tau, &v, nullptr, nullptr); return v; }
 };
 
 /// State of one point between the phases of the action computation: the point in prolate
@@ -190,7 +192,7 @@ __device__ __forceinline__ void limitRootEval(const FudgeFunction& f, int kind, 
     if(semiInf) tau = unscaleSemiInf(u0, x, &duds);
     const bool far = semiInf && tau > 1e100;
     double fval = 0, fder = 0;
-    if(!far) f.eval<true, false>(tau, &fval, &fder, nullptr);
+    if(!far) f.eval<true, false, true>(tau, &fval, &fder, nullptr);
     if(!semiInf) { *v = fval; *d = fder; }
     else if(far) { *v = f.E; *d = NAN; }
     else {
