@@ -82,7 +82,7 @@ constexpr double fdec = 0.333, finc = 6.0, safe = 0.9;   // step-size control
     G > 1: called together by a group of G lanes with the same point, which share the spline
     evaluations (the multi-harmonic evaluator kind only). */
 template<int NQ, int KIND, int G = 1, bool MIXED = false>
-__device__ __noinline__ void orbitRHS(const MultipoleView& M, double Omega, double time,
+__device__ __forceinline__ void orbitRHS(const MultipoleView& M, double Omega, double time,
     const double* xv, double* dxdt, double* accFac)
 {
     double ca = 1, sa = 0;
