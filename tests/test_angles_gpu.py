@@ -61,8 +61,13 @@ def test_angles_frequencies_fixed_focal_distance(cfg):
     g = np.load(os.path.join(GOLDEN, "actions_%s.npz" % cfg))
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
     J, A, F = agama_b200.actions(pot, g["points"], fd=g["fd"], angles=True, frequencies=True)
-    # the actions from the shared nodes are those of the actions-only path, bit for bit
-    assert np.array_equal(J, agama_b200.actions(pot, g["points"], fd=g["fd"]), equal_nan=True)
+    # the actions from the shared nodes are those of the actions-only path to round-off (the two
+    # kernels inline the same potential evaluation, each with its own instruction schedule)
+    J0 = agama_b200.actions(pot, g["points"], fd=g["fd"])
+    assert np.array_equal(np.isfinite(J), np.isfinite(J0))
+    fin = np.isfinite(J0)
+    atol = 1e-14 * np.max(np.abs(J0[fin]))
+    assert np.allclose(J[fin], J0[fin], rtol=1e-12, atol=atol), np.max(np.abs(J[fin] - J0[fin]))
     keep = well_conditioned(g["act_fd"])
     assert np.sum(~keep) <= 2
     print(cfg, "frequencies max rel %.2e" % check_frequencies(F[keep], g["freq_fd"][keep]),
