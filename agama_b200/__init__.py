@@ -155,6 +155,57 @@ class Potential:
         f, h = self.eval(points, pot=False, acc=True, der=True)
         return f, -h
 
+    def density(self, points):
+        """density (Laplacian of the potential / 4 pi) at points, as agama's Potential.density"""
+        if _is_device_array(points):
+            import torch
+            p = points.contiguous().view(-1, 3)
+            rho = torch.empty(p.shape[0], dtype=torch.float64, device=p.device)
+            check(_native.lib().agama_evalDensityManyDevice(self._h, p.shape[0], _dev_ptr(p), _dev_ptr(rho),
+                                                            _current_stream()))
+            return rho
+        p, single = _points(points, 3)
+        rho = _host_empty(len(p))
+        check(_native.lib().agama_evalDensityMany(self._h, len(p), ptr(p), 0.0, ptr(rho)))
+        return rho[0] if single else rho
+
+    # ---------------- radii in the equatorial plane (azimuthally averaged potential) ----------------
+    def _radii(self, query, a, b=None):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        single = a.ndim == 0
+        a = a.reshape(-1)
+        n = len(a)
+        out1 = _host_empty(n)
+        out2 = _host_empty(n) if b is not None else None
+        if b is not None:
+            b = np.ascontiguousarray(np.broadcast_to(np.asarray(b, dtype=np.float64).reshape(-1), (n,)))
+        check(_native.lib().agama_potentialRadiiMany(self._h, query, n, ptr(a), ptr(b), ptr(out1), ptr(out2)))
+        if b is None:
+            return out1[0] if single else out1
+        res = np.column_stack([out1, out2])
+        return res[0] if single else res
+
+    def Rcirc(self, L=None, E=None):
+        """radius of the circular orbit with angular momentum L or energy E (exactly one of them),
+        as agama's Potential.Rcirc (potential::R_from_Lz / R_circ)"""
+        if (L is None) == (E is None):
+            raise TypeError("Rcirc() takes exactly one argument (either L or E)")
+        return self._radii(1, L) if L is not None else self._radii(0, E)
+
+    def Rmax(self, E):
+        """root of Phi(R, z = 0) = E (potential::R_max)"""
+        return self._radii(2, E)
+
+    def Rperiapo(self, EL):
+        """peri- and apocentre radii of planar orbits from (E, L) pairs, as agama's Potential.Rperiapo
+        (potential::findPlanarOrbitExtent); returns (Rperi, Rapo) or an N x 2 array"""
+        EL = np.asarray(EL, dtype=np.float64)
+        if EL.shape[-1] != 2:
+            raise ValueError("Rperiapo: input must be a pair (E, L) or an N x 2 array of them")
+        if EL.ndim == 1:
+            return self._radii(3, EL[0], EL[1])
+        return self._radii(3, EL[:, 0], EL[:, 1])
+
 
 from .actions import ActionFinder, actions  # noqa: E402,F401
 from .orbit import (orbit, set_orbit_lanes, set_orbit_precision, jacobi_energy_error,  # noqa: E402,F401

@@ -26,6 +26,17 @@ SIGNATURES = {
     "agama_inspectMultipoleFile": (ctypes.c_int, [ctypes.c_char_p, I, I, I, I, I]),
     "agama_evalPotentialMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
     "agama_evalPotentialManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
+    "agama_createDensity": (VP, [ctypes.c_char_p]),
+    "agama_deleteDensity": (None, [VP]),
+    "agama_evalDensity": (ctypes.c_double, [VP, D, ctypes.c_double]),
+    "agama_evalDensityMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D]),
+    "agama_evalDensityManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP]),
+    "agama_R_circ": (ctypes.c_double, [VP, ctypes.c_double]),
+    "agama_R_from_Lz": (ctypes.c_double, [VP, ctypes.c_double]),
+    "agama_R_max": (ctypes.c_double, [VP, ctypes.c_double]),
+    "agama_findPlanarOrbitExtent": (None, [VP, ctypes.c_double, ctypes.c_double, D, D]),
+    "agama_potentialRadiiMany": (ctypes.c_int, [VP, ctypes.c_int, ctypes.c_long, D, D, D, D]),
+    "agama_potentialRadiiManyDevice": (ctypes.c_int, [VP, ctypes.c_int, ctypes.c_long, VP, VP, VP, VP, VP]),
     "agama_setOrbitLanesPerOrbit": (ctypes.c_int, [ctypes.c_int]),
     "agama_setOrbitPrecision": (ctypes.c_int, [ctypes.c_int]),
     "agama_integrateOrbitsTrajectoryManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,

@@ -149,6 +149,114 @@ double agama_evalPotential(const agama_Potential* p, const double pos[3], double
     return phi;
 }
 
+// ---- density of a potential
+
+agama_Density* agama_createDensity(const char* params)
+{
+    (void)params;
+    setError("createDensity: density models are not part of the B200 engine; a potential created by "
+             "agama_createPotential can be passed to agama_evalDensity instead");
+    return nullptr;
+}
+
+void agama_deleteDensity(agama_Density* density) { (void)density; }
+
+int agama_evalDensityManyDevice(const agama_Potential* p, long n, const double* pos, double* rho, void* stream)
+{
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && (!pos || !rho))) throw std::invalid_argument("evalDensityManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        launchDensity(p->pot->view, n, pos, rho, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int agama_evalDensityMany(const agama_Potential* p, long n, const double* pos, double time, double* rho)
+{
+    (void)time;
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && (!pos || !rho))) throw std::invalid_argument("evalDensityMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const MultipoleView& M = p->pot->view;
+        runChunked(n, { { pos, 3 * sizeof(double) } }, { { rho, sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchDensity(M, count, static_cast<const double*>(in[0]), static_cast<double*>(out[0]), s);
+            });
+    });
+}
+
+double agama_evalDensity(const agama_Density* density, const double pos[3], double time)
+{
+    // the only objects with a density here are potentials (agama_createDensity makes none)
+    double rho = NAN;
+    if(agama_evalDensityMany(reinterpret_cast<const agama_Potential*>(density), 1, pos, time, &rho) != 0)
+        return NAN;
+    return rho;
+}
+
+// ---- radii of circular, radial and planar orbits
+
+int agama_potentialRadiiManyDevice(const agama_Potential* p, int query, long n, const double* in1,
+    const double* in2, double* out1, double* out2, void* stream)
+{
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && (!in1 || !out1 || (query == RADIUS_PERIAPO && (!in2 || !out2)))))
+            throw std::invalid_argument("potentialRadiiManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        launchRadii(p->pot->view, query, n, in1, in2, out1, out2, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int agama_potentialRadiiMany(const agama_Potential* p, int query, long n, const double* in1, const double* in2,
+    double* out1, double* out2)
+{
+    return guarded([&] {
+        const bool two = query == RADIUS_PERIAPO;
+        if(!p || n < 0 || (n > 0 && (!in1 || !out1 || (two && (!in2 || !out2)))))
+            throw std::invalid_argument("potentialRadiiMany: invalid arguments");
+        if(query < RADIUS_CIRC_E || query > RADIUS_PERIAPO)
+            throw std::invalid_argument("potentialRadiiMany: unknown query " + std::to_string(query));
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const MultipoleView& M = p->pot->view;
+        runChunked(n, { { in1, sizeof(double) }, { two ? in2 : nullptr, sizeof(double) } },
+            { { out1, sizeof(double) }, { two ? out2 : nullptr, sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchRadii(M, query, count, static_cast<const double*>(in[0]), static_cast<const double*>(in[1]),
+                    static_cast<double*>(out[0]), static_cast<double*>(out[1]), s);
+            });
+    });
+}
+
+double agama_R_circ(const agama_Potential* p, double E)
+{
+    double R = NAN;
+    if(agama_potentialRadiiMany(p, RADIUS_CIRC_E, 1, &E, nullptr, &R, nullptr) != 0) return NAN;
+    return R;
+}
+
+double agama_R_from_Lz(const agama_Potential* p, double Lz)
+{
+    double R = NAN;
+    if(agama_potentialRadiiMany(p, RADIUS_CIRC_L, 1, &Lz, nullptr, &R, nullptr) != 0) return NAN;
+    return R;
+}
+
+double agama_R_max(const agama_Potential* p, double E)
+{
+    double R = NAN;
+    if(agama_potentialRadiiMany(p, RADIUS_MAX, 1, &E, nullptr, &R, nullptr) != 0) return NAN;
+    return R;
+}
+
+void agama_findPlanarOrbitExtent(const agama_Potential* p, double E, double L, double* Rperi, double* Rapo)
+{
+    double R1 = NAN, R2 = NAN;
+    if(agama_potentialRadiiMany(p, RADIUS_PERIAPO, 1, &E, &L, &R1, &R2) != 0) R1 = R2 = NAN;
+    if(Rperi) *Rperi = R1;
+    if(Rapo) *Rapo = R2;
+}
+
 }  // extern "C"
 
 extern "C" int agama_inspectMultipoleFile(const char* file, int* lmax, int* mmax, int* symmetry,

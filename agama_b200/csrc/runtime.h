@@ -80,6 +80,13 @@ FinderTablesHost buildFinderTables(const DevicePotential& P);
 /// launch helpers (defined in the .cu files)
 void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
     double* grad, double* hess, cudaStream_t stream);
+/// density (Laplacian / 4 pi inside the grid, closed form outside) at n Cartesian points
+void launchDensity(const MultipoleView& M, long n, const double* pos, double* rho, cudaStream_t stream);
+/// radius queries in the equatorial plane of the azimuthally averaged potential: a = E (or L for
+/// RADIUS_CIRC_L), b = L (RADIUS_PERIAPO only); out1 = radius (pericentre), out2 = apocentre
+enum RadiusQuery { RADIUS_CIRC_E = 0, RADIUS_CIRC_L = 1, RADIUS_MAX = 2, RADIUS_PERIAPO = 3 };
+void launchRadii(const MultipoleView& M, int query, long n, const double* a, const double* b, double* out1,
+    double* out2, cudaStream_t stream);
 /// DOP853 batch; queue != nullptr selects the persistent work-queue mapping (8-byte counter)
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes = 0);

@@ -53,14 +53,22 @@ __device__ double findRootInf(const F& f, double tol)
     return unscaleInf(findRoot(sf, 0, 1, tol), nullptr);
 }
 
+/// the potential of an axisymmetric Multipole and its R-derivatives in the equatorial plane, as
+/// the evaluator object of the radius routines below (any type with this call operator works)
+struct AxiRadial {
+    const MultipoleView* M;
+    __device__ void operator()(double R, double* val, double* der, double* der2) const { axiEvalR(*M, R, val, der, der2); }
+};
+
 /// Phi(R) + R/2 dPhi/dR = E in ln R (RcircRootFinder, potential_utils.cpp:262-288)
+template<class EV>
 struct RcircFn {
     static constexpr bool hasDeriv = true;
-    const MultipoleView* M; double E;
+    EV ev; double E;
     __device__ void operator()(double logR, double* val, double* der) const {
         const double R = exp(logR);
         double Phi, dR, d2R;
-        axiEvalR(*M, R, &Phi, &dR, der ? &d2R : nullptr);
+        ev(R, &Phi, &dR, der ? &d2R : nullptr);
         if(val) {
             const double v = 0.5 * R * dR;
             *val = Phi - E + (isFinite(v) ? v : 0);
@@ -75,13 +83,14 @@ struct RcircFn {
 };
 
 /// Phi(R) = E in ln R (RmaxRootFinder, potential_utils.cpp:232-256)
+template<class EV>
 struct RmaxFn {
     static constexpr bool hasDeriv = true;
-    const MultipoleView* M; double E;
+    EV ev; double E;
     __device__ void operator()(double logR, double* val, double* der) const {
         const double R = exp(logR);
         double Phi, dR;
-        axiEvalR(*M, R, &Phi, der ? &dR : nullptr, nullptr);
+        ev(R, &Phi, der ? &dR : nullptr, nullptr);
         if(val) {
             *val = Phi - E;
             if(!isFinite(*val)) {
@@ -94,9 +103,38 @@ struct RmaxFn {
     }
 };
 
-__device__ double shellRcirc(const MultipoleView& M, double E) { RcircFn f{ &M, E }; return exp(findRootInf(f, SHELL_ACCURACY_ROOT)); }
-__device__ double shellRmax(const MultipoleView& M, double E) { RmaxFn f{ &M, E }; return exp(findRootInf(f, SHELL_ACCURACY_ROOT)); }
-__device__ double shellVcirc(const MultipoleView& M, double R)
+/// L^2 - R^3 dPhi/dR in ln R (RfromLRootFinder, potential_utils.cpp:290-313)
+template<class EV>
+struct RfromLFn {
+    static constexpr bool hasDeriv = true;
+    EV ev; double L2;
+    __device__ void operator()(double logR, double* val, double* der) const {
+        const double R = exp(logR);
+        double dR, d2R;
+        ev(R, nullptr, &dR, der ? &d2R : nullptr);
+        const double F = R * R * R * dR;
+        if(val) *val = isFinite(F) ? F - L2 : (R < 1 ? -L2 : L2);
+        if(der) *der = R * R * R * (3 * dR + R * d2R);
+    }
+};
+
+/// R_circ(E), R_max(E), R_from_Lz(L) (potential_utils.cpp:617-633)
+template<class EV>
+__device__ double radiusCirc(const EV& ev, double E) { RcircFn<EV> f{ ev, E }; return exp(findRootInf(f, SHELL_ACCURACY_ROOT)); }
+template<class EV>
+__device__ double radiusMax(const EV& ev, double E) { RmaxFn<EV> f{ ev, E }; return exp(findRootInf(f, SHELL_ACCURACY_ROOT)); }
+template<class EV>
+__device__ double radiusFromLz(const EV& ev, double L)
+{
+    if(L == 0) return 0;
+    if(fabs(L) == INFINITY) return INFINITY;
+    RfromLFn<EV> f{ ev, L * L };
+    return exp(findRootInf(f, SHELL_ACCURACY_ROOT));
+}
+
+static __device__ double shellRcirc(const MultipoleView& M, double E) { return radiusCirc(AxiRadial{ &M }, E); }
+static __device__ double shellRmax(const MultipoleView& M, double E) { return radiusMax(AxiRadial{ &M }, E); }
+static __device__ double shellVcirc(const MultipoleView& M, double R)
 {
     double Phi, dR;
     if(R == 0) { axiEvalR(M, 0, &Phi, nullptr, nullptr); return isFinite(Phi) ? 0 : INFINITY; }
@@ -105,12 +143,13 @@ __device__ double shellVcirc(const MultipoleView& M, double R)
 }
 
 /// (E - Phi) R^2 - L^2/2 (RPeriApoRootFinder, potential_utils.cpp:315-330)
+template<class EV>
 struct PeriApoFn {
     static constexpr bool hasDeriv = true;
-    const MultipoleView* M; double E, halfL2;
+    EV ev; double E, halfL2;
     __device__ void operator()(double R, double* val, double* der) const {
         double Phi = 0, dR = 0;
-        axiEvalR(*M, R, &Phi, der ? &dR : nullptr, nullptr);
+        ev(R, &Phi, der ? &dR : nullptr, nullptr);
         if(val) *val = (R > 0 ? (E - Phi) * R * R : 0) - halfL2;
         if(der) *der = 2 * R * (E - Phi) - R * R * dR;
     }
@@ -127,10 +166,11 @@ struct PeriApoPowerLawFn {
 };
 
 /// Halley refinement of a peri/apocentre radius (refineRoot, potential_utils.cpp:355-365)
-__device__ double shellRefineRoot(const MultipoleView& M, double R, double E, double L)
+template<class EV>
+__device__ double refinePeriApo(const EV& ev, double R, double E, double L)
 {
     double val, der, der2;
-    axiEvalR(M, R, &val, &der, &der2);
+    ev(R, &val, &der, &der2);
     const double F = E - val - 0.5 * pow2(L / R);
     const double Fp = pow2(L / R) / R - der;
     const double Fpp = -3 * pow2(L / (R * R)) - der2;
@@ -139,12 +179,13 @@ __device__ double shellRefineRoot(const MultipoleView& M, double R, double E, do
 }
 
 /// pericentre and apocentre radii of a planar orbit (findPlanarOrbitExtent, potential_utils.cpp:663-729)
-__device__ void shellPlanarExtent(const MultipoleView& M, double E, double L, double& R1, double& R2)
+template<class EV>
+__device__ void planarOrbitExtent(const EV& ev, double E, double L, double& R1, double& R2)
 {
     // innerSlope (potential_utils.cpp:647-661) at r = 1e-10
     const double r = 1e-10;
     double Phi, dPhidR, d2PhidR2;
-    axiEvalR(M, r, &Phi, &dPhidR, &d2PhidR2);
+    ev(r, &Phi, &dPhidR, &d2PhidR2);
     const double slope = 1 + r * d2PhidR2 / dPhidR;
     const double coef = slope == 0 ? dPhidR * r : dPhidR / slope * pow(r, 1 - slope);
     const double Phi0 = slope == 0 ? Phi - r * dPhidR * log(r) : Phi - r * dPhidR / slope;
@@ -161,11 +202,11 @@ __device__ void shellPlanarExtent(const MultipoleView& M, double E, double L, do
             R1 = R2 = Rc;
         return;
     }
-    const double Rc = shellRcirc(M, E);
+    const double Rc = radiusCirc(ev, E);
     if(!isFinite(Rc)) { R1 = R2 = NAN; return; }
     if(Rc == 0) { R1 = R2 = 0; return; }
     double P, dR, d2R;
-    axiEvalR(M, Rc, &P, &dR, &d2R);
+    ev(Rc, &P, &dR, &d2R);
     const double Lc = Rc * sqrt(Rc * dR);
     if(L >= Lc || (!isFinite(Lc) && Rc <= 1. / SHELL_HUGE_NUMBER)) {
         R1 = R2 = Rc;
@@ -173,15 +214,20 @@ __device__ void shellPlanarExtent(const MultipoleView& M, double E, double L, do
         const double off = sqrt((1 - pow2(L / Lc)) * dR / (3 * dR + Rc * d2R));
         R1 = Rc * (1 - off);
         R2 = Rc * (1 + off);
-        R1 = fmin(Rc, shellRefineRoot(M, R1, E, L));
-        R2 = fmax(Rc, shellRefineRoot(M, R2, E, L));
+        R1 = fmin(Rc, refinePeriApo(ev, R1, E, L));
+        R2 = fmax(Rc, refinePeriApo(ev, R2, E, L));
     } else {
-        PeriApoFn f{ &M, E, 0.5 * L * L };
+        PeriApoFn<EV> f{ ev, E, 0.5 * L * L };
         R1 = findRoot(f, 0, Rc, SHELL_ACCURACY_ROOT);
         R2 = findRoot(f, Rc, 3 * Rc, SHELL_ACCURACY_ROOT);
         if(!isFinite(R2))
-            R2 = findRoot(f, Rc, (1 + SHELL_ACCURACY_ROOT) * shellRmax(M, E), SHELL_ACCURACY_ROOT);
+            R2 = findRoot(f, Rc, (1 + SHELL_ACCURACY_ROOT) * radiusMax(ev, E), SHELL_ACCURACY_ROOT);
     }
+}
+
+static __device__ void shellPlanarExtent(const MultipoleView& M, double E, double L, double& R1, double& R2)
+{
+    planarOrbitExtent(AxiRadial{ &M }, E, L, R1, R2);
 }
 
 /// meridional-plane orbit with its deviation vector: (R, z, vR, vz, dR, dz, dvR, dvz)
@@ -363,7 +409,7 @@ struct CrossingFn {
 
 /** launch an orbit from (R0, z=0) with vz > 0 and find where it crosses z = 0 downward, with the
     derivative dRcross/dR0 from the variational equations (findCrossingPointR, :150-219) */
-__device__ void shellCrossing(const MultipoleView& M, double E, double Lz, double R0,
+static __device__ void shellCrossing(const MultipoleView& M, double E, double Lz, double R0,
     double& Rcross, double& dRcrossdR0)
 {
     double Phi;
@@ -410,7 +456,7 @@ struct ClosedOrbitFn {
 
 /// focal distance of the shell orbit with energy E and angular momentum Lz; also its radius
 /// (estimateFocalDistanceShellOrbit, :257-297, non-OLD_METHOD branch)
-__device__ double shellFocalDistance(const MultipoleView& M, double E, double Lz, double* Rshell)
+static __device__ double shellFocalDistance(const MultipoleView& M, double E, double Lz, double* Rshell)
 {
     double Rmin, Rmax;
     shellPlanarExtent(M, E, Lz, Rmin, Rmax);

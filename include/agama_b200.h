@@ -20,6 +20,7 @@
 extern "C" {
 #endif
 
+typedef struct agama_Density agama_Density;
 typedef struct agama_Potential agama_Potential;
 typedef struct agama_ActionFinder agama_ActionFinder;
 
@@ -41,6 +42,41 @@ void agama_deletePotential(agama_Potential* potential);
    potential at pos, gradient into deriv[3] and Hessian into deriv2[6] when not NULL. */
 double agama_evalPotential(const agama_Potential* potential, const double pos[3], double time,
     double deriv[3], double deriv2[6]);
+
+/* reference: agama_createDensity, src/interface_c.h:35 (src/interface_c.cpp:20-29).  Density
+   models (Plummer, Spheroid, ...) only serve to construct potentials, which this engine reads
+   from coefficient files: always NULL, with the reason in agama_getError(). */
+agama_Density* agama_createDensity(const char* params);
+
+/* reference: agama_deleteDensity, src/interface_c.h:49 (nothing to free here) */
+void agama_deleteDensity(agama_Density* density);
+
+/* reference: agama_evalDensity, src/interface_c.h:61 (src/interface_c.cpp:63-66 ->
+   Multipole::densityCyl, src/potential_multipole.cpp:1550-1559).  As in the reference, the
+   object may be a potential (cast to agama_Density*): its density is the Laplacian of the
+   potential / 4 pi inside the radial grid and the closed form of the power-law expansions
+   outside.  NaN on failure. */
+double agama_evalDensity(const agama_Density* density, const double pos[3], double time);
+
+/* reference: agama_R_circ, src/interface_c.h:81 (src/interface_c.cpp:92-95 -> potential::R_circ,
+   src/potential_utils.cpp:617-619): radius of the circular orbit of energy E in the equatorial
+   plane; the potential is averaged over the azimuth if it is not axisymmetric
+   (Axisymmetrized, src/potential_base.cpp:256-283, 529-590).  NaN on failure. */
+double agama_R_circ(const agama_Potential* potential, double E);
+
+/* reference: agama_R_from_Lz, src/interface_c.h:86 (potential::R_from_Lz,
+   src/potential_utils.cpp:621-627): radius of the circular orbit of angular momentum Lz. */
+double agama_R_from_Lz(const agama_Potential* potential, double Lz);
+
+/* reference: agama_R_max, src/interface_c.h:91 (potential::R_max, src/potential_utils.cpp:629-631):
+   the root of Phi(R, z = 0) = E. */
+double agama_R_max(const agama_Potential* potential, double E);
+
+/* reference: agama_findPlanarOrbitExtent, src/interface_c.h:104 (potential::findPlanarOrbitExtent,
+   src/potential_utils.cpp:663-729): peri- and apocentre radii of the planar orbit (E, L); both
+   NaN when E is outside the allowed range, both R_circ(E) when L >= L_circ(E). */
+void agama_findPlanarOrbitExtent(const agama_Potential* potential, double E, double L,
+    double* Rperi, double* Rapo);
 
 /* ---------------------------------------------------------------------------------------
    Construction from arrays (reference: potential::Multipole(gridRadii, Phi, dPhi),
@@ -70,6 +106,28 @@ int agama_evalPotentialMany(const agama_Potential* potential, long n, const doub
 /* The same on device buffers, enqueued on the given stream. */
 int agama_evalPotentialManyDevice(const agama_Potential* potential, long n, const double* pos,
     double* phi, double* deriv, double* deriv2, void* stream);
+
+/* Batched density of a potential at n points (n x 3), host buffers: n calls of agama_evalDensity
+   (the reference's Python Density.density batches the same, src/interface_python.cpp:2439). */
+int agama_evalDensityMany(const agama_Potential* potential, long n, const double* pos, double time,
+    double* rho);
+
+/* The same on device buffers, enqueued on the given stream. */
+int agama_evalDensityManyDevice(const agama_Potential* potential, long n, const double* pos, double* rho,
+    void* stream);
+
+/* Batched radius queries, one per item, host buffers: query 0 = R_circ(in1 = E), 1 = R_from_Lz
+   (in1 = Lz), 2 = R_max(in1 = E): radius into out1 (in2, out2 unused, may be NULL);
+   3 = findPlanarOrbitExtent(in1 = E, in2 = L): pericentre into out1, apocentre into out2.
+   Replaces n calls of agama_R_circ / agama_R_from_Lz / agama_R_max / agama_findPlanarOrbitExtent
+   (the reference batches them in Python as Potential.Rcirc / Rmax / Rperiapo,
+   src/interface_python.cpp:3354-3512). */
+int agama_potentialRadiiMany(const agama_Potential* potential, int query, long n, const double* in1,
+    const double* in2, double* out1, double* out2);
+
+/* The same on device buffers, enqueued on the given stream. */
+int agama_potentialRadiiManyDevice(const agama_Potential* potential, int query, long n, const double* in1,
+    const double* in2, double* out1, double* out2, void* stream);
 
 /* ---------------------------------------------------------------------------------------
    Orbit integration (DOP853).  Each of the n orbits starts at ic[i] (x,y,z,vx,vy,vz, in the

@@ -9,6 +9,8 @@ Every function below forwards to the reference's own code path for the hot path:
   orbits_many          orbit::OrbitIntegrator<Car>::run       orbit.cpp:52-84 (DOP853, math_ode.cpp:107-406)
   actions_fd_many      actions::evalAxisymFudge               actions_staeckel.cpp:683-693
   ActionFinder.actions actions::ActionFinderAxisymFudge::eval actions_staeckel.cpp:954-979
+  CInterfacePotential  the reference's plain-C interface       interface_c.cpp:31-111
+                       (density, R_circ, R_from_Lz, R_max, findPlanarOrbitExtent)
 """
 import ctypes
 import os
@@ -202,3 +204,51 @@ class ActionFinder:
         L = np.empty_like(E)
         lib().ref_actionfinder_lcirc(self.h, len(E), _p(E), _p(L))
         return L
+
+
+class CInterfacePotential:
+    """A potential through the reference's own plain-C interface (src/interface_c.cpp, compiled
+    into the oracle library): agama_createPotential, agama_evalDensity, agama_R_circ,
+    agama_R_from_Lz, agama_R_max, agama_findPlanarOrbitExtent, one call per point."""
+
+    def __init__(self, params):
+        L = lib()
+        L.agama_getError.restype = ctypes.c_char_p
+        L.agama_createPotential.restype = ctypes.c_void_p
+        L.agama_createPotential.argtypes = [ctypes.c_char_p]
+        L.agama_deletePotential.argtypes = [ctypes.c_void_p]
+        L.agama_evalDensity.restype = ctypes.c_double
+        L.agama_evalDensity.argtypes = [ctypes.c_void_p, _D, ctypes.c_double]
+        for name in ("agama_R_circ", "agama_R_from_Lz", "agama_R_max"):
+            getattr(L, name).restype = ctypes.c_double
+            getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.agama_findPlanarOrbitExtent.restype = None
+        L.agama_findPlanarOrbitExtent.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D, _D]
+        self.h = L.agama_createPotential(params.encode())
+        if not self.h:
+            raise RuntimeError("oracle: " + L.agama_getError().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.agama_deletePotential(self.h)
+
+    def density(self, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        return np.array([lib().agama_evalDensity(self.h, _p(p), 0.0) for p in pos])
+
+    def R_circ(self, E):
+        return np.array([lib().agama_R_circ(self.h, float(e)) for e in np.ravel(E)])
+
+    def R_from_Lz(self, L):
+        return np.array([lib().agama_R_from_Lz(self.h, float(x)) for x in np.ravel(L)])
+
+    def R_max(self, E):
+        return np.array([lib().agama_R_max(self.h, float(e)) for e in np.ravel(E)])
+
+    def periapo(self, E, L):
+        out = np.empty((len(np.ravel(E)), 2))
+        r1, r2 = ctypes.c_double(), ctypes.c_double()
+        for i, (e, l) in enumerate(zip(np.ravel(E), np.ravel(L))):
+            lib().agama_findPlanarOrbitExtent(self.h, float(e), float(l), ctypes.byref(r1), ctypes.byref(r2))
+            out[i] = r1.value, r2.value
+        return out

@@ -2,7 +2,7 @@
 
 Run here, where the reference sources exist and the oracle has been built (make -C oracle):
 
-    python tests/golden/make_golden.py [potentials|orbits|actions|all]
+    python tests/golden/make_golden.py [potentials|orbits|actions|utils|all]
 
 It writes, into tests/golden/:
   <name>.coef            Multipole coefficient files written by the reference (writePotential)
@@ -13,7 +13,10 @@ It writes, into tests/golden/:
                          phase-space points, accepted step counts and statuses;
   actions_<name>.npz     phase-space points with the reference's Staeckel-fudge actions (fixed
                          focal distance and through ActionFinderAxisymFudge), plus the finder's
-                         focal-distance table and L_circ(E) spline.
+                         focal-distance table and L_circ(E) spline;
+  utils_<name>.npz       density at the potential_<name> points and R_circ(E), R_max(E),
+                         R_from_Lz(L), peri/apocentre radii of (E, L), through the reference's
+                         plain-C interface.
 All inputs are synthetic and seeded (agama_b200/workloads.py); no external dataset is involved.
 """
 import os
@@ -195,6 +198,39 @@ def make_action_vectors():
               "table", tab["delta"].shape, "LofE", tab["lofe"].shape)
 
 
+def make_utility_vectors():
+    """density and the radius routines through the reference's plain-C interface
+    (agama_evalDensity, agama_R_circ, agama_R_from_Lz, agama_R_max, agama_findPlanarOrbitExtent)"""
+    for i, name in enumerate(["cfg1", "cfg2", "quad", "sph", "lop"]):
+        cpot = ref.CInterfacePotential("file=" + coef_path(name))
+        pot = ref.Potential(file=coef_path(name))
+        pts = np.load(os.path.join(HERE, "potential_%s.npz" % name))["points"]
+        rho = cpot.density(pts)
+        rng = np.random.Generator(np.random.PCG64(900 + i))
+        # energies of radii log-uniform over [1e-4, 1e4] (inside, between and beyond the grid ends)
+        r = 10 ** rng.uniform(-4, 4, size=120)
+        E = pot.eval(np.column_stack([r, 0 * r, 0 * r]))[0]
+        phi0 = pot.eval(np.zeros((1, 3)))[0][0]
+        E = np.concatenate([E, [phi0 * 1.000001, 0.5 * phi0, -1e-12, 0.0, 0.1]])
+        # angular momenta log-uniform, with zero and a negative value
+        L = np.concatenate([10 ** rng.uniform(-4, 3, size=120), [0.0, -0.7, 1e-8]])
+        # (E, L) pairs: L a fraction u of the circular value at E (radial, eccentric, nearly
+        # circular, above circular) and energies outside the allowed range
+        rr = 10 ** rng.uniform(-3.5, 3.5, size=100)
+        Ep = pot.eval(np.column_stack([rr, 0 * rr, 0 * rr]))[0]
+        Rc = cpot.R_circ(Ep)
+        g = pot.eval(np.column_stack([Rc, 0 * Rc, 0 * Rc]))[1]
+        Lc = Rc * np.sqrt(np.abs(Rc * g[:, 0]))
+        u = np.concatenate([rng.uniform(0, 1, size=90), [0.0, 0.9999995, 0.999999, 1.0, 1.05, 0.5, 0.3, 0.1,
+                                                        0.99, 1e-6]])
+        EL = np.column_stack([Ep, u * Lc])
+        EL = np.vstack([EL, [[phi0 * 1.01, 0.1], [0.1, 0.5]]])
+        np.savez_compressed(os.path.join(HERE, "utils_%s.npz" % name), points=pts, rho=rho, E=E,
+                            Rcirc=cpot.R_circ(E), Rmax=cpot.R_max(E), L=L, RfromLz=cpot.R_from_Lz(L),
+                            EL=EL, periapo=cpot.periapo(EL[:, 0], EL[:, 1]))
+        print(name, "density points", len(pts), "energies", len(E), "L", len(L), "(E,L)", len(EL))
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     if what in ("potentials", "all"):
@@ -204,3 +240,5 @@ if __name__ == "__main__":
         make_orbit_vectors()
     if what in ("actions", "all"):
         make_action_vectors()
+    if what in ("utils", "all"):
+        make_utility_vectors()

@@ -50,6 +50,14 @@ def test_unsupported_parameters_rejected():
     assert "Multipole" in _native.error() or "not supported" in _native.error()
 
 
+def test_density_objects_not_constructed():
+    """density models only construct potentials, which come from coefficient files here"""
+    L = _native.lib()
+    assert not L.agama_createDensity(b"type=Plummer, mass=1")
+    assert "agama_evalDensity" in _native.error()
+    L.agama_deleteDensity(None)
+
+
 @pytest.mark.skipif(gpu_available(), reason="checks the no-device behaviour")
 def test_no_cpu_fallback():
     h = _native.lib().agama_createPotential(("file=" + os.path.join(GOLDEN, "cfg1.coef")).encode())
