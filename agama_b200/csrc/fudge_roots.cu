@@ -60,7 +60,9 @@ __device__ __forceinline__ bool startPlain(RootSearch& s, int kind, const FudgeE
     tolerance; when that bracket holds no sign change the plain search takes over, and a root found
     on a predicted bracket is accepted only if F is negative half-way from it to the plain end
     where F is negative (one more evaluation).  stats (may be null) accumulates {searches,
-    narrowed, fallbacks, iterations}. */
+    narrowed, fallbacks, iterations}.  LEARNED = false (no predictions, no stats) compiles the plain
+    searches alone, without the predicted-bracket state and counters (fewer registers). */
+template<bool LEARNED>
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
     FudgeRecord* __restrict__ rec, const FudgeEnds* __restrict__ ends, int* __restrict__ iters,
     unsigned long long* __restrict__ counter, const float* __restrict__ pred, const BracketWidths widths,
@@ -105,9 +107,9 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         // bracket half-widths of D2) keep the plain searches for all limits:
                         // there the GL action integrals resolve the integrands poorly and depend
                         // on the limits to the last bits of the plain searches
-                        const bool nearFocal = pred && (pred[3 * i] + 2 * widths.w[0] >= 1 ||
-                                                        pred[3 * i + 1] - 2 * widths.w[1] <= 0);
-                        if(pred && !nearFocal) {
+                        const bool nearFocal = LEARNED && pred && (pred[3 * i] + 2 * widths.w[0] >= 1 ||
+                                                                   pred[3 * i + 1] - 2 * widths.w[1] <= 0);
+                        if(LEARNED && pred && !nearFocal) {
                             const double tp = pred[3 * i + k], w = widths.w[k];
                             double nlo, nhi;
                             const double lmd = r.lambda - r.D2;
@@ -136,11 +138,13 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                                 lo = nlo; hi = nhi; narrow = true;
                             }
                         }
-                        nSearch++;
-                        nNarrow += narrow;
+                        if(LEARNED) {
+                            nSearch++;
+                            nNarrow += narrow;
+                        }
                         busy = true;
                         bool done = false;
-                        if(narrow) x = s.startAbs(lo, hi, tol);
+                        if(LEARNED && narrow) x = s.startAbs(lo, hi, tol);
                         else done = startPlain(s, kind, ends ? ends + i : nullptr, lo, hi, tol, u0, r.D2, r.E, &x);
                         if(done) {      // no sign change or a root at an end
                             busy = false;
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
         if(busy) {
             double fx, dx;
             limitRootEval(fnc, kind, u0, x, &fx, &dx);
-            if(verifying) {
+            if(LEARNED && verifying) {
                 // a root from a predicted bracket: F must have the sign of the plain bracket's
                 // end half-way between the root and that end (lambda_max: towards infinity in the
                 // scaled variable; lambda_min: towards D2; nu_max: towards D2), where it is
@@ -178,15 +182,15 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                     }
                 }
             } else if(s.feed(fx, dx, &x)) {
-                nIter += s.iter;
-                if(narrow && !isFinite(s.result)) {     // the predicted bracket missed: plain search
+                if(LEARNED) nIter += s.iter;
+                if(LEARNED && narrow && !isFinite(s.result)) {     // the predicted bracket missed: plain search
                     narrow = false;
                     nFallback++;
                     if(startPlain(s, kind, ends ? ends + point : nullptr, plainLo, plainHi, tol, u0, fnc.D2, fnc.E, &x)) {
                         busy = false;
                         storePlainLimit(rec[point], kind, s, u0, fnc.nu);
                     }
-                } else if(narrow) {
+                } else if(LEARNED && narrow) {
                     verifying = true;
                     verified = s.result;
                     x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? plainLo : plainHi));
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
             }
         }
     }
-    if(stats) {     // one atomic per warp and counter
+    if(LEARNED && stats) {     // one atomic per warp and counter
         nSearch = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nSearch));
         nNarrow = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nNarrow));
         nFallback = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nFallback));
@@ -229,7 +233,8 @@ __global__ void bracketTargetKernel(long n, const FudgeRecord* __restrict__ rec,
     }
 }
 
-/// resident blocks of the root kernel on the current device (cached per device)
+/// resident blocks of a root-kernel variant on the current device (cached per device and variant)
+template<bool LEARNED>
 int rootGridSize()
 {
     static std::mutex mutex;
@@ -241,7 +246,7 @@ int rootGridSize()
     if(it != cache.end()) return it->second;
     int sms = 0, perSM = 0;
     AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fudgeRootKernel, ROOT_BLOCK, 0));
+    AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fudgeRootKernel<LEARNED>, ROOT_BLOCK, 0));
     const int grid = std::max(1, sms * std::max(1, perSM));
     cache[dev] = grid;
     return grid;
@@ -255,8 +260,15 @@ void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const Fu
 {
     if(n <= 0) return;
     AGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
-    const long grid = std::min<long>(rootGridSize(), (3 * n + ROOT_BLOCK - 1) / ROOT_BLOCK);
-    fudgeRootKernel<<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, pred, widths, stats);
+    const long tasks = (3 * n + ROOT_BLOCK - 1) / ROOT_BLOCK;
+    if(pred || stats) {
+        const long grid = std::min<long>(rootGridSize<true>(), tasks);
+        fudgeRootKernel<true><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, pred, widths, stats);
+    } else {
+        const long grid = std::min<long>(rootGridSize<false>(), tasks);
+        fudgeRootKernel<false><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, nullptr, widths,
+            nullptr);
+    }
     AGB_CUDA(cudaGetLastError());
 }
 

@@ -22,7 +22,7 @@ using ChunkLaunch = std::function<void(long first, long count, void* const* dIn,
 /// Run a batch of n items over host arrays on the current device and return when the outputs
 /// are in host memory.  Pinned (page-locked) host arrays give full copy/compute overlap; pageable
 /// ones are staged by the driver and still overlap the kernels of the neighbouring chunks.
-/// chunk = 0 picks the chunk size (n/8, at least 65536 items, at most 1 << 20).
+/// chunk = 0 picks the chunk size (n/4, at least 65536 items, at most 1 << 20).
 void runChunked(long n, const std::vector<HostIn>& ins, const std::vector<HostOut>& outs,
     const ChunkLaunch& launch, long chunk = 0);
 

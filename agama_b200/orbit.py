@@ -124,6 +124,7 @@ class OrbitGraph:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _native._lib is not None:
-            _native._lib.agama_orbitGraphDelete(h)
+        lib = getattr(_native, "_lib", None)     # module globals may be gone at interpreter exit
+        if h and lib is not None:
+            lib.agama_orbitGraphDelete(h)
             self._h = None
