@@ -51,6 +51,16 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(value, dist, device):
+    """the largest of one value over all ranks (a step's time: the slowest replica sets the job's)"""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------------------------------------
 class ClockSampler:
     """samples nvidia-smi SM clocks and throttle reasons while the timed region runs"""
@@ -243,10 +253,7 @@ def run_engine_secondary(dev, flush, dist, cpu):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         t = float(np.mean(ms))
-        if dist:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(t, dist, dev)
         return t, r
 
     out, mixed_lines = [], []
@@ -349,10 +356,7 @@ def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         t = float(np.mean(ms))
-        if dist:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(t, dist, dev)
         return t
 
     def rel_err(J, Jref):
@@ -508,10 +512,7 @@ def run_engine(args):
     clocks = sampler.stop(physical_gpu_index(local)) if rank == 0 else None
     per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(np.sum(per))
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     value = n * world * args.steps / (total_ms / 1000)
     ms_per_step = total_ms / args.steps
 
@@ -527,11 +528,7 @@ def run_engine(args):
         out = af(hp)
         e2e_times.append(time.perf_counter() - t0)
     e2e_ms = 1000 * float(np.mean(e2e_times))
-    e2e_val = n * world / (e2e_ms / 1000)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = n * world / (float(t.item()) / 1000)
+    e2e_val = n * world / (max_over_ranks(e2e_ms, dist, dev) / 1000)
     if rank == 0:
         # ---- roofline (FP64-pipe bound): the dominant kernel (root searches), timed by CUDA events
         # around it during the timed steps, and the whole three-kernel step; executed FP64 flops
