@@ -574,13 +574,13 @@ def run_engine(args):
 # kernels per action step: prepare, root searches, integrals
 ACTION_LAUNCHES_PER_STEP = 3
 # executed FP64 flops per action (dadd + dmul + 2 dfma, ncu, config-2 workload, 200 000 particles):
-# prepare 3874, root searches 11014, integrals 9667
+# prepare 3880, root searches 11014, integrals 9687
 FLOPS_ROOT_PER_ACTION_CFG2 = 11014.0
-FLOPS_PER_ACTION_CFG2 = 3874.0 + 11014.0 + 9667.0
-# dram read + write of one 200 000-particle step (prepare 11.11 + 4.57 MB, roots 39.04 + 82.31 MB,
-# integrals 26.00 + 0.00 MB), scaled to 1e6 particles (the traffic grows with the particles)
-TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 121.35e6
-TRAFFIC_PER_STEP_CFG2 = 5 * 163.03e6
+FLOPS_PER_ACTION_CFG2 = 3880.0 + 11014.0 + 9687.0
+# dram read + write of one 200 000-particle step (prepare 11.21 + 4.43 MB, roots 36.06 + 25.31 MB,
+# integrals 26.01 + 0.00 MB), scaled to 1e6 particles (the traffic grows with the particles)
+TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 61.37e6
+TRAFFIC_PER_STEP_CFG2 = 5 * 103.02e6
 
 
 def ctypes_stream(stream):
