@@ -107,7 +107,9 @@ class ActionFinder:
         check(_native.lib().agama_actionFinderUseBrackets(self._h, 1 if on else 0))
 
     def bracket_stats(self, reset=False):
-        """{searches, narrowed, fallbacks, iterations} of the root searches since the last reset"""
+        """{searches, narrowed, fallbacks, iterations} of the root searches since the last reset:
+        narrowed = searches started from a predicted root, fallbacks = plain searches after a
+        failed check of such a root"""
         st = (ctypes.c_longlong * 4)()
         check(_native.lib().agama_actionFinderBracketStats(self._h, st, 1 if reset else 0))
         return dict(searches=st[0], narrowed=st[1], fallbacks=st[2], iterations=st[3])

@@ -376,6 +376,18 @@ struct RootSearch {
         return propose(xnext);
     }
 
+    /// replace the first iterate, just proposed after both end values were known (phase 2, the
+    /// bracket between a and c), by the guess t when t lies strictly inside the bracket: true and
+    /// *xnext = t; the step to t counts as the last step (d, e) for the next interpolation test
+    AGB_HD bool seed(double t, double* xnext)
+    {
+        if(phase != 2 || iter != 0 || !((t - a) * (c - t) > 0)) return false;
+        d = t - a; e = d;
+        b = t;
+        *xnext = t;
+        return true;
+    }
+
     /// both end values known: the bracket checks and the first iterate
     AGB_HD bool begin(double* xnext)
     {

@@ -55,13 +55,14 @@ __device__ __forceinline__ bool startPlain(RootSearch& s, int kind, const FudgeE
 
     With bracket predictions (pred != null: per point, in the order of the kinds, the fractions
     (nu_max - |nu|)/(D2 - |nu|), (lambda_min - D2)/(lambda - D2), (lambda - D2)/(lambda_max - D2),
-    all in [0, 1]) a search first runs
-    on the predicted bracket (t -+ width, inside the plain bracket) with the plain bracket's
-    tolerance; when that bracket holds no sign change the plain search takes over, and a root found
-    on a predicted bracket is accepted only if F is negative half-way from it to the plain end
-    where F is negative (one more evaluation).  stats (may be null) accumulates {searches,
-    narrowed, fallbacks, iterations}.  LEARNED = false (no predictions, no stats) compiles the plain
-    searches alone, without the predicted-bracket state and counters (fewer registers). */
+    all in [0, 1]) a search runs on its plain bracket, whose end values phase 1 has evaluated, but
+    its first iterate is the predicted root instead of the interpolated one (RootSearch::seed); the
+    search then goes on as the plain one does and ends inside the plain bracket with the plain
+    tolerance.  Its root is accepted only if F is negative half-way from it to the plain end where F
+    is negative (one more evaluation); otherwise F has more roots there and the plain search, which
+    may end on any of them, decides.  stats (may be null) accumulates {searches, seeded searches,
+    plain searches after a failed check, iterations}.  LEARNED = false (no predictions, no stats)
+    compiles the plain searches alone, without that state and the counters (fewer registers). */
 template<bool LEARNED>
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
     FudgeRecord* __restrict__ rec, const FudgeEnds* __restrict__ ends, int* __restrict__ iters,
@@ -70,11 +71,11 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
 {
     const long total = 3 * n;
     const unsigned lane = threadIdx.x & 31;
-    bool busy = false, drained = false, narrow = false, verifying = false;
+    bool busy = false, drained = false, seeded = false, verifying = false;
     long point = 0;
     int kind = 0;
-    double x = 0, u0 = 0, plainLo = 0, plainHi = 0, tol = 0, verified = 0;
-    unsigned long long nSearch = 0, nNarrow = 0, nFallback = 0, nIter = 0;
+    double x = 0, u0 = 0, verified = 0;
+    unsigned nSearch = 0, nSeeded = 0, nFallback = 0, nIter = 0;
     FudgeFunction fnc;
     RootSearch s;
     while(true) {
@@ -98,57 +99,36 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         kind = 1 << k;
                         loadFudgeFunction(M, r, fnc);
                         u0 = r.lambdaPos;
-                        plainLo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
-                        plainHi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
-                        tol = fabs(plainLo - plainHi) * FUDGE_ACCURACY_RANGE;
-                        double lo = plainLo, hi = plainHi;
-                        narrow = false;
-                        // points predicted near the focal line (nu_max or lambda_min within two
-                        // bracket half-widths of D2) keep the plain searches for all limits:
-                        // there the GL action integrals resolve the integrands poorly and depend
-                        // on the limits to the last bits of the plain searches
-                        const bool nearFocal = LEARNED && pred && (pred[3 * i] + 2 * widths.w[0] >= 1 ||
-                                                                   pred[3 * i + 1] - 2 * widths.w[1] <= 0);
-                        if(LEARNED && pred && !nearFocal) {
-                            const double tp = pred[3 * i + k], w = widths.w[k];
-                            double nlo, nhi;
-                            const double lmd = r.lambda - r.D2;
-                            if(kind == ROOT_NU_MAX) {
-                                const double span = r.D2 - fabs(r.nu);
-                                nlo = fabs(r.nu) + (tp - w) * span;
-                                nhi = fabs(r.nu) + (tp + w) * span;
-                            } else if(kind == ROOT_LAMBDA_MIN) {
-                                nlo = r.D2 + (tp - w) * lmd;
-                                nhi = r.D2 + (tp + w) * lmd;
-                            } else {                    // in the semi-infinite scaling about lambda_pos
-                                const double L0 = log(fmax(r.D2 + lmd / (tp + w), u0) / u0);
-                                nlo = L0 / (1 + L0);
-                                if(tp - w > 0) {
-                                    const double L1 = log(fmax(r.D2 + lmd / (tp - w), u0) / u0);
-                                    nhi = L1 / (1 + L1);
-                                } else
-                                    nhi = plainHi;
-                            }
-                            // only a bracket strictly inside the plain one: a prediction that reaches a
-                            // plain end (limits near the focal line lambda = nu = D2, or lambda_max
-                            // far out) leaves the search to the plain bracket, where the limit
-                            // is only fixed to the tolerance of the plain search and the actions
-                            // follow that search's own path
-                            if(isFinite(nlo) && isFinite(nhi) && nlo > plainLo && nhi < plainHi && nlo < nhi) {
-                                lo = nlo; hi = nhi; narrow = true;
+                        const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
+                        const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
+                        const double tol = fabs(lo - hi) * FUDGE_ACCURACY_RANGE;
+                        busy = true;
+                        seeded = false;
+                        const bool done = startPlain(s, kind, ends ? ends + i : nullptr, lo, hi, tol, u0, r.D2, r.E, &x);
+                        if(done) {      // no sign change or a root at an end
+                            busy = false;
+                            storePlainLimit(rec[i], kind, s, u0, fnc.nu);
+                        } else if(LEARNED && pred && s.phase == 2) {
+                            // points predicted near the focal line (nu_max or lambda_min within two
+                            // bracket half-widths of D2) keep the plain searches for all limits:
+                            // there the GL action integrals resolve the integrands poorly and depend
+                            // on the limits to the last bits of the plain searches
+                            const bool nearFocal = pred[3 * i] + 2 * widths.w[0] >= 1 || pred[3 * i + 1] - 2 * widths.w[1] <= 0;
+                            if(!nearFocal) {
+                                const double tp = pred[3 * i + k], lmd = r.lambda - r.D2;
+                                double guess;
+                                if(kind == ROOT_NU_MAX) guess = fabs(r.nu) + tp * (r.D2 - fabs(r.nu));
+                                else if(kind == ROOT_LAMBDA_MIN) guess = r.D2 + tp * lmd;
+                                else {          // in the semi-infinite scaling about lambda_pos
+                                    const double L0 = log(fmax(r.D2 + lmd / tp, u0) / u0);
+                                    guess = L0 / (1 + L0);
+                                }
+                                if(isFinite(guess)) seeded = s.seed(guess, &x);
                             }
                         }
                         if(LEARNED) {
                             nSearch++;
-                            nNarrow += narrow;
-                        }
-                        busy = true;
-                        bool done = false;
-                        if(LEARNED && narrow) x = s.startAbs(lo, hi, tol);
-                        else done = startPlain(s, kind, ends ? ends + i : nullptr, lo, hi, tol, u0, r.D2, r.E, &x);
-                        if(done) {      // no sign change or a root at an end
-                            busy = false;
-                            storePlainLimit(rec[i], kind, s, u0, fnc.nu);
+                            nSeeded += seeded;
                         }
                     }
                 }
@@ -159,41 +139,39 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
             double fx, dx;
             limitRootEval(fnc, kind, u0, x, &fx, &dx);
             if(LEARNED && verifying) {
-                // a root from a predicted bracket: F must have the sign of the plain bracket's
-                // end half-way between the root and that end (lambda_max: towards infinity in the
+                // a root from a seeded search: F must have the sign of the plain bracket's end
+                // half-way between the root and that end (lambda_max: towards infinity in the
                 // scaled variable; lambda_min: towards D2; nu_max: towards D2), where it is
-                // negative; otherwise F has more roots there and the plain search, which may end
-                // on any of them, decides
+                // negative; otherwise F has more roots there and the plain search decides
                 verifying = false;
                 nIter++;
+                const FudgeRecord& r = rec[point];
                 if(fx < 0) {
                     busy = false;
-                    FudgeRecord& r = rec[point];
-                    if(kind == ROOT_NU_MAX) r.nuMax = verified;
-                    else if(kind == ROOT_LAMBDA_MIN) r.lambdaMin = verified;
-                    else r.lambdaMax = unscaleSemiInf(u0, verified, nullptr);
+                    FudgeRecord& w = rec[point];
+                    if(kind == ROOT_NU_MAX) w.nuMax = verified;
+                    else if(kind == ROOT_LAMBDA_MIN) w.lambdaMin = verified;
+                    else w.lambdaMax = unscaleSemiInf(u0, verified, nullptr);
                     if(iters) atomicAdd(iters + point, s.iter + 1);
                 } else {
-                    narrow = false;
+                    seeded = false;
                     nFallback++;
-                    if(startPlain(s, kind, ends ? ends + point : nullptr, plainLo, plainHi, tol, u0, fnc.D2, fnc.E, &x)) {
+                    const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
+                    const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
+                    if(startPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
+                                  u0, fnc.D2, fnc.E, &x)) {
                         busy = false;
                         storePlainLimit(rec[point], kind, s, u0, fnc.nu);
                     }
                 }
             } else if(s.feed(fx, dx, &x)) {
                 if(LEARNED) nIter += s.iter;
-                if(LEARNED && narrow && !isFinite(s.result)) {     // the predicted bracket missed: plain search
-                    narrow = false;
-                    nFallback++;
-                    if(startPlain(s, kind, ends ? ends + point : nullptr, plainLo, plainHi, tol, u0, fnc.D2, fnc.E, &x)) {
-                        busy = false;
-                        storePlainLimit(rec[point], kind, s, u0, fnc.nu);
-                    }
-                } else if(LEARNED && narrow) {
+                if(LEARNED && seeded && isFinite(s.result)) {
                     verifying = true;
                     verified = s.result;
-                    x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? plainLo : plainHi));
+                    const FudgeRecord& r = rec[point];
+                    const double negEnd = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 1;
+                    x = 0.5 * (s.result + negEnd);
                 } else {
                     busy = false;
                     storePlainLimit(rec[point], kind, s, u0, fnc.nu);
@@ -203,15 +181,15 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
         }
     }
     if(LEARNED && stats) {     // one atomic per warp and counter
-        nSearch = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nSearch));
-        nNarrow = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nNarrow));
-        nFallback = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nFallback));
-        nIter = __reduce_add_sync(FULL_MASK, static_cast<unsigned>(nIter));
+        nSearch = __reduce_add_sync(FULL_MASK, nSearch);
+        nSeeded = __reduce_add_sync(FULL_MASK, nSeeded);
+        nFallback = __reduce_add_sync(FULL_MASK, nFallback);
+        nIter = __reduce_add_sync(FULL_MASK, nIter);
         if(lane == 0) {
-            atomicAdd(stats, nSearch);
-            atomicAdd(stats + 1, nNarrow);
-            atomicAdd(stats + 2, nFallback);
-            atomicAdd(stats + 3, nIter);
+            atomicAdd(stats, static_cast<unsigned long long>(nSearch));
+            atomicAdd(stats + 1, static_cast<unsigned long long>(nSeeded));
+            atomicAdd(stats + 2, static_cast<unsigned long long>(nFallback));
+            atomicAdd(stats + 3, static_cast<unsigned long long>(nIter));
         }
     }
 }

@@ -406,7 +406,7 @@ def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
                     "plain_fp64": {"value": n / (tp / 1000), "ms_per_step": tp},
                     "speedup_vs_plain": tp / tl,
                     "max_rel_err_vs_plain": emax, "rel_err_vs_plain_q999": e999,
-                    "narrowed_searches": learned["narrowed"] / max(1, learned["searches"]),
+                    "seeded_searches": learned["narrowed"] / max(1, learned["searches"]),
                     "fallback_rate": learned["fallbacks"] / max(1, learned["narrowed"]),
                     "root_iterations_vs_plain": learned["iterations"] / max(1, plain["iterations"]),
                     "training": {"samples": ntrain, "epochs": 20, "seconds": ttrain},

@@ -300,11 +300,11 @@ int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential
 
 /* ---------------------------------------------------------------------------------------
    Learned root brackets of the action finder (no reference counterpart): a network trained on the
-   finder's own root searches predicts nu_max, lambda_min and lambda_max of each point; the
-   searches then start on the predicted bracket (strictly inside the plain one, with the plain
-   bracket's tolerance) and fall back to the plain bracket when the prediction holds no sign
-   change; points predicted near the focal line keep the plain searches, so the actions keep the
-   finder's accuracy (1e-6 of the plain searches' actions).
+   finder's own root searches predicts nu_max, lambda_min and lambda_max of each point; each
+   search then runs on its plain bracket with the plain tolerance but takes the predicted root as
+   its first iterate, and its root is checked by one evaluation beyond it (a failed check hands the
+   limit to the plain search); points predicted near the focal line keep the plain searches, so the
+   actions keep the finder's accuracy (1e-6 of the plain searches' actions).
 
    agama_actionFinderBracketSamples: the network's inputs (n x 6: the point's E, Lz, R, z, vR, vz
    in scale-free form: ln r, |z|/r, vR/v_esc, vz sign(z)/v_esc, |vphi|/v_esc with v_esc =
@@ -316,8 +316,8 @@ int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential
    the brackets: half-width = twice the 95th percentile of the held-out error, reported in
    widths[3]), attaches it and switches it on; lossHistory (epochs floats) may be NULL.
    agama_actionFinderUseBrackets: switches the trained predictor on or off.
-   agama_actionFinderBracketStats: {root searches, searches on a predicted bracket, fallbacks to
-   the plain bracket, root-finder iterations} since the last reset. */
+   agama_actionFinderBracketStats: {root searches, searches started from a predicted root, failed
+   checks (plain searches after them), root-finder iterations} since the last reset. */
 int agama_actionFinderBracketSamples(const agama_ActionFinder* actionFinder, long n, const double* posvel,
     float* features, float* target, float* mask);
 int agama_actionFinderTrainBrackets(agama_ActionFinder* actionFinder, long n, const double* posvel, int epochs,
