@@ -47,6 +47,34 @@ __device__ __forceinline__ bool startPlain(RootSearch& s, int kind, const FudgeE
     return s.startKnownEnds(lo, hi, tol, fa, da, E, NAN, x);
 }
 
+/** The predicted bracket of a search: the predicted fraction tp -+ the half-width w (the units of
+    the bracket predictor's targets), mapped to the search variable of the kind (lambda_max: the
+    semi-infinite scaling about u0 = lambda_pos).  True when it lies strictly inside the plain
+    bracket [lo, hi]: a prediction that reaches a plain end (limits near the focal line, or
+    lambda_max far out) leaves the limit to the plain search. */
+__device__ __forceinline__ bool predictedBracket(const FudgeRecord& r, int kind, double tp, double w, double u0,
+    double lo, double hi, double* nlo, double* nhi)
+{
+    const double lmd = r.lambda - r.D2;
+    if(kind == ROOT_NU_MAX) {
+        const double span = r.D2 - fabs(r.nu);
+        *nlo = fabs(r.nu) + (tp - w) * span;
+        *nhi = fabs(r.nu) + (tp + w) * span;
+    } else if(kind == ROOT_LAMBDA_MIN) {
+        *nlo = r.D2 + (tp - w) * lmd;
+        *nhi = r.D2 + (tp + w) * lmd;
+    } else {
+        const double L0 = log(fmax(r.D2 + lmd / (tp + w), u0) / u0);
+        *nlo = L0 / (1 + L0);
+        if(tp - w > 0) {
+            const double L1 = log(fmax(r.D2 + lmd / (tp - w), u0) / u0);
+            *nhi = L1 / (1 + L1);
+        } else
+            *nhi = hi;
+    }
+    return isFinite(*nlo) && isFinite(*nhi) && *nlo > lo && *nhi < hi && *nlo < *nhi;
+}
+
 /** Phase 2: every root search of the integration limits (task t = kind * n + i for the kinds
     nu_max, lambda_min, lambda_max of point i) drained from one work counter by a persistent grid.
     Each lane runs one search as a RootSearch state machine and takes the next task as soon as
@@ -58,9 +86,10 @@ __device__ __forceinline__ bool startPlain(RootSearch& s, int kind, const FudgeE
     all in [0, 1]) a search runs on its plain bracket, whose end values phase 1 has evaluated, but
     its first iterate is the predicted root instead of the interpolated one (RootSearch::seed); the
     search then goes on as the plain one does and ends inside the plain bracket with the plain
-    tolerance.  Its root is accepted only if F is negative half-way from it to the plain end where F
-    is negative (one more evaluation); otherwise F has more roots there and the plain search, which
-    may end on any of them, decides.  stats (may be null) accumulates {searches, seeded searches,
+    tolerance.  Seeding needs the predicted bracket (predictedBracket) strictly inside the plain
+    one, and the root is accepted only if it lies inside that predicted bracket and F is negative
+    half-way from it to the plain end where F is negative (one more evaluation); otherwise F may
+    have more roots there and the plain search, which may end on any of them, decides.  stats (may be null) accumulates {searches, seeded searches,
     plain searches after a failed check, iterations}.  LEARNED = false (no predictions, no stats)
     compiles the plain searches alone, without that state and the counters (fewer registers). */
 template<bool LEARNED>
@@ -114,7 +143,8 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                             // there the GL action integrals resolve the integrands poorly and depend
                             // on the limits to the last bits of the plain searches
                             const bool nearFocal = pred[3 * i] + 2 * widths.w[0] >= 1 || pred[3 * i + 1] - 2 * widths.w[1] <= 0;
-                            if(!nearFocal) {
+                            double nlo, nhi;
+                            if(!nearFocal && predictedBracket(r, kind, pred[3 * i + k], widths.w[k], u0, lo, hi, &nlo, &nhi)) {
                                 const double tp = pred[3 * i + k], lmd = r.lambda - r.D2;
                                 double guess;
                                 if(kind == ROOT_NU_MAX) guess = fabs(r.nu) + tp * (r.D2 - fabs(r.nu));
@@ -166,13 +196,33 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                 }
             } else if(s.feed(fx, dx, &x)) {
                 if(LEARNED) nIter += s.iter;
-                if(LEARNED && seeded && isFinite(s.result)) {
-                    verifying = true;
-                    verified = s.result;
+                bool check = false;     // the search goes on (a check evaluation or a plain search)
+                if(LEARNED && seeded) {
+                    // a seeded root is a candidate only inside the predicted bracket (it may have
+                    // come from another root of F in the plain bracket otherwise)
                     const FudgeRecord& r = rec[point];
-                    const double negEnd = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 1;
-                    x = 0.5 * (s.result + negEnd);
-                } else {
+                    const int k = kind == ROOT_NU_MAX ? 0 : kind == ROOT_LAMBDA_MIN ? 1 : 2;
+                    const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
+                    const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
+                    double nlo, nhi;
+                    predictedBracket(r, kind, pred[3 * point + k], widths.w[k], u0, lo, hi, &nlo, &nhi);
+                    if(isFinite(s.result) && s.result >= nlo && s.result <= nhi) {
+                        check = true;
+                        verifying = true;
+                        verified = s.result;
+                        x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? lo : hi));
+                    } else {
+                        seeded = false;
+                        nFallback++;
+                        check = true;       // handled: the plain search runs from here
+                        if(startPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
+                                      u0, fnc.D2, fnc.E, &x)) {
+                            busy = false;
+                            storePlainLimit(rec[point], kind, s, u0, fnc.nu);
+                        }
+                    }
+                }
+                if(!check) {
                     busy = false;
                     storePlainLimit(rec[point], kind, s, u0, fnc.nu);
                     if(iters) atomicAdd(iters + point, s.iter);
