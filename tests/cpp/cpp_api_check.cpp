@@ -1,0 +1,65 @@
+// Drives the C++ mirror of the reference API (include/agama_b200.hpp) the way a reference C++
+// caller would: reads points from text files, writes the engine's results as text.
+//   cpp_api_check <coef file> <points n x 3> <phase-space points n x 6> <out prefix>
+// Writes <prefix>_pot.txt (Phi, dPhi/dx, dPhi/dy, dPhi/dz per point), <prefix>_act.txt
+// (Jr, Jz, Jphi per point through ActionFinderAxisymFudge::actions on PosVelCyl input) and
+// <prefix>_orb.txt (final point after T = 1 of each phase-space point, Omega = 0).
+// Exit status 3 when the engine refuses to run (no CUDA device), with the message on stderr.
+#include "agama_b200.hpp"
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <vector>
+
+using namespace agama_b200;
+
+static std::vector<double> readAll(const char* file)
+{
+    std::ifstream f(file);
+    std::vector<double> v;
+    double x;
+    while(f >> x) v.push_back(x);
+    return v;
+}
+
+int main(int argc, char** argv)
+{
+    if(argc != 5) { std::cerr << "usage: cpp_api_check coef pos3 posvel6 outprefix\n"; return 2; }
+    try {
+        potential::PtrPotential pot(new potential::Multipole(argv[1]));
+        const std::vector<double> p3 = readAll(argv[2]), p6 = readAll(argv[3]);
+        const std::string prefix = argv[4];
+        FILE* f = std::fopen((prefix + "_pot.txt").c_str(), "w");
+        for(size_t i = 0; i + 2 < p3.size(); i += 3) {
+            double phi;
+            coord::GradCar g;
+            pot->eval(coord::PosCar(p3[i], p3[i + 1], p3[i + 2]), &phi, &g);
+            std::fprintf(f, "%.17g %.17g %.17g %.17g\n", phi, g.dx, g.dy, g.dz);
+        }
+        std::fclose(f);
+        actions::ActionFinderAxisymFudge af(pot);
+        f = std::fopen((prefix + "_act.txt").c_str(), "w");
+        for(size_t i = 0; i + 5 < p6.size(); i += 6) {
+            // the reference's finder takes cylindrical points
+            const double x = p6[i], y = p6[i + 1], R = std::sqrt(x * x + y * y), phi = std::atan2(y, x);
+            const double c = R > 0 ? x / R : 1, s = R > 0 ? y / R : 0;
+            const coord::PosVelCyl pc(R, p6[i + 2], phi, p6[i + 3] * c + p6[i + 4] * s, p6[i + 5],
+                                      -p6[i + 3] * s + p6[i + 4] * c);
+            const actions::Actions a = af.actions(pc);
+            std::fprintf(f, "%.17g %.17g %.17g\n", a.Jr, a.Jz, a.Jphi);
+        }
+        std::fclose(f);
+        f = std::fopen((prefix + "_orb.txt").c_str(), "w");
+        for(size_t i = 0; i + 5 < p6.size(); i += 6) {
+            const coord::PosVelCar e = orbit::integrate(
+                coord::PosVelCar(p6[i], p6[i + 1], p6[i + 2], p6[i + 3], p6[i + 4], p6[i + 5]), 1.0, *pot);
+            std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", e.x, e.y, e.z, e.vx, e.vy, e.vz);
+        }
+        std::fclose(f);
+    } catch(std::exception& e) {
+        std::cerr << "cpp_api_check: " << e.what() << "\n";
+        return 3;
+    }
+    return 0;
+}
