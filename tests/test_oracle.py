@@ -42,6 +42,28 @@ def test_reference_orbits_reproduce_golden():
 
 
 @needs_ref
+def test_reference_rotating_frame_and_trajectories_reproduce_golden():
+    g = np.load(os.path.join(GOLDEN, "orbits_cfg3.npz"))
+    pot = ref.Potential(file=os.path.join(GOLDEN, "cfg3.coef"))
+    final, steps, _ = pot.orbits(g["ic"][:3], g["T"][:3], Omega=float(g["Omega"]), accuracy=float(g["accuracy"]),
+                                 nthreads=1)
+    np.testing.assert_array_equal(final, g["final"][:3])
+    np.testing.assert_array_equal(steps, g["steps"][:3])
+    traj = pot.orbits_traj(g["ic"][:3], g["T"][:3], 11, Omega=float(g["Omega"]), accuracy=float(g["accuracy"]),
+                           nthreads=1)
+    np.testing.assert_array_equal(traj, g["traj11"][:3])
+
+
+@needs_ref
+def test_reference_angles_reproduce_golden():
+    g = np.load(os.path.join(GOLDEN, "actions_cfg5.npz"))
+    pot = ref.Potential(file=os.path.join(GOLDEN, "cfg5.coef"))
+    act, ang, freq = pot.actions_angles_fd(g["points"][:100], g["fd"][:100], nthreads=1)
+    np.testing.assert_array_equal(ang, g["ang_fd"][:100])
+    np.testing.assert_array_equal(freq, g["freq_fd"][:100])
+
+
+@needs_ref
 def test_reference_actions_reproduce_golden():
     g = np.load(os.path.join(GOLDEN, "actions_cfg2.npz"))
     pot = ref.Potential(file=os.path.join(GOLDEN, "cfg2.coef"))
