@@ -11,6 +11,8 @@ Every function below forwards to the reference's own code path for the hot path:
   ActionFinder.actions actions::ActionFinderAxisymFudge::eval actions_staeckel.cpp:954-979
   CInterfacePotential  the reference's plain-C interface       interface_c.cpp:31-111
                        (density, R_circ, R_from_Lz, R_max, findPlanarOrbitExtent)
+  ref_find_root_poly   math::findRoot on a polynomial          math_core.cpp:895-1041
+                       (called through lib() by tests/test_rootsearch.py)
 """
 import ctypes
 import os

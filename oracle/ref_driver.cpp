@@ -28,6 +28,7 @@
 #include "actions_staeckel.h"
 #include "potential_utils.h"
 #include "math_spline.h"
+#include "math_core.h"
 #undef private
 #undef protected
 #include "potential_factory.h"
@@ -375,4 +376,33 @@ int ref_actionfinder_lcirc(void* handle, long n, const double* E, double* L) {
     return 0;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// The reference's root finder on a test function (checker of the engine's restatement)
+
+namespace {
+/// sum_k c[k] x^k and its derivative by Horner's rule: a test function with one derivative
+class PolyFnc : public math::IFunction {
+    const double* c;
+    int n;
+public:
+    PolyFnc(const double* c_, int n_) : c(c_), n(n_) {}
+    virtual void evalDeriv(const double x, double* val, double* der, double*) const {
+        double v = 0, d = 0;
+        for(int k = n - 1; k >= 0; k--) { d = d * x + v; v = v * x + c[k]; }
+        if(val) *val = v;
+        if(der) *der = d;
+    }
+    virtual unsigned int numDerivs() const { return 1; }
+};
+}  // namespace
+
+extern "C" {
+/// math::findRoot (src/math_core.cpp:895-1041) of the polynomial c[0..n-1] on [lo, hi]
+int ref_find_root_poly(const double* c, int n, double lo, double hi, double reltol, double* root)
+{
+    try { *root = math::findRoot(PolyFnc(c, n), lo, hi, reltol); return 0; }
+    catch(std::exception& e) { g_error = e.what(); return -1; }
+}
 }  // extern "C"
