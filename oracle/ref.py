@@ -12,7 +12,10 @@ Every function below forwards to the reference's own code path for the hot path:
   CInterfacePotential  the reference's plain-C interface       interface_c.cpp:31-111
                        (density, R_circ, R_from_Lz, R_max, findPlanarOrbitExtent)
   ref_find_root_poly   math::findRoot on a polynomial          math_core.cpp:895-1041
-                       (called through lib() by tests/test_rootsearch.py)
+  ref_sph_harm_array   math::sphHarmArray                      math_sphharm.cpp:63-132
+  ref_trig_multi_angle math::trigMultiAngle                    math_sphharm.cpp:134-154
+  ref_unscale / _scale math::unscale / scale                   math_core.cpp:296-396
+                       (called through lib() by tests/test_rootsearch.py, test_numerics_oracle.py)
 """
 import ctypes
 import os

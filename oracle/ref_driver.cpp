@@ -29,6 +29,7 @@
 #include "potential_utils.h"
 #include "math_spline.h"
 #include "math_core.h"
+#include "math_sphharm.h"
 #undef private
 #undef protected
 #include "potential_factory.h"
@@ -404,5 +405,42 @@ int ref_find_root_poly(const double* c, int n, double lo, double hi, double relt
 {
     try { *root = math::findRoot(PolyFnc(c, n), lo, hi, reltol); return 0; }
     catch(std::exception& e) { g_error = e.what(); return -1; }
+}
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// The reference's Legendre, multiple-angle and interval-scaling routines (checkers of the
+// engine's restatements)
+
+extern "C" {
+/// math::sphHarmArray (src/math_sphharm.cpp:63-132): lmax-m+1 values and derivatives
+int ref_sph_harm_array(int lmax, int m, double tau, double* P, double* dP, double* d2P)
+{
+    try { math::sphHarmArray(lmax, m, tau, P, dP, d2P); return 0; }
+    catch(std::exception& e) { g_error = e.what(); return -1; }
+}
+
+/// math::trigMultiAngle (src/math_sphharm.cpp:134-154)
+int ref_trig_multi_angle(double phi, int m, int needSine, double* out)
+{
+    math::trigMultiAngle(phi, m, needSine != 0, out);
+    return 0;
+}
+
+/// math::unscale / math::scale (src/math_core.cpp:296-396) of kind 0 ScalingInf, 1 ScalingSemiInf(a),
+/// 2 ScalingCub(a, b)
+int ref_unscale(int kind, double a, double b, double s, double* u, double* duds)
+{
+    if(kind == 0) *u = math::unscale(math::ScalingInf(), s, duds);
+    else if(kind == 1) *u = math::unscale(math::ScalingSemiInf(a), s, duds);
+    else *u = math::unscale(math::ScalingCub(a, b), s, duds);
+    return 0;
+}
+int ref_scale(int kind, double a, double b, double u, double* s)
+{
+    if(kind == 0) *s = math::scale(math::ScalingInf(), u);
+    else if(kind == 1) *s = math::scale(math::ScalingSemiInf(a), u);
+    else *s = math::scale(math::ScalingCub(a, b), u);
+    return 0;
 }
 }  // extern "C"
