@@ -10,7 +10,7 @@
      actions::ActionFinderAxisymFudge::eval / actions                    src/actions_base.h:65-75,
                                                                          src/actions_staeckel.cpp:954-979
      orbit::OrbitIntParams, orbit::integrate (final point of a DOP853     src/orbit.h:116-129, 165-315
-       orbit in the frame rotating with Omega)
+       orbit in the frame rotating with Omega), orbit::integrateTraj        src/orbit.h:297-316
 
    Errors raise std::runtime_error with the engine's message, as the reference's constructors and
    factories throw; evaluations of points without a value (unbound orbits) give NaN as there.
@@ -24,7 +24,9 @@
 #include <cstddef>
 #include <memory>
 #include <stdexcept>
+#include <algorithm>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace agama_b200 {
@@ -67,6 +69,26 @@ public:
     explicit Multipole(const std::string& coefFile)
     {
         agama_Potential* p = agama_createPotential(("type=Multipole, file=" + coefFile).c_str());
+        if(!p) throw std::runtime_error(agama_getError());
+        h.reset(p, agama_deletePotential);
+    }
+    /// from the spherical-harmonic coefficients at the radial grid: Phi[c][k], dPhi[c][k] for the
+    /// coefficient index c = l (l + 1) + m and radius k (Multipole(radii, Phi, dPhi),
+    /// src/potential_multipole.h:257-266)
+    Multipole(const std::vector<double>& radii, const std::vector<std::vector<double> >& Phi,
+        const std::vector<std::vector<double> >& dPhi)
+    {
+        const size_t nr = radii.size(), nc = Phi.size();
+        if(dPhi.size() != nc) throw std::invalid_argument("Multipole: Phi and dPhi differ in size");
+        std::vector<double> P(nc * nr), D(nc * nr);
+        for(size_t c = 0; c < nc; c++) {
+            if(Phi[c].size() != nr || dPhi[c].size() != nr)
+                throw std::invalid_argument("Multipole: each coefficient needs one value per radius");
+            std::copy(Phi[c].begin(), Phi[c].end(), P.begin() + c * nr);
+            std::copy(dPhi[c].begin(), dPhi[c].end(), D.begin() + c * nr);
+        }
+        agama_Potential* p = agama_createMultipoleFromCoefs(static_cast<int>(nr), radii.data(), static_cast<int>(nc),
+            P.data(), D.data());
         if(!p) throw std::runtime_error(agama_getError());
         h.reset(p, agama_deletePotential);
     }
@@ -220,6 +242,42 @@ inline coord::PosVelCar integrate(const coord::PosVelCar& ic, double T, const po
 {
     coord::PosVelCar out;
     integratemany(1, &ic, &T, pot, Omega, params, &out);
+    return out;
+}
+
+/// points of a trajectory with their times (orbit::Trajectory, src/orbit.h:82)
+typedef std::vector<std::pair<coord::PosVelCar, double> > Trajectory;
+
+/** The trajectory of one orbit sampled every samplingInterval from startTime to startTime +
+    totalTime (orbit::integrateTraj, src/orbit.h:297-316, with the reference's RuntimeTrajectory:
+    7th-order dense output of the DOP853 steps).  The engine samples at regular times that end on
+    totalTime, so samplingInterval must divide totalTime (to 1e-12 relative); recording every step
+    (samplingInterval = 0) is not offered. */
+inline Trajectory integrateTraj(const coord::PosVelCar& initialConditions, double totalTime, double samplingInterval,
+    const potential::Multipole& pot, double Omega = 0, const OrbitIntParams& params = OrbitIntParams(),
+    double startTime = 0)
+{
+    if(!(samplingInterval > 0))
+        throw std::invalid_argument("integrateTraj: the engine samples at regular intervals (samplingInterval > 0)");
+    const double steps = std::fabs(totalTime) / samplingInterval;
+    const double k = std::floor(steps + 0.5);
+    if(std::fabs(steps - k) > 1e-12 * std::fmax(1.0, steps))
+        throw std::invalid_argument("integrateTraj: samplingInterval must divide totalTime");
+    const int trajSize = static_cast<int>(k) + 1;
+    const double ic[6] = { initialConditions.x, initialConditions.y, initialConditions.z,
+                           initialConditions.vx, initialConditions.vy, initialConditions.vz };
+    std::vector<double> traj(6 * static_cast<size_t>(std::max(trajSize, 2)));
+    long numSteps = 0;
+    int status = 0;
+    detail::check(agama_integrateOrbitsTrajectoryMany(pot.handle(), 1, ic, &totalTime, Omega, params.accuracy,
+        static_cast<long>(params.maxNumSteps), std::max(trajSize, 2), traj.data(), NULL, &numSteps, &status));
+    Trajectory out;
+    for(int j = 0; j < trajSize; j++) {
+        const double* q = &traj[6 * j];
+        if(!std::isfinite(q[0])) break;           // the orbit stopped before this sample
+        const double t = trajSize > 1 ? totalTime * j / (trajSize - 1) : 0;
+        out.push_back(std::make_pair(coord::PosVelCar(q[0], q[1], q[2], q[3], q[4], q[5]), startTime + t));
+    }
     return out;
 }
 

@@ -3,7 +3,8 @@
 //   cpp_api_check <coef file> <points n x 3> <phase-space points n x 6> <out prefix>
 // Writes <prefix>_pot.txt (Phi, dPhi/dx, dPhi/dy, dPhi/dz per point), <prefix>_act.txt
 // (Jr, Jz, Jphi per point through ActionFinderAxisymFudge::actions on PosVelCyl input) and
-// <prefix>_orb.txt (final point after T = 1 of each phase-space point, Omega = 0).
+// <prefix>_orb.txt (final point after T = 1 of each phase-space point, Omega = 0) and
+// <prefix>_traj.txt (time and point of 11 samples of the first orbit over T = 1).
 // Exit status 3 when the engine refuses to run (no CUDA device), with the message on stderr.
 #include "agama_b200.hpp"
 #include <cmath>
@@ -57,6 +58,16 @@ int main(int argc, char** argv)
             std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", e.x, e.y, e.z, e.vx, e.vy, e.vz);
         }
         std::fclose(f);
+        // a trajectory of the first phase-space point: 11 samples over T = 1
+        if(p6.size() >= 6) {
+            const orbit::Trajectory traj = orbit::integrateTraj(
+                coord::PosVelCar(p6[0], p6[1], p6[2], p6[3], p6[4], p6[5]), 1.0, 0.1, *pot);
+            f = std::fopen((prefix + "_traj.txt").c_str(), "w");
+            for(size_t j = 0; j < traj.size(); j++)
+                std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", traj[j].second, traj[j].first.x,
+                             traj[j].first.y, traj[j].first.z, traj[j].first.vx, traj[j].first.vy, traj[j].first.vz);
+            std::fclose(f);
+        }
     } catch(std::exception& e) {
         std::cerr << "cpp_api_check: " << e.what() << "\n";
         return 3;
