@@ -13,7 +13,8 @@
        orbit in the frame rotating with Omega), orbit::integrateTraj        src/orbit.h:297-316
 
    Errors raise std::runtime_error with the engine's message, as the reference's constructors and
-   factories throw; evaluations of points without a value (unbound orbits) give NaN as there.
+   factories throw; evaluations of points without a value (unbound orbits) give NaN as there, and
+   the radius routines return NaN on failure as the plain-C interface does.
    The batched members (evalmany..., integratemany) take whole arrays in one call; the reference
    batches the same operations only in its Python binding. */
 #ifndef AGAMA_B200_HPP
