@@ -2,7 +2,8 @@
 // caller would: reads points from text files, writes the engine's results as text.
 //   cpp_api_check <coef file> <points n x 3> <phase-space points n x 6> <out prefix>
 // Writes <prefix>_pot.txt (Phi, dPhi/dx, dPhi/dy, dPhi/dz per point), <prefix>_act.txt
-// (Jr, Jz, Jphi per point through ActionFinderAxisymFudge::actions on PosVelCyl input) and
+// (Jr, Jz, Jphi per point through ActionFinderAxisymFudge::evalmany; the first point also through
+// actions() on cylindrical input, printed to stderr) and
 // <prefix>_orb.txt (final point after T = 1 of each phase-space point, Omega = 0) and
 // <prefix>_traj.txt (time and point of 11 samples of the first orbit over T = 1).
 // Exit status 3 when the engine refuses to run (no CUDA device), with the message on stderr.
@@ -40,23 +41,29 @@ int main(int argc, char** argv)
         }
         std::fclose(f);
         actions::ActionFinderAxisymFudge af(pot);
+        const size_t n6 = p6.size() / 6;
+        std::vector<coord::PosVelCar> pv(n6);
+        for(size_t i = 0; i < n6; i++)
+            pv[i] = coord::PosVelCar(p6[6 * i], p6[6 * i + 1], p6[6 * i + 2], p6[6 * i + 3], p6[6 * i + 4], p6[6 * i + 5]);
+        std::vector<actions::Actions> act(n6);
+        af.evalmany(n6, pv.data(), act.data());
         f = std::fopen((prefix + "_act.txt").c_str(), "w");
-        for(size_t i = 0; i + 5 < p6.size(); i += 6) {
-            // the reference's finder takes cylindrical points
-            const double x = p6[i], y = p6[i + 1], R = std::sqrt(x * x + y * y), phi = std::atan2(y, x);
-            const double c = R > 0 ? x / R : 1, s = R > 0 ? y / R : 0;
-            const coord::PosVelCyl pc(R, p6[i + 2], phi, p6[i + 3] * c + p6[i + 4] * s, p6[i + 5],
-                                      -p6[i + 3] * s + p6[i + 4] * c);
-            const actions::Actions a = af.actions(pc);
-            std::fprintf(f, "%.17g %.17g %.17g\n", a.Jr, a.Jz, a.Jphi);
-        }
+        for(size_t i = 0; i < n6; i++) std::fprintf(f, "%.17g %.17g %.17g\n", act[i].Jr, act[i].Jz, act[i].Jphi);
         std::fclose(f);
-        f = std::fopen((prefix + "_orb.txt").c_str(), "w");
-        for(size_t i = 0; i + 5 < p6.size(); i += 6) {
-            const coord::PosVelCar e = orbit::integrate(
-                coord::PosVelCar(p6[i], p6[i + 1], p6[i + 2], p6[i + 3], p6[i + 4], p6[i + 5]), 1.0, *pot);
-            std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", e.x, e.y, e.z, e.vx, e.vy, e.vz);
+        if(n6 > 0) {       // the reference's own call form: one cylindrical point
+            const double x = p6[0], y = p6[1], R = std::sqrt(x * x + y * y), phi = std::atan2(y, x);
+            const double c = R > 0 ? x / R : 1, s = R > 0 ? y / R : 0;
+            const actions::Actions a = af.actions(coord::PosVelCyl(R, p6[2], phi, p6[3] * c + p6[4] * s, p6[5],
+                                                                   -p6[3] * s + p6[4] * c));
+            std::fprintf(stderr, "actions of the first point (cylindrical input): %.17g %.17g %.17g\n", a.Jr, a.Jz, a.Jphi);
         }
+        std::vector<double> T(n6, 1.0);
+        std::vector<coord::PosVelCar> fin(n6);
+        orbit::integratemany(n6, pv.data(), T.data(), *pot, 0, orbit::OrbitIntParams(), fin.data());
+        f = std::fopen((prefix + "_orb.txt").c_str(), "w");
+        for(size_t i = 0; i < n6; i++)
+            std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", fin[i].x, fin[i].y, fin[i].z, fin[i].vx, fin[i].vy,
+                         fin[i].vz);
         std::fclose(f);
         // a trajectory of the first phase-space point: 11 samples over T = 1
         if(p6.size() >= 6) {
