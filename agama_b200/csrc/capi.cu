@@ -47,8 +47,19 @@ std::string coefFileFromParams(const char* params)
     return file;
 }
 
+/// restores the caller's current device when an entry point returns (the entry points make the
+/// device of their object current for their own work)
+struct CurrentDeviceGuard {
+    int device = -1;
+    CurrentDeviceGuard() { if(cudaGetDevice(&device) != cudaSuccess) { device = -1; cudaGetLastError(); } }
+    ~CurrentDeviceGuard() { if(device >= 0) cudaSetDevice(device); }
+    CurrentDeviceGuard(const CurrentDeviceGuard&) = delete;
+    CurrentDeviceGuard& operator=(const CurrentDeviceGuard&) = delete;
+};
+
 template<class F>
 int guarded(F&& f) {
+    CurrentDeviceGuard keep;
     try { f(); return 0; }
     catch(std::exception& e) { setError(e.what()); return -1; }
 }
@@ -391,6 +402,7 @@ extern "C" agama_OrbitGraph* agama_orbitGraphCreate(const agama_Potential* p, lo
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState, long* numSteps,
     long* numRejected, int* status)
 {
+    CurrentDeviceGuard keep;
     try {
         if(!p || n <= 0 || !ic || !T || !finalState) throw std::invalid_argument("orbitGraphCreate: invalid arguments");
         AGB_CUDA(cudaSetDevice(p->pot->device));
@@ -496,6 +508,7 @@ extern "C" agama_ActionFinder* agama_createActionFinderFromTables(const agama_Po
     int nLofE, const double* LofE, int nRofL, const double* RofL, int nPhiofR, const double* PhiofR,
     const double* scalars)
 {
+    CurrentDeviceGuard keep;
     try {
         requireAxisymmetric(p);
         if(nE < 2 || nL < 2 || !gridE || !gridL || !delta || nLofE < 2 || !LofE || nRofL < 2 || !RofL ||
@@ -517,6 +530,7 @@ extern "C" agama_ActionFinder* agama_createActionFinderFromTables(const agama_Po
 
 extern "C" agama_ActionFinder* agama_createActionFinder(const agama_Potential* p)
 {
+    CurrentDeviceGuard keep;
     try {
         requireAxisymmetric(p);
         AGB_CUDA(cudaSetDevice(p->pot->device));

@@ -14,6 +14,8 @@
 #include "host_pipeline.h"
 #include <cuda_bf16.h>
 #include <random>
+#include <mutex>
+#include <set>
 #include <algorithm>
 #include <cmath>
 
@@ -569,10 +571,15 @@ std::vector<float> Mlp::train(long n, const float* x, const float* t, const floa
 void Mlp::predict(long n, const float* x, float* y, cudaStream_t s) const
 {
     if(n <= 0) return;
-    static bool attr = false;
-    if(!attr) {
-        AGB_CUDA(cudaFuncSetAttribute(mlpInferKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, INF_SMEM));
-        attr = true;
+    {
+        // the kernel's shared-memory limit is a per-device attribute: raise it once per device
+        static std::mutex mtx;
+        static std::set<int> raised;
+        std::lock_guard<std::mutex> lock(mtx);
+        if(!raised.count(device)) {
+            AGB_CUDA(cudaFuncSetAttribute(mlpInferKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, INF_SMEM));
+            raised.insert(device);
+        }
     }
     int sms = 0;
     AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -587,7 +594,10 @@ void Mlp::checkError() const
 {
     int h = 0;
     AGB_CUDA(cudaMemcpy(&h, error.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-    if(h) throw std::runtime_error("mlp: tensor-core completion barrier timed out");
+    if(h) {
+        AGB_CUDA(cudaMemset(error.ptr, 0, sizeof(int)));      // reported once
+        throw std::runtime_error("mlp: tensor-core completion barrier timed out");
+    }
 }
 
 }  // namespace agb

@@ -12,6 +12,8 @@
 #include "umma.cuh"
 #include "mlp.h"
 #include <cuda_bf16.h>
+#include <map>
+#include <mutex>
 
 namespace agb {
 
@@ -91,14 +93,31 @@ __global__ void __launch_bounds__(128) gemmBf16Kernel(int M, int N, int K, const
     if(warp == 0) umma::tmemFree(tmem, 128);
 }
 
-int* gemmErrorFlag()
+/// per-device state of the GEMM: its completion-timeout flag (device memory of that device) and
+/// whether the kernel's dynamic shared-memory limit has been raised there
+struct GemmDeviceState {
+    int* flag = nullptr;
+    bool attr = false;
+};
+std::mutex g_gemmMutex;
+std::map<int, GemmDeviceState> g_gemmState;
+
+/// the state of the current device, set up on its first use (with that device current)
+GemmDeviceState& gemmState()
 {
-    static int* flag = nullptr;     // one per process on the first device used (zeroed at allocation)
-    if(!flag) {
-        AGB_CUDA(cudaMalloc(&flag, sizeof(int)));
-        AGB_CUDA(cudaMemset(flag, 0, sizeof(int)));
+    int dev;
+    AGB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_gemmMutex);
+    GemmDeviceState& st = g_gemmState[dev];        // map references stay valid as entries are added
+    if(!st.flag) {
+        AGB_CUDA(cudaMalloc(&st.flag, sizeof(int)));
+        AGB_CUDA(cudaMemset(st.flag, 0, sizeof(int)));
     }
-    return flag;
+    if(!st.attr) {
+        AGB_CUDA(cudaFuncSetAttribute(gemmBf16Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+        st.attr = true;
+    }
+    return st;
 }
 
 }  // namespace
@@ -109,22 +128,23 @@ void launchGemmBf16(int M, int N, int K, const void* A, const void* B, float* C,
     if(M <= 0 || N <= 0 || K <= 0) return;
     if(M % GEMM_BM || N % GEMM_BN || K % GEMM_BK || ldc < N)
         throw std::invalid_argument("gemmBf16: M, N must be multiples of 128, K of 64, ldc >= N");
-    static bool attr = false;
-    if(!attr) {
-        AGB_CUDA(cudaFuncSetAttribute(gemmBf16Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
-        attr = true;
-    }
+    GemmDeviceState& st = gemmState();
     const dim3 grid(N / GEMM_BN, M / GEMM_BM);
     gemmBf16Kernel<<<grid, 128, GEMM_SMEM, stream>>>(M, N, K, static_cast<const __nv_bfloat16*>(A),
-        static_cast<const __nv_bfloat16*>(B), C, ldc, accumulate ? 1 : 0, gemmErrorFlag());
+        static_cast<const __nv_bfloat16*>(B), C, ldc, accumulate ? 1 : 0, st.flag);
     AGB_CUDA(cudaGetLastError());
 }
 
 void checkGemmError()
 {
+    // the flag of the current device; cleared once read, so a timeout is reported once
+    int* flag = gemmState().flag;
     int h = 0;
-    AGB_CUDA(cudaMemcpy(&h, gemmErrorFlag(), sizeof(int), cudaMemcpyDeviceToHost));
-    if(h) throw std::runtime_error("gemmBf16: tensor-core completion barrier timed out");
+    AGB_CUDA(cudaMemcpy(&h, flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if(h) {
+        AGB_CUDA(cudaMemset(flag, 0, sizeof(int)));
+        throw std::runtime_error("gemmBf16: tensor-core completion barrier timed out");
+    }
 }
 
 }  // namespace agb

@@ -429,17 +429,6 @@ __device__ void evalInterp2d(const MultipoleView& M, double R, double z, double 
     }
 }
 
-/// sum of v over the G consecutive lanes of this lane's group, in a fixed lane order, so that
-/// every lane of the group gets the same bits
-template<int G>
-__device__ __forceinline__ double groupSum(double v, unsigned mask)
-{
-    double s = __shfl_sync(mask, v, 0, G);
-#pragma unroll
-    for(int j = 1; j < G; j++) s += __shfl_sync(mask, v, j, G);
-    return s;
-}
-
 /// the lanes of this lane's group of G consecutive lanes
 template<int G>
 __device__ __forceinline__ unsigned groupMask()
@@ -457,8 +446,9 @@ __device__ __forceinline__ unsigned groupMask()
     MIXED: the m != 0 harmonics from the FP32 table in FP32 arithmetic (their sum in FP64).
     G > 1: the evaluation is shared by a group of G consecutive lanes that evaluate the same
     point: lane j of the group evaluates the harmonics s = j, j + G, ..., the m = 0 terms are
-    broadcast from lane 0 and the Fourier sums are added over the group in a fixed order (every
-    lane returns the same bits; the sums are ordered by lane, not by m). */
+    broadcast from lane 0, every scaled harmonic is then broadcast from the lane that evaluated
+    it, and every lane forms the Fourier sums itself in the order m = 0, then ascending m.  The
+    arithmetic of each harmonic and of the sums is that of G = 1, so every G gives the same bits. */
 template<int NQ, int MAXS, int G = 1, bool MIXED = false>
 __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
@@ -524,14 +514,25 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
             }
         }
     }
+    if(G > 1) {     // every lane gets every harmonic from the lane that evaluated it
+#pragma unroll
+        for(int s = 1; s < MAXS; s++) {
+            if(s < M.nFast) {
+                P[s] = __shfl_sync(gmask, P[s], s % G, G);
+                if(NQ >= 3) { Dr[s] = __shfl_sync(gmask, Dr[s], s % G, G); Dt[s] = __shfl_sync(gmask, Dt[s], s % G, G); }
+                if(NQ == 6) {
+                    Drr[s] = __shfl_sync(gmask, Drr[s], s % G, G); Drt[s] = __shfl_sync(gmask, Drt[s], s % G, G);
+                    Dtt[s] = __shfl_sync(gmask, Dtt[s], s % G, G);
+                }
+            }
+        }
+    }
     // Fourier synthesis in the reference's order: m = 0, then the others by ascending m
-    // (G > 1: each lane sums its own harmonics, lane 0 starting from m = 0; then the group sum)
     SphDerivs gs; SphHess hs;
-    const bool own0 = gl == 0;
-    *pot = own0 ? P[0] : 0;
-    if(NQ >= 3) { gs.dr = own0 ? Dr[0] : 0; gs.dt = own0 ? Dt[0] : 0; gs.dphi = 0; }
+    *pot = P[0];
+    if(NQ >= 3) { gs.dr = Dr[0]; gs.dt = Dt[0]; gs.dphi = 0; }
     if(NQ == 6) {
-        hs.dr2 = own0 ? Drr[0] : 0; hs.drdt = own0 ? Drt[0] : 0; hs.dt2 = own0 ? Dtt[0] : 0;
+        hs.dr2 = Drr[0]; hs.drdt = Drt[0]; hs.dt2 = Dtt[0];
         hs.drdphi = hs.dtdphi = hs.dphi2 = 0;
     }
     if(MAXS > 1 && M.nFast > 1) {
@@ -554,7 +555,7 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
         }
 #pragma unroll
         for(int s = 1; s < MAXS; s++) {
-            if(s < M.nFast && s % G == gl) {
+            if(s < M.nFast) {
                 const int m = M.fastM[s];
                 const double tr = m > 0 ? cm[s] : sm[s];
                 const double dtr = m > 0 ? -m * sm[s] : -m * cm[s];
@@ -574,15 +575,6 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
                     hs.dphi2 += P[s] * d2tr;
                 }
             }
-        }
-    }
-    if(G > 1) {
-        *pot = groupSum<G>(*pot, gmask);
-        if(NQ >= 3) { gs.dr = groupSum<G>(gs.dr, gmask); gs.dt = groupSum<G>(gs.dt, gmask); gs.dphi = groupSum<G>(gs.dphi, gmask); }
-        if(NQ == 6) {
-            hs.dr2 = groupSum<G>(hs.dr2, gmask); hs.drdt = groupSum<G>(hs.drdt, gmask); hs.dt2 = groupSum<G>(hs.dt2, gmask);
-            hs.drdphi = groupSum<G>(hs.drdphi, gmask); hs.dtdphi = groupSum<G>(hs.dtdphi, gmask);
-            hs.dphi2 = groupSum<G>(hs.dphi2, gmask);
         }
     }
     if(NQ == 1) return;

@@ -101,22 +101,27 @@ def equatorial_average(fn, R, nphi=16):
     return v.reshape(len(R), nphi).mean(axis=1)
 
 
-def tcirc(potential_fn, force_fn, E, nphi=16, iters=80):
-    """T_circ(E) = 2 pi R_circ / v_circ(R_circ) of the axisymmetrized potential, R_circ from
-    Phi(R) + R dPhi/dR / 2 = E by bisection in ln R (the definition of T_circ,
-    src/potential_utils.h:83-87); NaN for E outside the range of circular-orbit energies"""
+def tcirc(potential_fn, force_fn, E, nphi=16, nodes=8193):
+    """T_circ(E) = 2 pi R_circ / v_circ(R_circ) of the axisymmetrized potential (the definition of
+    T_circ, src/potential_utils.h:83-87): E_c(R) = Phi(R) + R dPhi/dR / 2 and T_c(R) on a grid of
+    `nodes` radii log-spaced over [1e-8, 1e8] (spacing 0.0045 in ln R), then ln T_c as a monotone
+    cubic (PCHIP) function of E_c, evaluated at E (relative accuracy ~1e-9, far below what an
+    integration time of "10 or 100 T_circ" needs; the cost does not grow with the number of E
+    values).  E beyond the ends of the grid takes the end value."""
+    from scipy.interpolate import PchipInterpolator
+    lnR = np.linspace(np.log(1e-8), np.log(1e8), nodes)
+    R = np.exp(lnR)
+    phi = equatorial_average(potential_fn, R, nphi)
+    fR = equatorial_average(force_fn, R, nphi)
+    Ec = phi - 0.5 * R * fR
+    Tc = 2 * np.pi * R / np.sqrt(np.maximum(-R * fR, 1e-300))
+    fin = np.isfinite(Ec) & np.isfinite(Tc)
+    Ec, lnT = Ec[fin], np.log(Tc[fin])
+    top = np.maximum.accumulate(Ec)
+    keep = np.concatenate([[True], Ec[1:] > top[:-1]])     # the nodes where E_c rises strictly
+    Ec, lnT = Ec[keep], lnT[keep]
     E = np.asarray(E, dtype=np.float64)
-    lo, hi = np.full(E.shape, np.log(1e-8)), np.full(E.shape, np.log(1e8))
-    for _ in range(iters):
-        mid = 0.5 * (lo + hi)
-        R = np.exp(mid)
-        Ec = equatorial_average(potential_fn, R, nphi) - 0.5 * R * equatorial_average(force_fn, R, nphi)
-        below = Ec < E
-        lo = np.where(below, mid, lo)
-        hi = np.where(below, hi, mid)
-    R = np.exp(0.5 * (lo + hi))
-    vc = np.sqrt(-R * equatorial_average(force_fn, R, nphi))
-    return 2 * np.pi * R / vc
+    return np.exp(PchipInterpolator(Ec, lnT, extrapolate=False)(np.clip(E, Ec[0], Ec[-1])))
 
 
 def orbit_workload(cfg, potential_fn, force_fn, n=None):

@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--particles", type=int, default=1000000)
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-secondary", action="store_true", help="skip the force / orbit workloads")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run each workload's kernels once on a small case (for ncu instruction counts) and print "
+                         "the units each launch processed")
     return ap.parse_args()
 
 
@@ -148,7 +151,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "particles_per_step": sample, "threads": cores},
-        "cpu_baseline": {"value": value, "unit": "actions/s", "cores": cores, "kind": "reference",
+        "cpu_baseline": {"value": value, "unit": "actions/s", "cores": cores, "cpu_model": cpu_model(),
+                         "kind": "reference",
                          "sample": "%d of the %d config-2 particles per step" % (sample, args.particles)},
         "e2e": {"value": value, "unit": "actions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "secondary": None if args.no_secondary else run_reference_secondary(),
@@ -171,16 +175,17 @@ def run_reference_secondary():
     from agama_b200 import workloads
     _, pts1, ic1, T1, _, ic3, T3 = secondary_workloads(RefPot, lambda c: os.path.join(GOLDEN, c + ".coef"))
     p5 = RefPot(os.path.join(GOLDEN, "cfg5.coef"))
-    ic5, T5 = workloads.orbit_workload(5, p5.potential, p5.force, 1000)
+    ic5, T5 = workloads.orbit_workload(5, p5.potential, p5.force, ORBIT5_ORBITS)
     names = [("force evals/s", "config 1 forces"), ("orbit-steps/s", "config 1 orbits"),
              ("orbit-steps/s", "config 3 orbits, at most %d steps per orbit" % ORBIT3_MAX_STEPS),
              ("orbit-steps/s", "config 5 orbits"), ("actions/s", "config 5 actions of the final snapshot")]
     return [dict(metric=m, value=b and b["value"], unit=b and b.get("unit"), config=c, cpu_baseline=b)
-            for (m, c), b in zip(names, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5))]
+            for (m, c), (b, _) in zip(names, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5))]
 
 
-def cpu_baseline_line(pts):
-    """the reference's CPU action finder on the host cores, on a bounded sample"""
+def cpu_baseline_line(pts, J=None):
+    """the reference's CPU action finder on the host cores, on a bounded sample; with the engine's
+    actions J of the same points, their largest relative difference from the reference's"""
     try:
         from oracle import ref
         if not ref.available():
@@ -191,10 +196,14 @@ def cpu_baseline_line(pts):
         sample = min(len(pts), 200000)
         af.actions(pts[:2000], nthreads=cores)
         t0 = time.perf_counter()
-        af.actions(pts[:sample], nthreads=cores)
+        Jref = af.actions(pts[:sample], nthreads=cores)
         dt = time.perf_counter() - t0
-        return {"value": sample / dt, "unit": "actions/s", "cores": cores, "kind": "reference",
+        line = {"value": sample / dt, "unit": "actions/s", "cores": cores, "cpu_model": cpu_model(),
+                "kind": "reference",
                 "sample": "first %d of the config-2 particles, reference ActionFinderAxisymFudge, OpenMP" % sample}
+        if J is not None:
+            line["max_rel_err_vs_reference"] = rel_action_err(J[:sample], Jref)
+        return line
     except Exception as e:   # the baseline is reported, never required
         return {"value": None, "unit": "actions/s", "cores": os.cpu_count(), "kind": "reference",
                 "sample": "failed: %s" % e}
@@ -205,33 +214,81 @@ def cpu_baseline_line(pts):
 #   config 1 forces:  1e5 points of the triaxial Dehnen Multipole (lmax 6, 50 nodes), potential
 #                     and force per point                                   -> force evals/s
 #   config 1 orbits:  1e4 orbits, T = 10 T_circ(E), DOP853 accuracy 1e-8     -> orbit-steps/s
-#   config 3 orbits:  2e4 of the 1e5 config-3 orbits (T = 10-1000 T_circ, Omega = 0.05), at most
+#   config 3 orbits:  all 1e5 config-3 orbits (T = 10-1000 T_circ, Omega = 0.05), at most
 #                     ORBIT3_MAX_STEPS accepted steps per orbit: the workload's tail (orbits near
 #                     r ~ 1e3 whose T spans 1e4-1e6 turns of the rotating frame) needs up to 1e7
 #                     steps per orbit, hours of integration on either arm   -> orbit-steps/s
-ORBIT3_ORBITS = 20000
 ORBIT3_MAX_STEPS = 5000
-#   config 5:         5e4 of the 1e6 orbits (100 T_circ each) in the Spheroid + disk Multipole
-#                     (lmax 12, 80 nodes), then the actions of their final snapshot
-ORBIT5_ORBITS = 50000
+#   config 5:         all 1e6 orbits (100 T_circ each) in the Spheroid + disk Multipole (lmax 12,
+#                     80 nodes), then the actions of their final snapshot, plain FP64 and with
+#                     learned root brackets
+ORBIT5_ORBITS = 1000000
+# bounded samples of each workload on which the reference's CPU code is timed and compared
+REF_SAMPLE = {"orbits1": 2000, "orbits3": 400, "orbits5": 200, "actions5": 4000}
 
 
-def secondary_workloads(potential_cls, coef):
+def cpu_model():
+    """the host CPU's model name (for the cpu_baseline records)"""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def secondary_workloads(potential_cls, coef, n3=None):
     """inputs of the secondary workloads for a potential class with .potential / .force"""
     from agama_b200 import workloads
     pot1 = potential_cls(coef("cfg1"))
     pts1 = workloads.dehnen_positions(100000, 1.0, q=(0.8, 0.6), seed=workloads.SEEDS["points1"])
     ic1, T1 = workloads.orbit_workload(1, pot1.potential, pot1.force)
     pot3 = potential_cls(coef("cfg3"))
-    ic3, T3 = workloads.orbit_workload(3, pot3.potential, pot3.force, ORBIT3_ORBITS)
+    ic3, T3 = workloads.orbit_workload(3, pot3.potential, pot3.force, n3)
     return pot1, pts1, ic1, T1, pot3, ic3, T3
 
 
-def run_engine_secondary(dev, flush, dist, cpu):
+def rel_action_err(J, Jref):
+    """largest relative action error (the parity tests' measure: |dJ| / max(|J|, 1e-3 sum|J|)) and
+    whether the NaN patterns (unbound points) agree"""
+    J, Jref = np.asarray(J), np.asarray(Jref)
+    ok = np.isfinite(Jref).all(1)
+    tot = np.abs(Jref[ok]).sum(1, keepdims=True)
+    e = np.abs(J[ok] - Jref[ok]) / np.maximum(np.abs(Jref[ok]), 1e-3 * tot)
+    return {"max": float(e.max()) if e.size else 0.0, "q999": float(np.quantile(e, 0.999)) if e.size else 0.0,
+            "points": int(len(Jref)), "nan_pattern_equal": bool(np.array_equal(np.isfinite(J), np.isfinite(Jref)))}
+
+
+def orbit_deviation(final, status, final_ref, status_ref):
+    """final points of the engine against the reference's on the same orbits: regular orbits agree
+    to round-off growth (<= 1e-7 in the tests), chaotic ones diverge (that is their nature), so the
+    distribution is given"""
+    ok = (np.asarray(status) == 0) & (np.asarray(status_ref) == 0)
+    d = np.linalg.norm(final[ok, :3] - final_ref[ok, :3], axis=1) / np.linalg.norm(final_ref[ok, :3], axis=1)
+    return {"orbits": int(len(final)), "status_equal": float(np.mean(np.asarray(status) == np.asarray(status_ref))),
+            "final_pos_rel_median": float(np.median(d)) if d.size else None,
+            "final_pos_rel_p25": float(np.quantile(d, 0.25)) if d.size else None,
+            "frac_le_1e-7": float(np.mean(d <= 1e-7)) if d.size else None}
+
+
+def fp64_roofline(kernel, flops_per_unit, per, units, ms, peak, source):
+    """roofline record of an FP64-pipe-bound workload: executed FP64 flops per unit (ncu count of
+    dadd + dmul + 2 dfma of the kernel on this workload) x units / CUDA-event time"""
+    achieved = flops_per_unit * units / (ms / 1000) / 1e12 if flops_per_unit else None
+    return {"bound": "fp64", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if peak and achieved else None, "flops_per_unit": flops_per_unit, "per": per,
+            "flops_source": source, "peak_source": "measured FP64 FMA throughput of this device"}
+
+
+def run_engine_secondary(dev, flush, dist, cpu, peak64):
     """device-timed throughputs of the secondary workloads (max over ranks), with the reference
     on the host cores beside each when cpu is true"""
     import torch
     import agama_b200
+    from agama_b200 import workloads
 
     class Pot(agama_b200.Potential):
         def __init__(self, f):
@@ -256,50 +313,91 @@ def run_engine_secondary(dev, flush, dist, cpu):
         t = max_over_ranks(t, dist, dev)
         return t, r
 
-    out, mixed_lines = [], []
+    out, mixed_lines, engine_res = [], [], {}
     d1 = torch.tensor(pts1, device=dev)
-    t, _ = timed(lambda: pot1.eval(d1, pot=True, acc=True), 3, 10)
+    t, (phi1, acc1) = timed(lambda: pot1.eval(d1, pot=True, acc=True), 3, 10)
+    engine_res["forces1"] = (phi1.cpu().numpy(), acc1.cpu().numpy())
     out.append({"metric": "force evals/s", "value": len(pts1) / (t / 1000), "unit": "evals/s", "ms_per_step": t,
                 "config": "config 1: 1e5 points, triaxial Dehnen Multipole lmax 6 / 50 nodes, potential + force",
-                "steps": 10, "warmup": 3, "gpu_launches_per_step": 1})
-    for name, pot, ic, T, Om, mx, warm, steps in (
-            ("config 1: 1e4 orbits x 10 T_circ, DOP853 1e-8", pot1, ic1, T1, 0.0, 0, 3, 5),
-            ("config 3: %d of the 1e5 orbits (10-1000 T_circ, Omega 0.05), DOP853 1e-8, at most %d steps per orbit"
-             % (ORBIT3_ORBITS, ORBIT3_MAX_STEPS), pot3, ic3, T3, 0.05, ORBIT3_MAX_STEPS, 1, 2)):
+                "steps": 10, "warmup": 3, "gpu_launches_per_step": 1,
+                "roofline": fp64_roofline("evalPotentialKernel", FLOPS["forces1"], "evaluation", len(pts1), t, peak64,
+                                          FLOPS_SOURCE)})
+    for key, name, pot, ic, T, Om, mx, warm, steps in (
+            ("orbits1", "config 1: 1e4 orbits x 10 T_circ, DOP853 1e-8", pot1, ic1, T1, 0.0, 0, 3, 5),
+            ("orbits3", "config 3: all 1e5 orbits (10-1000 T_circ, Omega 0.05), DOP853 1e-8, at most %d steps per orbit"
+             % ORBIT3_MAX_STEPS, pot3, ic3, T3, 0.05, ORBIT3_MAX_STEPS, 1, 2)):
         dic, dT = torch.tensor(ic, device=dev), torch.tensor(T, device=dev)
         # the batch is captured once in a CUDA graph (work-counter reset + persistent kernel, lanes
         # per orbit chosen by the autotuner before the capture) and replayed every step
         graph = agama_b200.OrbitGraph(pot, dic, dT, Omega=Om, maxNumSteps=mx)
         t, _ = timed(graph.launch, warm, steps)
         nst, nrej = int(graph.steps.sum().item()), int(graph.rejected.sum().item())
-        out.append({"metric": "orbit-steps/s", "value": nst / (t / 1000), "unit": "accepted DOP853 steps/s",
-                    "ms_per_step": t, "config": name, "steps": steps, "warmup": warm, "accepted_steps": nst,
-                    "rejected_attempts": nrej, "gpu_launches_per_step": 1, "launch": "CUDA graph",
-                    "lanes_per_orbit": graph.lanes})
+        status = graph.status.cpu().numpy()
+        k = REF_SAMPLE[key]
+        engine_res[key] = (graph.final[:k].cpu().numpy(), status[:k])
+        line = {"metric": "orbit-steps/s", "value": nst / (t / 1000), "unit": "accepted DOP853 steps/s",
+                "ms_per_step": t, "config": name, "steps": steps, "warmup": warm, "accepted_steps": nst,
+                "rejected_attempts": nrej, "gpu_launches_per_step": 1, "launch": "CUDA graph",
+                "lanes_per_orbit": graph.lanes,
+                "roofline": fp64_roofline("dop853Kernel", FLOPS[key], "accepted step", nst, t, peak64, FLOPS_SOURCE)}
+        if mx:
+            line["orbits_at_step_cap"] = float(np.mean(status == 1))
+        out.append(line)
         mixed_lines.append(mixed_orbit_entry(agama_b200, timed, pot, dic, dT, Om, mx, warm, steps, name, graph, t))
         del graph
-    # config 5: orbits, then the actions of the final snapshot
-    from agama_b200 import workloads
+    # config 5: all 1e6 orbits, then the actions of the final snapshot (plain and learned brackets)
     pot5 = Pot(os.path.join(GOLDEN, "cfg5.coef"))
     ic5, T5 = workloads.orbit_workload(5, pot5.potential, pot5.force, ORBIT5_ORBITS)
     dic5, dT5 = torch.tensor(ic5, device=dev), torch.tensor(T5, device=dev)
     graph5 = agama_b200.OrbitGraph(pot5, dic5, dT5)
-    t5, _ = timed(graph5.launch, 1, 1)
+    t5, _ = timed(graph5.launch, 1, 2)
     nst5 = int(graph5.steps.sum().item())
+    engine_res["orbits5"] = (graph5.final[:REF_SAMPLE["orbits5"]].cpu().numpy(),
+                             graph5.status[:REF_SAMPLE["orbits5"]].cpu().numpy())
     af5 = agama_b200.ActionFinder(pot5)
     snap = graph5.final.clone()
-    ta, _ = timed(lambda: af5(snap), 3, 5)
+    ta, J5 = timed(lambda: af5(snap), 3, 5)
+    J5 = J5.clone()
+    engine_res["actions5"] = (snap[:REF_SAMPLE["actions5"]].cpu().numpy(), J5[:REF_SAMPLE["actions5"]].cpu().numpy())
     out.append({"metric": "orbit-steps/s", "value": nst5 / (t5 / 1000), "unit": "accepted DOP853 steps/s",
-                "ms_per_step": t5, "config": "config 5: %d of the 1e6 orbits x 100 T_circ, Spheroid + disk Multipole "
-                "lmax 12 / 80 nodes, DOP853 1e-8" % ORBIT5_ORBITS, "steps": 1, "warmup": 1, "accepted_steps": nst5,
-                "gpu_launches_per_step": 1, "launch": "CUDA graph", "lanes_per_orbit": graph5.lanes})
-    out.append({"metric": "actions/s", "value": ORBIT5_ORBITS / (ta / 1000), "unit": "actions/s", "ms_per_step": ta,
-                "config": "config 5: actions of the final snapshot of those orbits (action finder, FP64)",
-                "steps": 5, "warmup": 3, "gpu_launches_per_step": 3})
+                "ms_per_step": t5, "config": "config 5: all %d orbits x 100 T_circ, Spheroid + disk Multipole "
+                "lmax 12 / 80 nodes, DOP853 1e-8 (FP64: one harmonic, so the FP32 m != 0 mode has nothing to do)"
+                % ORBIT5_ORBITS, "steps": 2, "warmup": 1, "accepted_steps": nst5,
+                "gpu_launches_per_step": 1, "launch": "CUDA graph", "lanes_per_orbit": graph5.lanes,
+                "roofline": fp64_roofline("dop853Kernel", FLOPS["orbits5"], "accepted step", nst5, t5, peak64,
+                                          FLOPS_SOURCE)})
+    line5 = {"metric": "actions/s", "value": ORBIT5_ORBITS / (ta / 1000), "unit": "actions/s", "ms_per_step": ta,
+             "config": "config 5: actions of the final snapshot of those orbits (action finder, plain FP64)",
+             "steps": 5, "warmup": 3, "gpu_launches_per_step": 3,
+             "roofline": fp64_roofline("fudge kernels (3)", FLOPS["actions5"], "action", ORBIT5_ORBITS, ta, peak64,
+                                       FLOPS_SOURCE)}
+    out.append(line5)
+    # learned brackets on the snapshot: the network trained on the orbits' initial points (the same
+    # distribution, other points), then used on the final points
+    t0 = time.perf_counter()
+    af5.train_brackets(ic5[:1000000], epochs=20, batch=2048, lr=2e-3, seed=1)
+    ttrain5 = time.perf_counter() - t0
+    af5.use_brackets(True)
+    tl, J5l = timed(lambda: af5(snap), 3, 5)
+    af5.bracket_stats(reset=True)
+    J5l = af5(snap)
+    st5 = af5.bracket_stats(reset=True)
+    af5.use_brackets(False)
+    out.append({"metric": "actions/s", "mode": "learned root brackets (BF16 tcgen05 network + FP64 searches)",
+                "value": ORBIT5_ORBITS / (tl / 1000), "unit": "actions/s", "ms_per_step": tl,
+                "config": "config 5: actions of the final snapshot, learned root brackets",
+                "plain_fp64": {"value": ORBIT5_ORBITS / (ta / 1000), "ms_per_step": ta}, "speedup_vs_plain": ta / tl,
+                "max_rel_err_vs_plain": rel_action_err(J5l.cpu().numpy(), J5.cpu().numpy())["max"],
+                "seeded_searches": st5["narrowed"] / max(1, st5["searches"]),
+                "fallback_rate": st5["fallbacks"] / max(1, st5["narrowed"]),
+                "training": {"samples": 1000000, "epochs": 20, "seconds": ttrain5, "points": "the orbits' initial points"},
+                "steps": 5, "warmup": 3, "gpu_launches_per_step": 4})
     del graph5
     if cpu:
-        for line, base in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5)):
+        for line, (base, parity) in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5, engine_res)):
             line["cpu_baseline"] = base
+            if parity is not None:
+                line["max_rel_err_vs_reference" if "max" in parity else "vs_reference"] = parity
     return out + mixed_lines
 
 
@@ -415,45 +513,61 @@ def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
     return out
 
 
-def reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5):
-    """the reference's own CPU code on bounded samples of the secondary workloads, all host cores"""
+def reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5, engine=None):
+    """the reference's own CPU code on bounded samples of the secondary workloads, all host cores:
+    (cpu_baseline, parity against the engine's results on the same sample) per workload, in the
+    order forces, config-1 orbits, config-3 orbits, config-5 orbits, config-5 snapshot actions"""
     try:
         from oracle import ref
         if not ref.available():
-            return [None] * 5
-        cores = os.cpu_count()
+            return [(None, None)] * 5
+        cores, model = os.cpu_count(), cpu_model()
+        base = lambda v, unit, sample: {"value": v, "unit": unit, "cores": cores, "cpu_model": model,
+                                        "kind": "reference", "sample": sample}
         p1 = ref.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
         p3 = ref.Potential(file=os.path.join(GOLDEN, "cfg3.coef"))
         res = []
         p1.eval(pts1[:1000], nthreads=cores)
         t0 = time.perf_counter()
-        p1.eval(pts1, nthreads=cores)
+        phi, grad, _ = p1.eval(pts1, nthreads=cores)
         dt = time.perf_counter() - t0
-        res.append({"value": len(pts1) / dt, "unit": "evals/s", "cores": cores, "kind": "reference",
-                    "sample": "all 1e5 config-1 points, potential + force, OpenMP"})
-        for ic, T, Om, mx, n, what in ((ic1, T1, 0.0, 0, 2000, "config 1"),
-                                       (ic3, T3, 0.05, ORBIT3_MAX_STEPS, 400, "config 3")):
+        parity = None
+        if engine is not None:
+            ephi, eacc = engine["forces1"]
+            parity = {"max": float(max(np.max(np.abs(ephi - phi) / np.abs(phi)),
+                                       np.max(np.linalg.norm(-eacc - grad, axis=1) / np.linalg.norm(grad, axis=1)))),
+                      "of": "potential and force, relative", "points": len(pts1)}
+        res.append((base(len(pts1) / dt, "evals/s", "all 1e5 config-1 points, potential + force, OpenMP"), parity))
+        for key, pot, ic, T, Om, mx, what in (("orbits1", p1, ic1, T1, 0.0, 0, "config 1"),
+                                              ("orbits3", p3, ic3, T3, 0.05, ORBIT3_MAX_STEPS, "config 3")):
+            n = REF_SAMPLE[key]
             t0 = time.perf_counter()
-            _, steps, _ = p1.orbits(ic[:n], T[:n], Omega=Om, maxSteps=mx, nthreads=cores) if what == "config 1" else \
-                p3.orbits(ic[:n], T[:n], Omega=Om, maxSteps=mx, nthreads=cores)
+            fin, steps, status = pot.orbits(ic[:n], T[:n], Omega=Om, maxSteps=mx, nthreads=cores)
             dt = time.perf_counter() - t0
-            res.append({"value": float(steps.sum()) / dt, "unit": "accepted DOP853 steps/s", "cores": cores,
-                        "kind": "reference", "sample": "first %d orbits of the %s workload, OpenMP dynamic 1" % (n, what)})
+            parity = orbit_deviation(*engine[key], fin, status) if engine is not None else None
+            res.append((base(float(steps.sum()) / dt, "accepted DOP853 steps/s",
+                             "first %d orbits of the %s workload, OpenMP dynamic 1" % (n, what)), parity))
         p5 = ref.Potential(file=os.path.join(GOLDEN, "cfg5.coef"))
+        n = REF_SAMPLE["orbits5"]
         t0 = time.perf_counter()
-        fin5, steps5, _ = p5.orbits(ic5[:200], T5[:200], nthreads=cores)
+        fin5, steps5, status5 = p5.orbits(ic5[:n], T5[:n], nthreads=cores)
         dt = time.perf_counter() - t0
-        res.append({"value": float(steps5.sum()) / dt, "unit": "accepted DOP853 steps/s", "cores": cores,
-                    "kind": "reference", "sample": "first 200 orbits of the config 5 workload, OpenMP dynamic 1"})
+        parity = orbit_deviation(*engine["orbits5"], fin5, status5) if engine is not None else None
+        res.append((base(float(steps5.sum()) / dt, "accepted DOP853 steps/s",
+                         "first %d orbits of the config 5 workload, OpenMP dynamic 1" % n), parity))
         af5 = ref.ActionFinder(p5)
+        # the actions of the engine's own snapshot points (the same inputs on both sides), or of the
+        # reference's final points when there is no engine run (reference arm)
+        pts = engine["actions5"][0] if engine is not None else fin5
         t0 = time.perf_counter()
-        af5.actions(fin5, nthreads=cores)
+        J = af5.actions(pts, nthreads=cores)
         dt = time.perf_counter() - t0
-        res.append({"value": len(fin5) / dt, "unit": "actions/s", "cores": cores, "kind": "reference",
-                    "sample": "actions of those 200 final points, reference ActionFinderAxisymFudge, OpenMP"})
+        parity = rel_action_err(engine["actions5"][1], J) if engine is not None else None
+        res.append((base(len(pts) / dt, "actions/s", "actions of %d final points of the config-5 orbits, reference "
+                         "ActionFinderAxisymFudge, OpenMP" % len(pts)), parity))
         return res
     except Exception as e:   # the baseline is reported, never required
-        return [{"value": None, "kind": "reference", "sample": "failed: %s" % e}] * 5
+        return [({"value": None, "kind": "reference", "sample": "failed: %s" % e}, None)] * 5
 
 
 def run_engine(args):
@@ -529,12 +643,12 @@ def run_engine(args):
         e2e_times.append(time.perf_counter() - t0)
     e2e_ms = 1000 * float(np.mean(e2e_times))
     e2e_val = n * world / (max_over_ranks(e2e_ms, dist, dev) / 1000)
+    pk = ctypes.c_double(0)
+    _native.check(lib.agama_measureFP64Throughput(ctypes.byref(pk)))
     if rank == 0:
         # ---- roofline (FP64-pipe bound): the dominant kernel (root searches), timed by CUDA events
         # around it during the timed steps, and the whole three-kernel step; executed FP64 flops
         # per action from an ncu capture of this workload; peak measured on this device
-        pk = ctypes.c_double(0)
-        _native.check(lib.agama_measureFP64Throughput(ctypes.byref(pk)))
         achieved = FLOPS_ROOT_PER_ACTION_CFG2 * n / (phase_ms[2] / 1000) / 1e12
         step_achieved = FLOPS_PER_ACTION_CFG2 * n / (ms_per_step / 1000) / 1e12
         line = {
@@ -557,9 +671,10 @@ def run_engine(args):
                                   "phase_ms": {"prepare": phase_ms[0], "roots": phase_ms[2],
                                                "integrals": phase_ms[3]}}},
             "clocks": clocks,
-            "cpu_baseline": None if args.no_baseline else cpu_baseline_line(pts),
+            "cpu_baseline": None if args.no_baseline else cpu_baseline_line(pts, act.cpu().numpy()),
         }
-    secondary = None if args.no_secondary else run_engine_secondary(dev, flush, dist, rank == 0 and not args.no_baseline)
+    secondary = None if args.no_secondary else run_engine_secondary(dev, flush, dist, rank == 0 and not args.no_baseline,
+                                                                    pk.value)
     if not args.no_secondary:
         secondary += run_bracket_modes(dev, flush, dist, af, dpts, act.clone())
     if rank == 0:
@@ -581,6 +696,10 @@ FLOPS_PER_ACTION_CFG2 = 3880.0 + 11014.0 + 9687.0
 # integrals 26.01 + 0.00 MB), scaled to 1e6 particles (the traffic grows with the particles)
 TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 61.37e6
 TRAFFIC_PER_STEP_CFG2 = 5 * 103.02e6
+# executed FP64 flops (dadd + dmul + 2 dfma, ncu) per unit of the secondary workloads: per force
+# evaluation, per accepted DOP853 step (the rejected attempts' work included), per action
+FLOPS = {"forces1": None, "orbits1": None, "orbits3": None, "orbits5": None, "actions5": None}
+FLOPS_SOURCE = "ncu FP64 instruction counts of the kernel on a case of this workload (bench.py --profile-case)"
 
 
 def ctypes_stream(stream):
@@ -588,8 +707,45 @@ def ctypes_stream(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
+def run_profile_case():
+    """one launch of each workload's kernels on a small case, in a fixed order, with the units
+    each launch processed (force evaluations, accepted steps, actions) printed as one JSON line:
+    the ncu instruction counts of these launches divided by these units give the FLOPS table.
+    Lanes per orbit are fixed to 1 (the autotuner's trial would add launches of its own)."""
+    import torch
+    import agama_b200
+    from agama_b200 import workloads
+    dev = torch.device("cuda", 0)
+    agama_b200.set_orbit_lanes(1)
+    units = {}
+    pot1 = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+    pts1 = workloads.dehnen_positions(100000, 1.0, q=(0.8, 0.6), seed=workloads.SEEDS["points1"])
+    d1 = torch.tensor(pts1, device=dev)
+    pot1.eval(d1, pot=True, acc=True)
+    torch.cuda.synchronize()
+    units["forces1"] = len(pts1)
+    for key, coef, cfg, n, Om, mx in (("orbits1", "cfg1", 1, 10000, 0.0, 0), ("orbits3", "cfg3", 3, 20000, 0.05, 500),
+                                      ("orbits5", "cfg5", 5, 20000, 0.0, 0)):
+        pot = pot1 if coef == "cfg1" else agama_b200.Potential(file=os.path.join(GOLDEN, coef + ".coef"))
+        ic, T = workloads.orbit_workload(cfg, pot.potential, pot.force, n)
+        fin, info = agama_b200.orbit(pot, torch.tensor(ic, device=dev), torch.tensor(T, device=dev), Omega=Om,
+                                     maxNumSteps=mx, queue=True, info=True)
+        torch.cuda.synchronize()
+        units[key] = int(info["steps"].sum().item())
+        if key == "orbits5":
+            af5 = agama_b200.ActionFinder(pot)
+            af5(fin)
+            torch.cuda.synchronize()
+            units["actions5"] = n
+    agama_b200.set_orbit_lanes(0)
+    print(json.dumps({"profile_case_units": units, "order": ["forces1", "orbits1", "orbits3", "orbits5", "actions5"]}))
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        run_profile_case()
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -207,7 +207,10 @@ int agama_integrateOrbitsManyDevice(const agama_Potential* potential, long n, co
    before the launch; the array keeps the last call's values.  Calls that overlap on the GPU and
    use the same slot race (orbits may be skipped or integrated twice): give batches that may run
    at the same time different slots.  The first call on each device looks up the array's device
-   address (cudaGetSymbolAddress) -- make that first call before any stream capture. */
+   address (cudaGetSymbolAddress) -- make that first call before any stream capture.
+   It always integrates in FP64 with one lane per orbit: agama_setOrbitPrecision and
+   agama_setOrbitLanesPerOrbit do not apply to it (with mixed precision switched on, its results
+   are those of the FP64 batch, not those of agama_integrateOrbitsManyDevice). */
 int agama_integrateOrbitsManyDeviceNoAlloc(const agama_Potential* potential, long n, const double* ic,
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, long* numRejected, int* status, int queueSlot, void* stream);

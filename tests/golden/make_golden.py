@@ -10,7 +10,8 @@ It writes, into tests/golden/:
   potential_<name>.npz   evaluation points (incl. edge cases) with the reference's potential,
                          gradient and Hessian at them;
   orbits_<name>.npz      initial conditions, integration times and the reference's final
-                         phase-space points, accepted step counts and statuses;
+                         phase-space points, accepted step counts and statuses (configs 1, 3 and 5,
+                         the general-kind potential 'lop', long config-3 times 'cfg3long');
   actions_<name>.npz     phase-space points with the reference's Staeckel-fudge actions (fixed
                          focal distance and through ActionFinderAxisymFudge), plus the finder's
                          focal-distance table and L_circ(E) spline;
@@ -159,6 +160,48 @@ def make_orbit_vectors():
     print("cfg3 orbits", len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max())
 
 
+def make_more_orbit_vectors():
+    """orbit sets for the other evaluator kinds and the long config-3 times:
+    orbits_cfg5.npz  the axisymmetric kind (lmax 12, one harmonic): 192 orbits of the config-5
+                     workload, T = 100 T_circ(E);
+    orbits_lop.npz   the general kind (11 harmonics, m < 0 terms, no symmetry): 48 orbits,
+                     T = 10 T_circ(E);
+    orbits_cfg3long.npz  480 orbits of the config-3 distribution with T = T_circ(E) 10^U[1, 3]
+                     (10-1000 dynamical times) in the frame rotating at Omega = 0.05; only the
+                     orbits that the reference finishes within MAX_STEPS_LONG accepted steps are kept
+                     (the rest of the workload's tail needs up to 1e7 steps per orbit)."""
+    MAX_STEPS_LONG = 40000
+    for name, n, scale_fn, Omega in (("cfg5", 192, None, 0.0), ("lop", 48, None, 0.0), ("cfg3", 480, None, 0.05)):
+        coef = coef_path(name)
+        pot = ref.Potential(file=coef)
+        potential_fn = lambda p: pot.eval(p)[0]
+        force_fn = lambda p: -pot.eval(p)[1]
+        if name == "cfg5":
+            ic, T = workloads.orbit_workload(5, potential_fn, force_fn, n)
+        elif name == "cfg3":
+            ic, T = workloads.orbit_workload(3, potential_fn, force_fn, n)
+        else:
+            x = workloads.dehnen_positions(n, gamma=1, q=(0.8, 0.6), seed=707)
+            ic = workloads.orbit_ics(x, potential_fn, seed=708)
+            E = potential_fn(ic[:, :3]) + 0.5 * np.sum(ic[:, 3:] ** 2, axis=1)
+            T = 10 * workloads.tcirc(potential_fn, force_fn, E)
+        mx = MAX_STEPS_LONG if name == "cfg3" else 0
+        final, steps, status = pot.orbits(ic, T, Omega=Omega, accuracy=1e-8, maxSteps=mx)
+        if name == "cfg3":
+            keep = status == 0
+            ic, T, final, steps, status = ic[keep], T[keep], final[keep], steps[keep], status[keep]
+        f1, _, _ = pot.orbits(ic * (1 + 1e-12), T, Omega=Omega, accuracy=1e-8, maxSteps=mx)
+        d = np.max(np.abs(f1 - final) / np.maximum(np.abs(final), 1e-300), axis=1)
+        sc = np.linalg.norm(f1[:, :3] - final[:, :3], axis=1) / np.linalg.norm(final[:, :3], axis=1)
+        regular = (sc < 1e-9) & (d < 1e-6)
+        fname = "orbits_%s.npz" % ("cfg3long" if name == "cfg3" else name)
+        np.savez_compressed(os.path.join(HERE, fname), ic=ic, T=T, Omega=Omega, accuracy=1e-8,
+                            final=final, steps=steps, status=status, regular=regular)
+        print(fname, len(ic), "regular", regular.sum(), "steps", steps.min(), steps.max(),
+              "T/T_circ max", "%.0f" % (T / workloads.tcirc(potential_fn, force_fn,
+                                                            potential_fn(ic[:, :3]) + 0.5 * np.sum(ic[:, 3:] ** 2, 1))).max())
+
+
 def action_points(pot, n, seed, Rd=3.0, hz=0.3):
     """disk-like points of the benchmark distribution plus edge cases: in the plane (z = 0),
     no rotation (Lz = 0), counter-rotating, nearly circular, on the z axis, unbound"""
@@ -238,6 +281,8 @@ if __name__ == "__main__":
         make_potential_vectors()
     if what in ("orbits", "all"):
         make_orbit_vectors()
+    if what in ("orbits", "more_orbits", "all"):
+        make_more_orbit_vectors()
     if what in ("actions", "all"):
         make_action_vectors()
     if what in ("utils", "all"):

@@ -42,6 +42,20 @@ def test_reference_orbits_reproduce_golden():
 
 
 @needs_ref
+@pytest.mark.parametrize("name", ["cfg5", "lop", "cfg3long"])
+def test_reference_orbit_sets_reproduce_golden(name):
+    """the axisymmetric (config 5), general-kind and long config-3 orbit sets"""
+    g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % name))
+    pot = ref.Potential(file=os.path.join(GOLDEN, name.replace("long", "") + ".coef"))
+    k = np.arange(0, len(g["ic"]), max(1, len(g["ic"]) // 6))[:6]
+    final, steps, status = pot.orbits(g["ic"][k], g["T"][k], Omega=float(g["Omega"]),
+                                      accuracy=float(g["accuracy"]), nthreads=1)
+    np.testing.assert_array_equal(final, g["final"][k])
+    np.testing.assert_array_equal(steps, g["steps"][k])
+    np.testing.assert_array_equal(status, g["status"][k])
+
+
+@needs_ref
 def test_reference_rotating_frame_and_trajectories_reproduce_golden():
     g = np.load(os.path.join(GOLDEN, "orbits_cfg3.npz"))
     pot = ref.Potential(file=os.path.join(GOLDEN, "cfg3.coef"))

@@ -28,17 +28,36 @@ def rel_vec(a, b):
     return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)
 
 
-@pytest.mark.parametrize("cfg", ["cfg1", "cfg3"])
-@pytest.mark.parametrize("queue,lanes", [(True, 0), (False, 1), (True, 1), (True, 2), (True, 4), (True, 8), (False, 4)])
+# orbit sets and the evaluator kind of their potential: cfg1, cfg3 (triaxial, <= 8 harmonics in
+# registers), cfg3long (config 3 with 10-1000 dynamical times), cfg5 (axisymmetric, lmax 12),
+# lop (11 harmonics incl. m < 0: the general kind)
+ORBIT_SETS = ["cfg1", "cfg3", "cfg3long", "cfg5", "lop"]
+LANE_CASES = [(True, 0), (False, 1), (True, 1), (True, 2), (True, 4), (True, 8), (False, 4)]
+
+
+def _orbit_cases():
+    for cfg in ORBIT_SETS:
+        for queue, lanes in LANE_CASES:
+            # lane groups serve the multi-harmonic kind only: the other sets run the queue and the
+            # one-orbit-per-thread mappings
+            if cfg in ("cfg5", "lop") and lanes not in (0, 1):
+                continue
+            yield cfg, queue, lanes
+
+
+@pytest.mark.parametrize("cfg,queue,lanes", list(_orbit_cases()))
 def test_orbit_parity(cfg, queue, lanes):
     """lanes: lanes of a warp per orbit (0: the autotuner's choice)"""
     import agama_b200
-    agama_b200.set_orbit_lanes(lanes)
     g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % cfg))
-    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg.replace("long", "") + ".coef"))
     Omega = float(g["Omega"])
-    final, info = agama_b200.orbit(pot, g["ic"], g["T"], Omega=Omega, accuracy=float(g["accuracy"]),
-                                   queue=queue, info=True)
+    agama_b200.set_orbit_lanes(lanes)
+    try:
+        final, info = agama_b200.orbit(pot, g["ic"], g["T"], Omega=Omega, accuracy=float(g["accuracy"]),
+                                       queue=queue, info=True)
+    finally:
+        agama_b200.set_orbit_lanes(0)
     reg = g["regular"] & (g["status"] == 0)
     assert np.all(info["status"] == g["status"])
     epos = rel_vec(final[reg, :3], g["final"][reg, :3])
@@ -52,7 +71,26 @@ def test_orbit_parity(cfg, queue, lanes):
     drift_ref = np.abs(jacobi_energy(pot, g["final"], Omega) / E0 - 1)
     ok = g["status"] == 0
     assert np.all(drift[ok] <= np.maximum(10 * drift_ref[ok], 1e-9)), (drift[ok].max(), drift_ref[ok].max())
-    agama_b200.set_orbit_lanes(0)
+
+
+@pytest.mark.parametrize("cfg", ["cfg1", "cfg3"])
+def test_orbit_bits_independent_of_lanes(cfg):
+    """every lane count gives the same bits (the harmonics of a lane group are summed in one
+    order), so the autotuner's timing-based choice never changes a result"""
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % cfg))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    results = []
+    for lanes in (1, 2, 4, 8):
+        agama_b200.set_orbit_lanes(lanes)
+        try:
+            results.append(agama_b200.orbit(pot, g["ic"], g["T"], Omega=float(g["Omega"]),
+                                            accuracy=float(g["accuracy"]), info=True))
+        finally:
+            agama_b200.set_orbit_lanes(0)
+    for final, info in results[1:]:
+        assert np.array_equal(final, results[0][0])
+        assert np.array_equal(info["steps"], results[0][1]["steps"])
 
 
 def test_orbit_edge_cases():

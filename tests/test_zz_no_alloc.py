@@ -6,9 +6,12 @@ synchronise the device, plugin hosts that account for all device memory).  Its w
 sits in a static device array of 32 slots instead of a per-call allocation.
 
 Checked here, through the C-ABI: two calls in a row give the same final points, step counts and
-statuses as the allocating entry point (agama_integrateOrbitsManyDevice with the work queue),
-within the orbit tests' bound of 1e-7 (the second call shows that the counter is cleared between
-calls), and an out-of-range slot is rejected with an error.  This file is collected last.
+statuses as the allocating entry point (agama_integrateOrbitsManyDevice with the work queue, one
+lane per orbit as the allocation-free call uses), within the orbit tests' bound of 1e-7 (the second
+call shows that the counter is cleared between calls); the device's free memory is the same before
+and after a call (nothing was allocated; the first call may load the kernel's code, so this is
+checked on the second); an out-of-range slot is rejected with an error.  This file is collected
+last.
 """
 import ctypes
 import os
@@ -21,16 +24,20 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 
-def _run(entry, pot, ic, T, slot=None):
+def _buffers(ic):
+    import torch
+    n = ic.shape[0]
+    return (torch.empty_like(ic), torch.empty(n, dtype=torch.int64, device=ic.device),
+            torch.empty(n, dtype=torch.int64, device=ic.device), torch.empty(n, dtype=torch.int32, device=ic.device))
+
+
+def _run(pot, ic, T, bufs, slot=None):
+    """one batch through the C-ABI into preallocated buffers; slot None: the allocating entry point"""
     import torch
     from agama_b200 import _native, _dev_ptr
-    n = ic.shape[0]
-    out = torch.empty_like(ic)
-    steps = torch.empty(n, dtype=torch.int64, device=ic.device)
-    rej = torch.empty(n, dtype=torch.int64, device=ic.device)
-    st = torch.empty(n, dtype=torch.int32, device=ic.device)
+    out, steps, rej, st = bufs
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    args = [pot.handle, n, _dev_ptr(ic), _dev_ptr(T), 0.0, 1e-8, 0, _dev_ptr(out), _dev_ptr(steps),
+    args = [pot.handle, ic.shape[0], _dev_ptr(ic), _dev_ptr(T), 0.0, 1e-8, 0, _dev_ptr(out), _dev_ptr(steps),
             _dev_ptr(rej), _dev_ptr(st)]
     lib = _native.lib()
     if slot is None:
@@ -39,7 +46,10 @@ def _run(entry, pot, ic, T, slot=None):
         rc = lib.agama_integrateOrbitsManyDeviceNoAlloc(*args, slot, stream)
     assert rc == 0, _native.error()
     torch.cuda.synchronize()
-    return out.cpu().numpy(), steps.cpu().numpy(), rej.cpu().numpy(), st.cpu().numpy()
+
+
+def _host(bufs):
+    return tuple(b.cpu().numpy() for b in bufs)
 
 
 def test_no_alloc_orbits_match_allocating_entry_point():
@@ -49,9 +59,23 @@ def test_no_alloc_orbits_match_allocating_entry_point():
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
     ic = torch.tensor(g["ic"], device="cuda")
     T = torch.tensor(g["T"], device="cuda")
-    ref_out, ref_steps, ref_rej, ref_st = _run("alloc", pot, ic, T)
+    ref_bufs = _buffers(ic)
+    agama_b200.set_orbit_lanes(1)          # the allocation-free call runs one lane per orbit
+    try:
+        _run(pot, ic, T, ref_bufs)
+    finally:
+        agama_b200.set_orbit_lanes(0)
+    ref_out, ref_steps, ref_rej, ref_st = _host(ref_bufs)
+    bufs = _buffers(ic)
     for call in range(2):          # two calls in a row: the shared counter must be cleared each time
-        out, steps, rej, st = _run("noalloc", pot, ic, T, slot=3)
+        bufs[0].fill_(np.nan)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        _run(pot, ic, T, bufs, slot=3)
+        free_after = torch.cuda.mem_get_info()[0]
+        if call == 1:
+            assert free_after == free_before, (free_before, free_after)
+        out, steps, rej, st = _host(bufs)
         scale = np.maximum(np.linalg.norm(ref_out[:, :3], axis=1), 1e-300)
         assert np.all(np.linalg.norm(out[:, :3] - ref_out[:, :3], axis=1) <= 1e-7 * scale), call
         vscale = np.maximum(np.linalg.norm(ref_out[:, 3:], axis=1), 1e-300)
