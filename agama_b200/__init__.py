@@ -107,6 +107,12 @@ class Potential:
         lmax, mmax, sym, nr, nt = (x.value for x in v)
         return dict(lmax=lmax, mmax=mmax, symmetry=sym, gridSizeR=nr, gridSizeTau=nt)
 
+    def export(self, file):
+        """write the coefficient file of this potential (the reference's Potential.export /
+        writePotential text format, numbers with 17 significant digits), readable by the reference
+        and by Potential(file=...)"""
+        check(_native.lib().agama_writePotential(str(file).encode(), self._h))
+
     # ---------------- evaluation ----------------
     def eval(self, points, pot=True, acc=False, der=False):
         """Potential, acceleration (-grad Phi) and/or Hessian (xx,yy,zz,xy,yz,zx) at points."""
@@ -208,7 +214,7 @@ class Potential:
         return self._radii(3, EL[:, 0], EL[:, 1])
 
 
-from .actions import ActionFinder, actions  # noqa: E402,F401
-from .orbit import (orbit, set_orbit_lanes, set_orbit_precision, jacobi_energy_error,  # noqa: E402,F401
+from .actions import ActionFinder, actions, set_action_precision  # noqa: E402,F401
+from .orbit import (orbit, orbit_target, Target, set_orbit_lanes, set_orbit_block, set_orbit_precision, jacobi_energy_error,  # noqa: E402,F401
                     trajectory, OrbitGraph)
 from .mlp import BracketNet  # noqa: E402,F401

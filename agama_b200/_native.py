@@ -24,6 +24,8 @@ SIGNATURES = {
     "agama_createMultipoleFromCoefs": (VP, [ctypes.c_int, D, ctypes.c_int, D, D]),
     "agama_getPotentialInfo": (ctypes.c_int, [VP, I, I, I, I, I]),
     "agama_inspectMultipoleFile": (ctypes.c_int, [ctypes.c_char_p, I, I, I, I, I]),
+    "agama_writePotential": (ctypes.c_int, [ctypes.c_char_p, VP]),
+    "agama_writeMultipoleCoefs": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, D, ctypes.c_int, D, D]),
     "agama_evalPotentialMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
     "agama_evalPotentialManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
     "agama_createDensity": (VP, [ctypes.c_char_p]),
@@ -38,16 +40,27 @@ SIGNATURES = {
     "agama_potentialRadiiMany": (ctypes.c_int, [VP, ctypes.c_int, ctypes.c_long, D, D, D, D]),
     "agama_potentialRadiiManyDevice": (ctypes.c_int, [VP, ctypes.c_int, ctypes.c_long, VP, VP, VP, VP, VP]),
     "agama_setOrbitLanesPerOrbit": (ctypes.c_int, [ctypes.c_int]),
+    "agama_setOrbitBlockSize": (ctypes.c_int, [ctypes.c_int]),
+    "agama_setActionPrecision": (ctypes.c_int, [ctypes.c_int]),
     "agama_setOrbitPrecision": (ctypes.c_int, [ctypes.c_int]),
     "agama_integrateOrbitsTrajectoryManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
                                                                  ctypes.c_double, ctypes.c_long, ctypes.c_int, VP, VP,
                                                                  VP, VP, VP]),
     "agama_integrateOrbitsTrajectoryMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
                                                            ctypes.c_long, ctypes.c_int, D, D, L, I]),
+    "agama_createTargetDensityClassic": (VP, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, ctypes.c_double,
+                                              ctypes.c_double]),
+    "agama_deleteTarget": (None, [VP]),
+    "agama_targetNumCoefs": (ctypes.c_int, [VP]),
+    "agama_integrateOrbitsTargetManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, ctypes.c_double,
+                                                             ctypes.c_double, ctypes.c_long, VP, VP, VP, VP, VP, VP]),
+    "agama_integrateOrbitsTargetMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
+                                                       ctypes.c_long, VP, F, D, L, I]),
     "agama_orbitGraphCreate": (VP, [VP, ctypes.c_long, VP, VP, ctypes.c_double, ctypes.c_double, ctypes.c_long,
                                     VP, VP, VP, VP]),
     "agama_orbitGraphLaunch": (ctypes.c_int, [VP, VP]),
     "agama_orbitGraphLanes": (ctypes.c_int, [VP]),
+    "agama_orbitGraphBlockSize": (ctypes.c_int, [VP]),
     "agama_orbitGraphDelete": (None, [VP]),
     "agama_integrateOrbitsMany": (ctypes.c_int, [VP, ctypes.c_long, D, D, ctypes.c_double, ctypes.c_double,
                                                  ctypes.c_long, D, L, I]),

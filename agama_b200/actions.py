@@ -217,3 +217,11 @@ def actions(potential, points, fd, iters=False, angles=False, frequencies=False)
         fda = np.ascontiguousarray(np.broadcast_to(np.asarray(fd, dtype=np.float64), (n,)))
         check(_native.lib().agama_evalActionsStandaloneMany(potential.handle, n, ptr(p), ptr(fda), 0.0, ptr(act)))
     return act[0] if single else act
+
+
+def set_action_precision(mixed=False):
+    """mixed=True: later action computations (without angles / frequencies) evaluate the action
+    integrands after F(tau) and their Gauss-Legendre sums in FP32 (compensated sums), with the
+    potential, F(tau), the integrals of motion and the root searches in FP64; False (the default):
+    everything in FP64"""
+    check(_native.lib().agama_setActionPrecision(1 if mixed else 0))

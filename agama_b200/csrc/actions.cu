@@ -2,6 +2,7 @@
 #include "runtime.h"
 #include <array>
 #include <mutex>
+#include <atomic>
 #include <vector>
 #include "fudge.cuh"
 #include "host_pipeline.h"
@@ -130,6 +131,9 @@ struct PhaseTimer {
 };
 PhaseTimer g_phaseTimer;
 
+/// mixed-precision action integrals in later calls (off by default)
+std::atomic<int> g_actionMixed{ 0 };
+
 /// events of one pass, or null when the timing is off
 std::array<cudaEvent_t, 5>* phaseEvents()
 {
@@ -194,12 +198,14 @@ void runActions(const MultipoleView& M, const FudgeTables& F, long n, const doub
             launchFudgeAngles(M, gl, count, rec, a, ang ? ang + 3 * first : nullptr,
                 freq ? freq + 3 * first : nullptr, stream);
         else
-            launchFudgeIntegrals(M, gl, count, rec, a, counter + 1, stream);
+            launchFudgeIntegrals(M, gl, count, rec, a, counter + 1, g_actionMixed != 0, stream);
         mark(4);
     }
 }
 
 }  // namespace
+
+void setActionMixedPrecision(bool mixed) { g_actionMixed = mixed ? 1 : 0; }
 
 void setActionPhaseTiming(bool on, double* ms, long* passes)
 {

@@ -287,6 +287,33 @@ extern "C" int agama_inspectMultipoleFile(const char* file, int* lmax, int* mmax
     });
 }
 
+extern "C" int agama_writePotential(const char* fileName, const agama_Potential* p)
+{
+    return guarded([&] {
+        if(!fileName || !p) throw std::invalid_argument("writePotential: invalid arguments");
+        const MultipoleHost& H = p->pot->host;
+        writeMultipoleCoefFile(fileName, H.radii, H.Phi, H.dPhi, H.ind.sym);
+    });
+}
+
+extern "C" int agama_writeMultipoleCoefs(const char* fileName, int gridSizeR, const double* radii, int numCoefs,
+    const double* Phi, const double* dPhi)
+{
+    // host-only: the tables are built to validate the coefficients and find their symmetry
+    return guarded([&] {
+        if(!fileName || gridSizeR < 2 || numCoefs < 1 || !radii || !Phi || !dPhi)
+            throw std::invalid_argument("writeMultipoleCoefs: invalid arguments");
+        std::vector<double> r(radii, radii + gridSizeR);
+        std::vector<std::vector<double>> P(numCoefs), D(numCoefs);
+        for(int c = 0; c < numCoefs; c++) {
+            P[c].assign(Phi + static_cast<size_t>(c) * gridSizeR, Phi + static_cast<size_t>(c + 1) * gridSizeR);
+            D[c].assign(dPhi + static_cast<size_t>(c) * gridSizeR, dPhi + static_cast<size_t>(c + 1) * gridSizeR);
+        }
+        const MultipoleHost H = buildMultipole(r, P, D);
+        writeMultipoleCoefFile(fileName, H.radii, H.Phi, H.dPhi, H.ind.sym);
+    });
+}
+
 // ------------------------------------------------------------------------------------------
 // orbits
 
@@ -311,6 +338,23 @@ extern "C" int agama_setOrbitLanesPerOrbit(int lanes)
         if(!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8))
             throw std::invalid_argument("setOrbitLanesPerOrbit: lanes must be 0 (autotuned), 1, 2, 4 or 8");
         setOrbitLanes(lanes);
+    });
+}
+
+extern "C" int agama_setActionPrecision(int mixed)
+{
+    return guarded([&] {
+        if(mixed != 0 && mixed != 1) throw std::invalid_argument("setActionPrecision: 0 (FP64) or 1 (mixed)");
+        setActionMixedPrecision(mixed == 1);
+    });
+}
+
+extern "C" int agama_setOrbitBlockSize(int block)
+{
+    return guarded([&] {
+        if(!(block == 0 || block == 32 || block == 64 || block == 128))
+            throw std::invalid_argument("setOrbitBlockSize: block must be 0 (autotuned), 32, 64 or 128");
+        setOrbitBlock(block);
     });
 }
 
@@ -384,6 +428,111 @@ extern "C" int agama_integrateOrbitsTrajectoryMany(const agama_Potential* p, lon
     });
 }
 
+// ---- orbits with a target (runtime function accumulating a density grid)
+
+struct agama_Target {
+    int degree = 0, strips = 0;
+    std::vector<double> shellRadii;
+    double axisX = 1, axisY = 1, axisZ = 1;
+    int valuesPerShell = 0, numValues = 0;
+};
+
+extern "C" agama_Target* agama_createTargetDensityClassic(int degree, int stripsPerPane, int gridSize,
+    const double* gridr, double axisRatioY, double axisRatioZ)
+{
+    try {
+        if(degree != 0 && degree != 1) throw std::invalid_argument("createTargetDensityClassic: degree must be 0 or 1");
+        if(gridSize < 1 || !gridr) throw std::invalid_argument("createTargetDensityClassic: no radial grid");
+        agama_Target* T = new agama_Target;
+        T->degree = degree;
+        T->strips = stripsPerPane;
+        // TargetDensityClassic constructor (src/galaxymodel_densitygrid.cpp:149-167): a leading
+        // zero node is implied and dropped; the axes keep the volume (axisX axisY axisZ = 1)
+        const int first = gridr[0] > 0 ? 0 : 1;
+        T->shellRadii.assign(gridr + first, gridr + gridSize);
+        T->axisX = 1. / cbrt(axisRatioY * axisRatioZ);
+        T->axisY = axisRatioY * T->axisX;
+        T->axisZ = axisRatioZ * T->axisX;
+        bool ok = T->shellRadii.size() >= 1 && T->shellRadii[0] > 0;
+        for(size_t k = 1; k < T->shellRadii.size(); k++) ok &= T->shellRadii[k] > T->shellRadii[k - 1];
+        if(!ok || stripsPerPane < 1 || !(axisRatioY > 0) || !(axisRatioZ > 0)) {
+            delete T;
+            throw std::invalid_argument("TargetDensityClassic: invalid grid parameters");
+        }
+        T->valuesPerShell = 3 * stripsPerPane * (stripsPerPane + degree) + degree;
+        T->numValues = T->valuesPerShell * static_cast<int>(T->shellRadii.size()) + degree;
+        return T;
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+extern "C" void agama_deleteTarget(agama_Target* target) { delete target; }
+
+extern "C" int agama_targetNumCoefs(const agama_Target* target) { return target ? target->numValues : 0; }
+
+extern "C" int agama_integrateOrbitsTargetManyDevice(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, const agama_Target* target, float* output,
+    double* finalState, long* numSteps, int* status, void* stream)
+{
+    return guarded([&] {
+        if(!p || !target || n < 0 || (n > 0 && (!ic || !T || !output || !finalState)))
+            throw std::invalid_argument("integrateOrbitsTargetManyDevice: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        OrbitParams P = makeOrbitParams(Omega, accuracy, maxNumSteps);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t cubeBytes = static_cast<size_t>(n) * target->numValues * sizeof(double);
+        const size_t radiiBytes = target->shellRadii.size() * sizeof(double);
+        Scratch scratch(cubeBytes + radiiBytes + 512, s);
+        double* cube = static_cast<double*>(scratch.ptr);
+        double* radii = reinterpret_cast<double*>(static_cast<char*>(scratch.ptr) + cubeBytes);
+        unsigned long long* queue = reinterpret_cast<unsigned long long*>(
+            static_cast<char*>(scratch.ptr) + cubeBytes + ((radiiBytes + 255) / 256) * 256);
+        AGB_CUDA(cudaMemsetAsync(cube, 0, cubeBytes, s));
+        AGB_CUDA(cudaMemcpyAsync(radii, target->shellRadii.data(), radiiBytes, cudaMemcpyHostToDevice, s));
+        TargetView& V = P.target;
+        V.degree = target->degree;
+        V.strips = target->strips;
+        V.nShells = static_cast<int>(target->shellRadii.size());
+        V.valuesPerShell = target->valuesPerShell;
+        V.numValues = target->numValues;
+        V.shellRadii = radii;
+        V.axisX = target->axisX; V.axisY = target->axisY; V.axisZ = target->axisZ;
+        V.datacube = cube;
+        V.output = output;
+        launchOrbits(p->pot->view, P, n, ic, T, finalState, numSteps, nullptr, status, queue, s);
+        // the scratch (accumulators, radii) is released in stream order after the kernel
+    });
+}
+
+extern "C" int agama_integrateOrbitsTargetMany(const agama_Potential* p, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, const agama_Target* target, float* output,
+    double* finalState, long* numSteps, int* status)
+{
+    return guarded([&] {
+        if(!p || !target || n < 0 || (n > 0 && (!ic || !T || !output)))
+            throw std::invalid_argument("integrateOrbitsTargetMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const size_t m = static_cast<size_t>(n) * target->numValues;
+        DevBuf<double> dic(6 * n), dT(n), dout(6 * n);
+        DevBuf<float> dres(m);
+        DevBuf<long> dsteps(n);
+        DevBuf<int> dstat(n);
+        AGB_CUDA(cudaMemcpy(dic.ptr, ic, 6 * n * sizeof(double), cudaMemcpyHostToDevice));
+        AGB_CUDA(cudaMemcpy(dT.ptr, T, n * sizeof(double), cudaMemcpyHostToDevice));
+        if(agama_integrateOrbitsTargetManyDevice(p, n, dic.ptr, dT.ptr, Omega, accuracy, maxNumSteps, target,
+                dres.ptr, dout.ptr, dsteps.ptr, dstat.ptr, nullptr) != 0)
+            throw std::runtime_error(lastError());
+        AGB_CUDA(cudaMemcpy(output, dres.ptr, m * sizeof(float), cudaMemcpyDeviceToHost));
+        if(finalState) AGB_CUDA(cudaMemcpy(finalState, dout.ptr, 6 * n * sizeof(double), cudaMemcpyDeviceToHost));
+        if(numSteps) AGB_CUDA(cudaMemcpy(numSteps, dsteps.ptr, n * sizeof(long), cudaMemcpyDeviceToHost));
+        if(status) AGB_CUDA(cudaMemcpy(status, dstat.ptr, n * sizeof(int), cudaMemcpyDeviceToHost));
+    });
+}
+
 // ---- orbit batches captured once in a CUDA graph and replayed
 
 struct agama_OrbitGraph {
@@ -391,7 +540,7 @@ struct agama_OrbitGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     DevBuf<unsigned long long> queue;
-    int lanes = 1;
+    OrbitShape shape;
     ~agama_OrbitGraph() {
         if(exec) cudaGraphExecDestroy(exec);
         if(graph) cudaGraphDestroy(graph);
@@ -413,12 +562,12 @@ extern "C" agama_OrbitGraph* agama_orbitGraphCreate(const agama_Potential* p, lo
             g->queue.alloc(1);
             cudaStream_t s;
             AGB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-            // the lanes per orbit are settled (autotuner trial) before the capture begins
-            g->lanes = orbitLanesFor(p->pot->view, P, n, ic, T, s);
+            // the launch shape is settled (autotuner trial) before the capture begins
+            g->shape = orbitShapeFor(p->pot->view, P, n, ic, T, s);
             AGB_CUDA(cudaStreamSynchronize(s));
             AGB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             launchOrbits(p->pot->view, P, n, ic, T, finalState, numSteps, numRejected, status, g->queue.ptr, s,
-                g->lanes);
+                g->shape);
             AGB_CUDA(cudaStreamEndCapture(s, &g->graph));
             AGB_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0));
             AGB_CUDA(cudaStreamDestroy(s));
@@ -442,7 +591,8 @@ extern "C" int agama_orbitGraphLaunch(agama_OrbitGraph* g, void* stream)
     });
 }
 
-extern "C" int agama_orbitGraphLanes(const agama_OrbitGraph* g) { return g ? g->lanes : 0; }
+extern "C" int agama_orbitGraphLanes(const agama_OrbitGraph* g) { return g ? g->shape.lanes : 0; }
+extern "C" int agama_orbitGraphBlockSize(const agama_OrbitGraph* g) { return g ? g->shape.block : 0; }
 
 extern "C" void agama_orbitGraphDelete(agama_OrbitGraph* g) { delete g; }
 

@@ -5,6 +5,20 @@
 
 namespace agb {
 
+/** A runtime function of the orbits: time-weighted samples of each orbit accumulated into the
+    basis elements of a spheroidal density grid (the reference's RuntimeFncTarget with
+    TargetDensityClassic<N>, src/galaxymodel_target.h:99-150, src/galaxymodel_densitygrid.cpp:149-237):
+    shells in the spheroidal radius sqrt((x/ax)^2 + (y/ay)^2 + (z/az)^2), each octant surface cut
+    into three panes of strips x strips cells; degree 0 = top-hat cells, 1 = trilinear nodes. */
+struct TargetView {
+    int degree = -1;              ///< -1: no target; 0: DensityClassicTopHat; 1: DensityClassicLinear
+    int strips = 0, nShells = 0, valuesPerShell = 0, numValues = 0;
+    const double* shellRadii = nullptr;   ///< nShells positive increasing radii
+    double axisX = 1, axisY = 1, axisZ = 1;
+    double* datacube = nullptr;   ///< n x numValues accumulators (zeroed before the launch)
+    float* output = nullptr;      ///< n x numValues results, normalised by the integration time
+};
+
 /// integration parameters shared by all orbits of a batch
 struct OrbitParams {
     double Omega;        ///< pattern speed of the rotating frame
@@ -13,7 +27,65 @@ struct OrbitParams {
     long   maxSteps;     ///< maximum number of accepted steps per orbit
     int    trajSize = 0; ///< samples per orbit at regular times 0 .. T (0: final point only)
     double* traj = nullptr;   ///< n x trajSize x 6 samples (rotating frame), NaN where none
+    TargetView target;        ///< optional runtime function of the orbits (degree -1: none)
 };
+
+/** Add one point to the basis elements of a classic density grid, weighted by mult
+    (TargetDensityClassic<N>::addPoint and getCornerIndicesClassic, src/galaxymodel_densitygrid.cpp:59-84,
+    :170-238): the shell from a binary search in the spheroidal radius, the pane from the largest
+    coordinate, the strips from the angles atan(c1/c0), atan(c2/c0) in units of pi/4.  Points
+    outside the last shell add nothing; a point whose pane cannot be determined (NaN coordinates,
+    where the reference throws) adds nothing either.  values is the row of one orbit, owned by one
+    lane: the sums run in the order of the samples, as in the reference. */
+__device__ inline void targetAddPoint(const TargetView& T, const double p[3], double mult, double* values)
+{
+    const double X = fabs(p[0] / T.axisX), Y = fabs(p[1]) / T.axisY, Z = fabs(p[2]) / T.axisZ;
+    const double r = sqrt(X * X + Y * Y + Z * Z);
+    const int indShell = binSearch(r, T.shellRadii, T.nShells) + 1;
+    if(indShell >= T.nShells || mult == 0) return;
+    int pane;
+    double c0, c1, c2;
+    if(X >= Y && X > Z)       { pane = 0; c0 = X; c1 = Y; c2 = Z; }
+    else if(Y >= Z && Y > X)  { pane = 1; c0 = Y; c1 = Z; c2 = X; }
+    else if(Z >= X && Z >= Y) { pane = 2; c0 = Z; c1 = X; c2 = Y; }
+    else return;
+    const int S = T.strips;
+    double ratio1 = fmin(atan(c1 / c0) * (4 / M_PI), 1.) * S;
+    double ratio2 = fmin(atan(c2 / c0) * (4 / M_PI), 1.) * S;
+    const int ind1 = min(static_cast<int>(ratio1), S - 1), ind2 = min(static_cast<int>(ratio2), S - 1);
+    if(T.degree == 0) {
+        values[ind1 + (ind2 + pane * S) * S + indShell * T.valuesPerShell] += mult;
+        return;
+    }
+    // degree 1: the four corner nodes of the cell on the two shells around the point
+    const int ll = ind1 + (ind2 + pane * S) * (S + 1), ul = ll + 1;
+    int lu, uu;
+    if(ind2 < S - 1) { lu = ll + S + 1; uu = lu + 1; }
+    else {
+        const int adj = (pane + 2) % 3;
+        lu = (ind1 + adj * S + 1) * (S + 1) - 1;
+        uu = ind1 < S - 1 ? lu + S + 1 : 3 * S * (S + 1);
+    }
+    ratio1 -= ind1;
+    ratio2 -= ind2;
+    double val = indShell == 0 ? mult * r / T.shellRadii[0] :
+        mult * (r - T.shellRadii[indShell - 1]) / (T.shellRadii[indShell] - T.shellRadii[indShell - 1]);
+    double* off = values + indShell * T.valuesPerShell + 1;
+    off[ll] += (1 - ratio1) * (1 - ratio2) * val;
+    off[ul] += ratio1 * (1 - ratio2) * val;
+    off[lu] += (1 - ratio1) * ratio2 * val;
+    off[uu] += ratio1 * ratio2 * val;
+    if(indShell == 0)
+        values[0] += mult - val;
+    else {
+        off -= T.valuesPerShell;
+        val = mult - val;
+        off[ll] += (1 - ratio1) * (1 - ratio2) * val;
+        off[ul] += ratio1 * (1 - ratio2) * val;
+        off[lu] += (1 - ratio1) * ratio2 * val;
+        off[uu] += ratio1 * ratio2 * val;
+    }
+}
 
 /// per-orbit outcome codes
 enum OrbitStatus { ORBIT_OK = 0, ORBIT_MAX_STEPS = 1, ORBIT_BAD_STEP = 2, ORBIT_NONFINITE = 3, ORBIT_BUDGET = 4 };

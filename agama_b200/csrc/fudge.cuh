@@ -309,6 +309,22 @@ static __device__ double fudgeMomentumNode(const FudgeFunction& fnc, double lo, 
     return v * duds;
 }
 
+/** The same node with the integrand's arithmetic in FP32 (the mixed-precision form of the action
+    quadrature): F(tau) and the point tau come from FP64 (the potential and the cancellation in
+    F stay FP64), then p^2 = F / (2 (tau - D2)^2 tau), its square root (the hardware reciprocal
+    square root) and the product with du/ds are FP32; the caller accumulates the weighted terms with
+    compensation. */
+static __device__ float fudgeMomentumNode32(const FudgeFunction& fnc, double lo, double hi, double s)
+{
+    double duds;
+    const double tau = unscaleCub(lo, hi, s, &duds);
+    const float tmd = static_cast<float>(tau - fnc.D2), t = static_cast<float>(tau);
+    const float p2 = static_cast<float>(fnc.value(tau)) / (2.f * tmd * tmd * t);
+    float v = p2 > 0.f ? p2 * rsqrtf(p2) : 0.f;
+    if(!(v < INFINITY)) v = 0.f;
+    return v * static_cast<float>(duds);
+}
+
 /** Phase 1 of the actions of one point (R, z, phi, vR, vz, vphi) for focal distance fd
     (evalAxisymFudge, src/actions_staeckel.cpp:683-693: fd <= 0 falls back to max(R,1)*1e-4);
     Phi is the potential at the point.  Writes Jphi into act[2]; for a point without actions

@@ -21,6 +21,9 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
 /// integrals of different orders (10 to 40 nodes) keep every lane busy.  The nodes of one integral
 /// are summed in order (computeActions, src/actions_staeckel.cpp:604-619: Jr = I_lambda / pi,
 /// Jz = 2 I_nu / pi).
+/// MIXED: the integrand's arithmetic after F(tau) in FP32 (fudgeMomentumNode32) and the weighted
+/// terms summed in FP32 with a compensation term (Kahan), converted to FP64 at the end.
+template<bool MIXED>
 __global__ void __launch_bounds__(INTEGRAL_BLOCK, 4) fudgeIntegralKernel(const __grid_constant__ MultipoleView M,
     const __grid_constant__ GLRules gl, long n, const FudgeRecord* __restrict__ rec, double* __restrict__ act,
     unsigned long long* __restrict__ counter)
@@ -31,6 +34,7 @@ __global__ void __launch_bounds__(INTEGRAL_BLOCK, 4) fudgeIntegralKernel(const _
     long point = 0;
     int which = 0, node = 0, numNodes = 0;
     double lo = 0, hi = 0, sum = 0;
+    float sum32 = 0.f, comp32 = 0.f;
     const double* x = nullptr;
     const double* w = nullptr;
     FudgeFunction fnc;
@@ -61,6 +65,7 @@ __global__ void __launch_bounds__(INTEGRAL_BLOCK, 4) fudgeIntegralKernel(const _
                         w = gl.weights + gl.offset[N];
                         node = 0;
                         sum = 0;
+                        sum32 = comp32 = 0.f;
                         busy = true;
                     }
                 }
@@ -68,16 +73,24 @@ __global__ void __launch_bounds__(INTEGRAL_BLOCK, 4) fudgeIntegralKernel(const _
         }
         if(!__any_sync(FULL_MASK, busy)) break;
         if(busy) {
-            sum += ldg(w + node) * fudgeMomentumNode(fnc, lo, hi, ldg(x + node));
+            if(MIXED) {
+                const float term = static_cast<float>(ldg(w + node)) * fudgeMomentumNode32(fnc, lo, hi, ldg(x + node));
+                const float y = term - comp32, t = sum32 + y;
+                comp32 = (t - sum32) - y;
+                sum32 = t;
+            } else
+                sum += ldg(w + node) * fudgeMomentumNode(fnc, lo, hi, ldg(x + node));
             if(++node == numNodes) {
                 busy = false;
+                if(MIXED) sum = static_cast<double>(sum32) - static_cast<double>(comp32);
                 act[3 * point + which] = which == 0 ? sum / M_PI : sum / M_PI * 2;
             }
         }
     }
 }
 
-/// resident blocks of the integral kernel on the current device (cached per device)
+/// resident blocks of the integral kernel on the current device (cached per device and variant)
+template<bool MIXED>
 int integralGridSize()
 {
     static std::mutex mutex;
@@ -89,7 +102,7 @@ int integralGridSize()
     if(it != cache.end()) return it->second;
     int sms = 0, perSM = 0;
     AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fudgeIntegralKernel, INTEGRAL_BLOCK, 0));
+    AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fudgeIntegralKernel<MIXED>, INTEGRAL_BLOCK, 0));
     const int grid = std::max(1, sms * std::max(1, perSM));
     cache[dev] = grid;
     return grid;
@@ -98,12 +111,18 @@ int integralGridSize()
 }  // namespace
 
 void launchFudgeIntegrals(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,
-    unsigned long long* counter, cudaStream_t stream)
+    unsigned long long* counter, bool mixed, cudaStream_t stream)
 {
     if(n <= 0) return;
     AGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
-    const long grid = std::min<long>(integralGridSize(), (2 * n + INTEGRAL_BLOCK - 1) / INTEGRAL_BLOCK);
-    fudgeIntegralKernel<<<grid, INTEGRAL_BLOCK, 0, stream>>>(M, gl, n, rec, act, counter);
+    const long tasks = (2 * n + INTEGRAL_BLOCK - 1) / INTEGRAL_BLOCK;
+    if(mixed) {
+        const long grid = std::min<long>(integralGridSize<true>(), tasks);
+        fudgeIntegralKernel<true><<<grid, INTEGRAL_BLOCK, 0, stream>>>(M, gl, n, rec, act, counter);
+    } else {
+        const long grid = std::min<long>(integralGridSize<false>(), tasks);
+        fudgeIntegralKernel<false><<<grid, INTEGRAL_BLOCK, 0, stream>>>(M, gl, n, rec, act, counter);
+    }
     AGB_CUDA(cudaGetLastError());
 }
 

@@ -28,9 +28,10 @@ void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const Fu
 void launchBracketTargets(long n, const FudgeRecord* rec, float* target, float* mask, cudaStream_t stream);
 
 /// phase 3: Jr and Jz of every valid record into act[3 i], act[3 i + 1], drained by a persistent
-/// grid from a device work counter (8 bytes, zeroed here on the stream)
+/// grid from a device work counter (8 bytes, zeroed here on the stream); mixed: the integrand's
+/// arithmetic after F(tau) and the sums in FP32 (compensated), F(tau) in FP64
 void launchFudgeIntegrals(const MultipoleView& M, const GLRules& gl, long n, const FudgeRecord* rec, double* act,
-    unsigned long long* counter, cudaStream_t stream);
+    unsigned long long* counter, bool mixed, cudaStream_t stream);
 
 /// phase 3 with angles / frequencies: actions into act (n x 3, Jphi already there), frequencies
 /// (Omega_r, Omega_z, Omega_phi) and angles (theta_r, theta_z, theta_phi) into freq / ang when

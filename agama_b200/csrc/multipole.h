@@ -89,6 +89,13 @@ MultipoleHost buildMultipole(const std::vector<double>& radii,
 void readMultipoleCoefFile(const std::string& fileName, std::vector<double>& radii,
     std::vector<std::vector<double>>& Phi, std::vector<std::vector<double>>& dPhi);
 
+/// write the coefficients in the same text format (the layout of writePotentialMultipole,
+/// reference src/potential_factory.cpp:909-930: [Potential] section, gridSizeR, lmax, symmetry
+/// name, #Phi and #dPhi/dr blocks of tab-separated columns l=..,m=..), with every number in 17
+/// significant digits so that reading the file back gives the same doubles
+void writeMultipoleCoefFile(const std::string& fileName, const std::vector<double>& radii,
+    const std::vector<std::vector<double>>& Phi, const std::vector<std::vector<double>>& dPhi, int symmetry);
+
 // helpers shared with the action-finder construction
 double lambertW(double x, bool lowerBranch);
 void glNodesWeights(int n, double* nodes, double* weights);   // on [-1, 1], ascending

@@ -8,6 +8,8 @@
 #include <sstream>
 #include <algorithm>
 #include <cstring>
+#include <cstdio>
+#include <cmath>
 
 namespace agb {
 
@@ -511,6 +513,64 @@ void parseBlock(const std::vector<std::string>& lines, size_t& pos, size_t gridS
     }
 }
 }  // namespace
+
+namespace {
+/// names of the symmetry types as the reference writes them (getSymmetryNameByType,
+/// src/potential_factory.cpp:240-252); other combinations as their number
+std::string symmetryName(int sym)
+{
+    switch(sym) {
+        case SYM_NONE: return "None";
+        case SYM_REFL: return "Reflection";
+        case SYM_XREFL | SYM_YREFL | SYM_REFL: return "Bisymmetric";
+        case SYM_TRIAXIAL: return "Triaxial";
+        case SYM_AXISYMMETRIC: return "Axisymmetric";
+        case SYM_SPHERICAL: return "Spherical";
+        default: return std::to_string(sym);
+    }
+}
+
+void writeBlock(std::ostream& out, const std::vector<double>& radii, const std::vector<std::vector<double>>& coefs)
+{
+    const int lmax = static_cast<int>(std::lround(std::sqrt(static_cast<double>(coefs.size())))) - 1;
+    out << "#radius";
+    for(int l = 0; l <= lmax; l++)
+        for(int m = -l; m <= l; m++) out << "\tl=" << l << ",m=" << m;
+    out << '\n';
+    char buf[40];
+    for(size_t k = 0; k < radii.size(); k++) {
+        snprintf(buf, sizeof(buf), "%.17g", radii[k]);
+        out << buf;
+        for(size_t c = 0; c < coefs.size(); c++) {
+            const double v = k < coefs[c].size() ? coefs[c][k] : 0;
+            if(v == 0) out << "\t0";
+            else { snprintf(buf, sizeof(buf), "%.17g", v); out << '\t' << buf; }
+        }
+        out << '\n';
+    }
+}
+}  // namespace
+
+void writeMultipoleCoefFile(const std::string& fileName, const std::vector<double>& radii,
+    const std::vector<std::vector<double>>& Phi, const std::vector<std::vector<double>>& dPhi, int symmetry)
+{
+    if(radii.size() < 2 || Phi.empty() || Phi.size() != dPhi.size())
+        throw std::invalid_argument("writeMultipoleCoefFile: inconsistent coefficients");
+    const size_t nc = Phi.size();
+    const size_t lp1 = static_cast<size_t>(std::lround(std::sqrt(static_cast<double>(nc))));
+    if(lp1 * lp1 != nc)
+        throw std::invalid_argument("writeMultipoleCoefFile: the number of coefficients is not (lmax+1)^2");
+    std::ofstream out(fileName);
+    if(!out)
+        throw std::runtime_error("cannot write " + fileName);
+    out << "[Potential]\ntype=Multipole\ngridSizeR=" << radii.size() << "\nlmax=" << (lp1 - 1) << "\nsymmetry="
+        << symmetryName(symmetry) << "\nCoefficients\n#Phi\n";
+    writeBlock(out, radii, Phi);
+    out << "\n#dPhi/dr\n";
+    writeBlock(out, radii, dPhi);
+    if(!out)
+        throw std::runtime_error("error writing " + fileName);
+}
 
 void readMultipoleCoefFile(const std::string& fileName, std::vector<double>& radii,
     std::vector<std::vector<double>>& Phi, std::vector<std::vector<double>>& dPhi)

@@ -14,12 +14,15 @@
 #include <mutex>
 #include <tuple>
 #include <algorithm>
+#include <set>
+#include <utility>
+#include <vector>
 
 namespace agb {
 
 namespace {
 
-constexpr int ORBIT_BLOCK = 64;
+constexpr int ORBIT_BLOCK_MAX = 128;                 // largest block of the orbit kernels
 constexpr int NUM_STAGE_VECTORS = 9;                 // k2 .. k10 (k11..k13 reuse k2..k4)
 constexpr int MAX_ATTEMPTS_PER_STEP = 1000;          // guard against a runaway rejection loop
 constexpr double HMIN = 1e-12, HMAX = 1e12;          // initial-step limits, src/math_ode.cpp:40
@@ -78,15 +81,60 @@ __host__ __device__ constexpr StageTable makeStageTable()
 }
 __constant__ StageTable STAGE_TABLE = makeStageTable();
 
+/** The 7th-order dense output of the last accepted step [t, t + h] at offset (0..h) from its start
+    (OdeStepperDOP853::getSol and its coefficients, src/math_ode.cpp:381-426), in the integration
+    (inertial) frame. */
+__device__ void denseOutput(double h, double offset, const double* x, const double* xt, const double* k1,
+    const double* k13, const StageStore& S, double* v)
+{
+    using namespace dp853;
+    if(offset == h) {
+        for(int c = 0; c < 6; c++) v[c] = xt[c];
+        return;
+    }
+    if(offset == 0) {
+        for(int c = 0; c < 6; c++) v[c] = x[c];
+        return;
+    }
+    const double p = offset / h, q = 1.0 - p;
+    for(int c = 0; c < 6; c++) {
+        const double k6 = S.at(4, c), k7 = S.at(5, c), k8 = S.at(6, c), k9 = S.at(7, c), k10 = S.at(8, c),
+            k11 = S.at(0, c), k12 = S.at(1, c);
+        const double xd = xt[c] - x[c], xc = h * k1[c] - xd;
+        const double r4 = xd - h * k13[c] - xc;
+        const double r5 = h * (d41 * k1[c] + d46 * k6 + d47 * k7 + d48 * k8 + d49 * k9 + d410 * k10 +
+                               d411 * k11 + d412 * k12 + d413 * k13[c]);
+        const double r6 = h * (d51 * k1[c] + d56 * k6 + d57 * k7 + d58 * k8 + d59 * k9 + d510 * k10 +
+                               d511 * k11 + d512 * k12 + d513 * k13[c]);
+        const double r7 = h * (d61 * k1[c] + d66 * k6 + d67 * k7 + d68 * k8 + d69 * k9 + d610 * k10 +
+                               d611 * k11 + d612 * k12 + d613 * k13[c]);
+        const double r8 = h * (d71 * k1[c] + d76 * k6 + d77 * k7 + d78 * k8 + d79 * k9 + d710 * k10 +
+                               d711 * k11);
+        v[c] = x[c] + p * (xd + q * (xc + p * (r4 + q * (r5 + p * (r6 + q * (r7 + p * r8))))));
+    }
+}
+
+/// a phase-space point of the integration frame rotated to the frame of the potential at time
+/// tabs (OrbitIntegrator<Car>::getSolNative, src/orbit.cpp:119-133)
+__device__ __forceinline__ void toPotentialFrame(double Omega, double tabs, const double* v, double* o)
+{
+    double ca = 1, sa = 0;
+    if(Omega != 0) sincos(Omega * tabs, &sa, &ca);
+    o[0] = v[0] * ca + v[1] * sa;
+    o[1] = v[1] * ca - v[0] * sa;
+    o[2] = v[2];
+    o[3] = v[3] * ca + v[4] * sa;
+    o[4] = v[4] * ca - v[3] * sa;
+    o[5] = v[5];
+}
+
 /** Trajectory samples inside one accepted step [t, t + h] at the regular times k T/(trajSize-1)
     (RuntimeTrajectory::processTimestep, src/orbit.cpp:15-47: sample range with the 10 eps
-    round-off allowance, offsets clipped into the step) from the 7th-order dense output of the step
-    (OdeStepperDOP853::getSol and its coefficients, src/math_ode.cpp:381-426), rotated to the frame of
-    the potential at each sample time (OrbitIntegrator<Car>::getSolNative, src/orbit.cpp:119-133). */
+    round-off allowance, offsets clipped into the step) from the dense output of the step, rotated
+    to the frame of the potential at each sample time. */
 __device__ void sampleStep(const OrbitParams& P, long i, double tEnd, double sign, double t, double h,
     const double* x, const double* xt, const double* k1, const double* k13, const StageStore& S)
 {
-    using namespace dp853;
     const double dt = fabs(tEnd) / (P.trajSize - 1), tend = t + h;
     const double roundoff = 10 * DBL_EPSILON * fmax(fabs(tend), fabs(t));
     long iout = static_cast<long>(ceil(sign * t / dt));
@@ -96,37 +144,26 @@ __device__ void sampleStep(const OrbitParams& P, long i, double tEnd, double sig
         const double timeout = sign * dt * iout;
         const double offset = clip(sign * (timeout - t), 0.0, sign * h) * sign;
         double v[6];
-        if(offset == h) {
-            for(int c = 0; c < 6; c++) v[c] = xt[c];
-        } else if(offset == 0) {
-            for(int c = 0; c < 6; c++) v[c] = x[c];
-        } else {
-            const double p = offset / h, q = 1.0 - p;
-            for(int c = 0; c < 6; c++) {
-                const double k6 = S.at(4, c), k7 = S.at(5, c), k8 = S.at(6, c), k9 = S.at(7, c), k10 = S.at(8, c),
-                    k11 = S.at(0, c), k12 = S.at(1, c);
-                const double xd = xt[c] - x[c], xc = h * k1[c] - xd;
-                const double r4 = xd - h * k13[c] - xc;
-                const double r5 = h * (d41 * k1[c] + d46 * k6 + d47 * k7 + d48 * k8 + d49 * k9 + d410 * k10 +
-                                       d411 * k11 + d412 * k12 + d413 * k13[c]);
-                const double r6 = h * (d51 * k1[c] + d56 * k6 + d57 * k7 + d58 * k8 + d59 * k9 + d510 * k10 +
-                                       d511 * k11 + d512 * k12 + d513 * k13[c]);
-                const double r7 = h * (d61 * k1[c] + d66 * k6 + d67 * k7 + d68 * k8 + d69 * k9 + d610 * k10 +
-                                       d611 * k11 + d612 * k12 + d613 * k13[c]);
-                const double r8 = h * (d71 * k1[c] + d76 * k6 + d77 * k7 + d78 * k8 + d79 * k9 + d710 * k10 +
-                                       d711 * k11);
-                v[c] = x[c] + p * (xd + q * (xc + p * (r4 + q * (r5 + p * (r6 + q * (r7 + p * r8))))));
-            }
-        }
-        double ca = 1, sa = 0;
-        if(P.Omega != 0) sincos(P.Omega * (t + offset), &sa, &ca);
-        double* o = P.traj + (i * P.trajSize + iout) * 6;
-        o[0] = v[0] * ca + v[1] * sa;
-        o[1] = v[1] * ca - v[0] * sa;
-        o[2] = v[2];
-        o[3] = v[3] * ca + v[4] * sa;
-        o[4] = v[4] * ca - v[3] * sa;
-        o[5] = v[5];
+        denseOutput(h, offset, x, xt, k1, k13, S, v);
+        toPotentialFrame(P.Omega, t + offset, v, P.traj + (i * P.trajSize + iout) * 6);
+    }
+}
+
+/// samples of one accepted step for the target of the batch (RuntimeFncTarget::processTimestep,
+/// src/galaxymodel_target.h:140-152): NUM_SAMPLES_PER_STEP points at the middles of equal
+/// sub-steps of the step, each weighted by the sub-step's duration
+constexpr int TARGET_SAMPLES_PER_STEP = 10;
+__device__ void targetStep(const OrbitParams& P, long i, double t, double h, const double* x, const double* xt,
+    const double* k1, const double* k13, const StageStore& S)
+{
+    const double substep = h / TARGET_SAMPLES_PER_STEP;
+    double* row = P.target.datacube + i * P.target.numValues;
+    for(int k = 0; k < TARGET_SAMPLES_PER_STEP; k++) {
+        const double off = substep * (k + 0.5);
+        double v[6], w[6];
+        denseOutput(h, off, x, xt, k1, k13, S, v);
+        toPotentialFrame(P.Omega, t + off, v, w);
+        targetAddPoint(P.target, w, substep, row);
     }
 }
 
@@ -151,7 +188,7 @@ enum { PH_FETCH, PH_INIT1, PH_INIT2, PH_INIT3, PH_STAGE, PH_FINISH };
     MIXED: the forces of the multi-harmonic kind with the m != 0 harmonics in FP32 (the radial m = 0
     part, the Fourier sums, the state, the stages and the error norm stay FP64). */
 template<int KIND, int G, bool MIXED>
-__global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constant__ MultipoleView M, const OrbitParams P,
+__global__ void __launch_bounds__(ORBIT_BLOCK_MAX) dop853Kernel(const __grid_constant__ MultipoleView M, const OrbitParams P,
     long n, const double* __restrict__ ic, const double* __restrict__ T, double* __restrict__ out,
     long* __restrict__ nsteps, long* __restrict__ nrej, int* __restrict__ status,
     unsigned long long* queue)
@@ -172,7 +209,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
     int phase = queue ? PH_FETCH : PH_INIT1;
     double x[6], k1[6], xt[6], k1b[6];
     double t = 0, tEnd = 0, sign = 1, h = 0, h1 = 0, hNext = 0, accFac = 1, preverr = INFINITY, tb = 0, hLast = 0,
-        remaining = 0;
+        remaining = 0, targetTime = 0;
     long steps = 0, rejects = 0;
     int st = ORBIT_OK, row = 0, nbad = 0, attempts = 0;
 
@@ -202,7 +239,7 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
         if(phase == PH_INIT1) {          // a new orbit: load its start
             for(int c = 0; c < 6; c++) x[c] = ic[6 * i + c];
             tEnd = T[i];
-            t = 0; tb = 0; hLast = 0; steps = 0; rejects = 0; st = ORBIT_OK; accFac = 1;
+            t = 0; tb = 0; hLast = 0; steps = 0; rejects = 0; st = ORBIT_OK; accFac = 1; targetTime = 0;
             sign = tEnd >= 0 ? 1 : -1;
             if(P.traj && gl == 0) {
                 // no sample yet; an orbit that is not integrated gets its start as sample 0 (and, for
@@ -228,6 +265,17 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
                 if(nsteps) nsteps[i] = steps;
                 if(nrej) nrej[i] = rejects;
                 if(status) status[i] = st;
+                if(P.target.degree >= 0) {
+                    // RuntimeFncTarget's finalisation: the sums converted to FP32, then scaled
+                    // by the inverse integration time in FP32 (src/galaxymodel_target.h:127-135)
+                    const double* row = P.target.datacube + i * P.target.numValues;
+                    float* o = P.target.output + i * P.target.numValues;
+                    const float inv = static_cast<float>(1. / targetTime);
+                    for(int k = 0; k < P.target.numValues; k++) {
+                        o[k] = static_cast<float>(row[k]);
+                        if(targetTime != 0) o[k] *= inv;
+                    }
+                }
             }
             if(!queue) break;
             phase = PH_FETCH;
@@ -323,6 +371,10 @@ __global__ void __launch_bounds__(ORBIT_BLOCK) dop853Kernel(const __grid_constan
                 }
             }
             if(P.traj && gl == 0) sampleStep(P, i, tEnd, sign, t, h, x, xt, k1, k, S);
+            if(P.target.degree >= 0 && gl == 0) {
+                targetStep(P, i, t, h, x, xt, k1, k, S);
+                targetTime += h;
+            }
             for(int c = 0; c < 6; c++) { x[c] = xt[c]; k1[c] = k[c]; }
             tb = t;
             hLast = h;
@@ -363,15 +415,32 @@ OrbitKernel orbitKernel(int kind, int lanes, bool mixed)
 /// FP32 non-axisymmetric harmonics in later batches (multi-harmonic potentials only; off by default)
 std::atomic<int> g_mixedSetting{ 0 };
 
+/// raise the dynamic shared-memory limit of an orbit kernel on the current device once (the
+/// stage vectors of 128 threads take 54 KB, above the default 48 KB)
+void allowOrbitSharedMemory(OrbitKernel kernel)
+{
+    static std::mutex mutex;
+    static std::set<std::pair<int, const void*>> done;
+    int dev;
+    AGB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mutex);
+    const auto key = std::make_pair(dev, reinterpret_cast<const void*>(kernel));
+    if(done.count(key)) return;
+    AGB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(orbitSharedBytes(ORBIT_BLOCK_MAX))));
+    done.insert(key);
+}
+
 void launchOrbitKernel(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, int lanes, bool mixed,
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, int lanes, int block, bool mixed,
     cudaStream_t stream)
 {
-    const int block = ORBIT_BLOCK;
+    if(block != 32 && block != 64 && block != 128) block = 64;
     const size_t shmem = orbitSharedBytes(block);
     mixed = mixed && evalKindOf(M) == EVAL_FAST;
     if(mixed) lanes = 1;
     const OrbitKernel kernel = orbitKernel(evalKindOf(M), lanes, mixed);
+    allowOrbitSharedMemory(kernel);
     const long threads = n * lanes;
     long grid;
     if(queue) {
@@ -393,40 +462,60 @@ void launchOrbitKernel(const MultipoleView& M, const OrbitParams& P, long n, con
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
-// Lanes per orbit: chosen by a timing trial on the caller's own orbits, once per device,
-// potential and batch-size class (powers of two), then cached.
+// Launch shape (lanes per orbit and threads per block): chosen by a timing trial on the caller's
+// own orbits, once per device, potential, batch-size class (powers of two) and precision, then
+// cached.  Every shape gives the same bits (the lanes of a group sum the harmonics in one order;
+// the block size only changes which orbits share a block), so the choice never changes a result.
 
 namespace {
 
-std::mutex g_laneMutex;
-std::map<std::tuple<int, const void*, int>, int> g_laneChoice;
-std::atomic<int> g_laneSetting{ 0 };
+std::mutex g_shapeMutex;
+std::map<std::tuple<int, const void*, int, int>, OrbitShape> g_shapeChoice;
+std::atomic<int> g_laneSetting{ 0 }, g_blockSetting{ 0 };
 constexpr int TRIAL_ORBITS = 32768, TRIAL_STEPS = 24;
 
-/// time each candidate on the first orbits of the batch, each integrated for TRIAL_STEPS steps
-int tuneLanes(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    cudaStream_t stream)
+/// time each candidate shape on the first orbits of the batch, each integrated for TRIAL_STEPS
+/// steps; candidates: lanes in {1, 2, 4, 8} (the multi-harmonic kind in FP64; 1 otherwise) times
+/// blocks in {32, 64, 128}
+OrbitShape tuneShape(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+    bool mixed, int fixedLanes, int fixedBlock, cudaStream_t stream)
 {
     const long m = std::min<long>(n, TRIAL_ORBITS);
     OrbitParams Pt = P;
     Pt.maxSteps = TRIAL_STEPS;
+    Pt.traj = nullptr;
+    Pt.trajSize = 0;
+    Pt.target = TargetView();
     Scratch scratch(m * 6 * sizeof(double) + 256, stream);
     double* out = static_cast<double*>(scratch.ptr);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(out + 6 * m);
+    std::vector<int> laneList, blockList;
+    const bool groups = evalKindOf(M) == EVAL_FAST && !mixed;
+    for(int l : { 1, 2, 4, 8 })
+        if((fixedLanes ? l == fixedLanes : true) && (groups || l == 1)) laneList.push_back(l);
+    for(int b : { 32, 64, 128 })
+        if(fixedBlock ? b == fixedBlock : true) blockList.push_back(b);
+    if(laneList.empty()) laneList.push_back(1);
+    if(blockList.empty()) blockList.push_back(64);
     cudaEvent_t a, b;
     AGB_CUDA(cudaEventCreate(&a));
     AGB_CUDA(cudaEventCreate(&b));
-    int best = 1;
+    OrbitShape best;
+    best.lanes = laneList[0];
+    best.block = blockList[0];
     float bestMs = INFINITY;
-    const int candidates[] = { 1, 1, 2, 4, 8 };          // the first run also absorbs one-time set-up
-    for(int c = 0; c < 5; c++) {
-        AGB_CUDA(cudaEventRecord(a, stream));
-        launchOrbitKernel(M, Pt, m, ic, T, out, nullptr, nullptr, nullptr, counter, candidates[c], false, stream);
-        AGB_CUDA(cudaEventRecord(b, stream));
-        AGB_CUDA(cudaEventSynchronize(b));
-        float ms = 0;
-        AGB_CUDA(cudaEventElapsedTime(&ms, a, b));
-        if(c > 0 && ms < bestMs) { bestMs = ms; best = candidates[c]; }
+    // one untimed run absorbs the one-time set-up (module loading, attributes)
+    launchOrbitKernel(M, Pt, m, ic, T, out, nullptr, nullptr, nullptr, counter, laneList[0], blockList[0], mixed, stream);
+    for(int l : laneList) {
+        for(int bl : blockList) {
+            AGB_CUDA(cudaEventRecord(a, stream));
+            launchOrbitKernel(M, Pt, m, ic, T, out, nullptr, nullptr, nullptr, counter, l, bl, mixed, stream);
+            AGB_CUDA(cudaEventRecord(b, stream));
+            AGB_CUDA(cudaEventSynchronize(b));
+            float ms = 0;
+            AGB_CUDA(cudaEventElapsedTime(&ms, a, b));
+            if(ms < bestMs) { bestMs = ms; best.lanes = l; best.block = bl; }
+        }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -436,36 +525,44 @@ int tuneLanes(const MultipoleView& M, const OrbitParams& P, long n, const double
 }  // namespace
 
 void setOrbitLanes(int lanes) { g_laneSetting = lanes; }
+void setOrbitBlock(int block) { g_blockSetting = block; }
 void setOrbitMixedPrecision(bool mixed) { g_mixedSetting = mixed ? 1 : 0; }
 
-int orbitLanesFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+OrbitShape orbitShapeFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     cudaStream_t stream)
 {
-    if(evalKindOf(M) != EVAL_FAST || g_mixedSetting) return 1;
-    const int fixed = g_laneSetting;
-    if(fixed == 1 || fixed == 2 || fixed == 4 || fixed == 8) return fixed;
+    const bool mixed = g_mixedSetting != 0 && evalKindOf(M) == EVAL_FAST;
+    const bool groups = evalKindOf(M) == EVAL_FAST && !mixed;
+    int fixedLanes = g_laneSetting, fixedBlock = g_blockSetting;
+    if(fixedLanes != 1 && fixedLanes != 2 && fixedLanes != 4 && fixedLanes != 8) fixedLanes = 0;
+    if(!groups) fixedLanes = 1;
+    if(fixedBlock != 32 && fixedBlock != 64 && fixedBlock != 128) fixedBlock = 0;
+    if(fixedLanes && fixedBlock) { OrbitShape s; s.lanes = fixedLanes; s.block = fixedBlock; return s; }
     int dev;
     AGB_CUDA(cudaGetDevice(&dev));
     int bucket = 0;
     while((1L << bucket) < n) bucket++;
-    const auto key = std::make_tuple(dev, static_cast<const void*>(M.spl2d), bucket);
+    // the key holds the fixed parts too (0 = tuned), so fixing one of them tunes only the other
+    const auto key = std::make_tuple(dev, static_cast<const void*>(M.spl2d), bucket,
+        (mixed ? 1 : 0) | (fixedLanes << 1) | (fixedBlock << 5));
     {
-        std::lock_guard<std::mutex> lock(g_laneMutex);
-        auto it = g_laneChoice.find(key);
-        if(it != g_laneChoice.end()) return it->second;
+        std::lock_guard<std::mutex> lock(g_shapeMutex);
+        auto it = g_shapeChoice.find(key);
+        if(it != g_shapeChoice.end()) return it->second;
     }
-    const int lanes = tuneLanes(M, P, n, ic, T, stream);
-    std::lock_guard<std::mutex> lock(g_laneMutex);
-    g_laneChoice[key] = lanes;
-    return lanes;
+    const OrbitShape shape = tuneShape(M, P, n, ic, T, mixed, fixedLanes, fixedBlock, stream);
+    std::lock_guard<std::mutex> lock(g_shapeMutex);
+    g_shapeChoice[key] = shape;
+    return shape;
 }
 
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes)
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, OrbitShape shape)
 {
     if(n <= 0) return;
-    if(lanes <= 0) lanes = orbitLanesFor(M, P, n, ic, T, stream);
-    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, queue, lanes, g_mixedSetting != 0, stream);
+    if(shape.lanes <= 0 || shape.block <= 0) shape = orbitShapeFor(M, P, n, ic, T, stream);
+    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, queue, shape.lanes, shape.block,
+        g_mixedSetting != 0, stream);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -516,7 +613,7 @@ void launchOrbitsNoAlloc(const MultipoleView& M, const OrbitParams& P, long n, c
     // the launch clears the counter (cudaMemsetAsync on the stream) before the kernel runs;
     // one lane per orbit (the lane autotuner's trial would allocate scratch), always FP64
     if(n <= 0) return;
-    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, 1, false, stream);
+    launchOrbitKernel(M, P, n, ic, T, out, nsteps, nrej, status, base + slot, 1, 64, false, stream);
 }
 
 }  // namespace agb

@@ -87,20 +87,30 @@ void launchDensity(const MultipoleView& M, long n, const double* pos, double* rh
 enum RadiusQuery { RADIUS_CIRC_E = 0, RADIUS_CIRC_L = 1, RADIUS_MAX = 2, RADIUS_PERIAPO = 3 };
 void launchRadii(const MultipoleView& M, int query, long n, const double* a, const double* b, double* out1,
     double* out2, cudaStream_t stream);
+/// launch shape of an orbit batch: lanes of a warp per orbit (1, 2, 4, 8) and threads per block
+/// (32, 64, 128); 0 = chosen by the autotuner.  Neither changes any result bit.
+struct OrbitShape { int lanes = 0, block = 0; };
 /// DOP853 batch; queue != nullptr selects the persistent work-queue mapping (8-byte counter)
 void launchOrbits(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
-    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream, int lanes = 0);
+    double* out, long* nsteps, long* nrej, int* status, unsigned long long* queue, cudaStream_t stream,
+    OrbitShape shape = OrbitShape());
 /// phase timing of the action computation: on = true clears and starts recording; on = false
 /// stops and returns the summed device durations (ms) of prepare, bracket inference, root
 /// searches and integrals, and the number of passes timed
 void setActionPhaseTiming(bool on, double* ms, long* passes);
+/// mixed precision for the action integrals of later calls: the integrand's arithmetic after
+/// F(tau) and the Gauss-Legendre sums in FP32 (compensated); false (default) = all FP64
+void setActionMixedPrecision(bool mixed);
 /// lanes per orbit for all later batches: 1, 2, 4, 8, or 0 (default) for the autotuner
 void setOrbitLanes(int lanes);
+/// threads per block of the orbit kernels for all later batches: 32, 64, 128, or 0 (default)
+/// for the autotuner
+void setOrbitBlock(int block);
 /// mixed precision for later batches in multi-harmonic potentials: the m != 0 harmonics of the
 /// force from an FP32 copy of the spline table (one lane per orbit); false (default) = all FP64
 void setOrbitMixedPrecision(bool mixed);
-/// the lanes per orbit a batch will use (runs the autotuner's trial on the stream if needed)
-int orbitLanesFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
+/// the launch shape a batch will use (runs the autotuner's trial on the stream if needed)
+OrbitShape orbitShapeFor(const MultipoleView& M, const OrbitParams& P, long n, const double* ic, const double* T,
     cudaStream_t stream);
 
 /// the same work-queue batch with its counter in the library's static device array (slot 0..31),

@@ -26,6 +26,66 @@ def trajectory(potential, ic, time, trajsize, Omega=0.0, accuracy=1e-8, maxNumSt
     return times, traj
 
 
+class Target:
+    """A density-grid target for orbits (the reference's Target(type='DensityClassicTopHat' or
+    'DensityClassicLinear', gridr=..., stripsPerPane=2, axisRatioY=1, axisRatioZ=1)): radial shells
+    with three panes of stripsPerPane^2 cells per octant surface; orbit_target() records, for each
+    orbit, the fraction of its time spent in each cell (top-hat) or the trilinear weights of the
+    grid nodes (linear)."""
+
+    def __init__(self, type="DensityClassicTopHat", gridr=None, stripsPerPane=2, axisRatioY=1.0, axisRatioZ=1.0):
+        t = str(type).lower()
+        if t not in ("densityclassictophat", "densityclassiclinear"):
+            raise ValueError("Target: only DensityClassicTopHat / DensityClassicLinear are supported")
+        g = np.ascontiguousarray(gridr, dtype=np.float64).ravel()
+        if len(g) < 2:
+            raise ValueError("gridr must be an array with >=2 elements")
+        h = _native.lib().agama_createTargetDensityClassic(0 if t.endswith("tophat") else 1, int(stripsPerPane),
+                                                           len(g), ptr(g), float(axisRatioY), float(axisRatioZ))
+        if not h:
+            raise ValueError("agama_b200: " + _native.error())
+        self._h = ctypes.c_void_p(h)
+
+    def __len__(self):
+        return _native.lib().agama_targetNumCoefs(self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        lib = getattr(_native, "_lib", None)     # module globals may be gone at interpreter exit
+        if h and lib is not None:
+            lib.agama_deleteTarget(h)
+            self._h = None
+
+
+def orbit_target(potential, ic, time, target, Omega=0.0, accuracy=1e-8, maxNumSteps=0):
+    """Orbits with a target's runtime function (as the reference's orbit(..., targets=[target])):
+    returns (final points n x 6, n x len(target) float32 matrix of the time-weighted samples of
+    each orbit, normalised by its integration time); numpy or CUDA tensors in, the same out."""
+    from . import _is_device_array, _dev_ptr, _current_stream
+    m = len(target)
+    if _is_device_array(ic):
+        import torch
+        x = ic.contiguous().view(-1, 6)
+        n = x.shape[0]
+        T = time if _is_device_array(time) else torch.full((n,), float(time), dtype=torch.float64, device=x.device)
+        T = T.contiguous()
+        out = torch.empty_like(x)
+        res = torch.empty((n, m), dtype=torch.float32, device=x.device)
+        check(_native.lib().agama_integrateOrbitsTargetManyDevice(
+            potential.handle, n, _dev_ptr(x), _dev_ptr(T), float(Omega), float(accuracy), int(maxNumSteps),
+            target._h, _dev_ptr(res), _dev_ptr(out), None, None, _current_stream()))
+        return out, res
+    x = np.ascontiguousarray(ic, dtype=np.float64).reshape(-1, 6)
+    n = len(x)
+    T = np.ascontiguousarray(np.broadcast_to(np.asarray(time, dtype=np.float64), (n,)))
+    out = np.empty((n, 6))
+    res = np.empty((n, m), dtype=np.float32)
+    check(_native.lib().agama_integrateOrbitsTargetMany(
+        potential.handle, n, ptr(x), ptr(T), float(Omega), float(accuracy), int(maxNumSteps), target._h,
+        res.ctypes.data_as(_native.F), ptr(out), None, None))
+    return out, res
+
+
 def orbit(potential, ic, time, Omega=0.0, accuracy=1e-8, maxNumSteps=0, queue=True, info=False):
     """Integrate orbits; returns the final phase-space points (n x 6), and with info=True also
     a dict with the accepted step counts, rejected attempts and statuses
@@ -90,6 +150,12 @@ def set_orbit_lanes(lanes=0):
     check(_native.lib().agama_setOrbitLanesPerOrbit(int(lanes)))
 
 
+def set_orbit_block(block=0):
+    """threads per block of the orbit kernels: 32, 64, 128, or 0 (autotuned with the lanes, the
+    default); no setting changes a result"""
+    check(_native.lib().agama_setOrbitBlockSize(int(block)))
+
+
 class OrbitGraph:
     """an orbit batch over CUDA tensors captured once in a CUDA graph; launch() replays it on the
     current stream (with final is ic, every launch continues the orbits for another T)"""
@@ -116,6 +182,10 @@ class OrbitGraph:
     @property
     def lanes(self):
         return _native.lib().agama_orbitGraphLanes(self._h)
+
+    @property
+    def block(self):
+        return _native.lib().agama_orbitGraphBlockSize(self._h)
 
     def launch(self):
         from . import _current_stream

@@ -338,7 +338,7 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
         line = {"metric": "orbit-steps/s", "value": nst / (t / 1000), "unit": "accepted DOP853 steps/s",
                 "ms_per_step": t, "config": name, "steps": steps, "warmup": warm, "accepted_steps": nst,
                 "rejected_attempts": nrej, "gpu_launches_per_step": 1, "launch": "CUDA graph",
-                "lanes_per_orbit": graph.lanes,
+                "lanes_per_orbit": graph.lanes, "block": graph.block,
                 "roofline": fp64_roofline("dop853Kernel", FLOPS[key], "accepted step", nst, t, peak64, FLOPS_SOURCE)}
         if mx:
             line["orbits_at_step_cap"] = float(np.mean(status == 1))
@@ -363,7 +363,7 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
                 "ms_per_step": t5, "config": "config 5: all %d orbits x 100 T_circ, Spheroid + disk Multipole "
                 "lmax 12 / 80 nodes, DOP853 1e-8 (FP64: one harmonic, so the FP32 m != 0 mode has nothing to do)"
                 % ORBIT5_ORBITS, "steps": 2, "warmup": 1, "accepted_steps": nst5,
-                "gpu_launches_per_step": 1, "launch": "CUDA graph", "lanes_per_orbit": graph5.lanes,
+                "gpu_launches_per_step": 1, "launch": "CUDA graph", "lanes_per_orbit": graph5.lanes, "block": graph5.block,
                 "roofline": fp64_roofline("dop853Kernel", FLOPS["orbits5"], "accepted step", nst5, t5, peak64,
                                           FLOPS_SOURCE)})
     line5 = {"metric": "actions/s", "value": ORBIT5_ORBITS / (ta / 1000), "unit": "actions/s", "ms_per_step": ta,
@@ -372,33 +372,33 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
              "roofline": fp64_roofline("fudge kernels (3)", FLOPS["actions5"], "action", ORBIT5_ORBITS, ta, peak64,
                                        FLOPS_SOURCE)}
     out.append(line5)
-    # learned brackets on the snapshot: the network trained on the orbits' initial points (the same
-    # distribution, other points), then used on the final points
+    # the north star's forms on the snapshot: the network trained on the orbits' initial points (the
+    # same distribution, other points), then used on the final points
     t0 = time.perf_counter()
     af5.train_brackets(ic5[:1000000], epochs=20, batch=2048, lr=2e-3, seed=1)
     ttrain5 = time.perf_counter() - t0
-    af5.use_brackets(True)
-    tl, J5l = timed(lambda: af5(snap), 3, 5)
-    af5.bracket_stats(reset=True)
-    J5l = af5(snap)
-    st5 = af5.bracket_stats(reset=True)
     af5.use_brackets(False)
-    out.append({"metric": "actions/s", "mode": "learned root brackets (BF16 tcgen05 network + FP64 searches)",
-                "value": ORBIT5_ORBITS / (tl / 1000), "unit": "actions/s", "ms_per_step": tl,
-                "config": "config 5: actions of the final snapshot, learned root brackets",
-                "plain_fp64": {"value": ORBIT5_ORBITS / (ta / 1000), "ms_per_step": ta}, "speedup_vs_plain": ta / tl,
-                "max_rel_err_vs_plain": rel_action_err(J5l.cpu().numpy(), J5.cpu().numpy())["max"],
-                "seeded_searches": st5["narrowed"] / max(1, st5["searches"]),
-                "fallback_rate": st5["fallbacks"] / max(1, st5["narrowed"]),
-                "training": {"samples": 1000000, "epochs": 20, "seconds": ttrain5, "points": "the orbits' initial points"},
-                "steps": 5, "warmup": 3, "gpu_launches_per_step": 4})
+
+    def rel_err(J, Jref):
+        e = rel_action_err(J.cpu().numpy(), Jref.cpu().numpy())
+        return e["max"], e["q999"]
+    out5 = action_mode_lines(agama_b200, timed_ms(timed), rel_err, af5, snap, J5,
+                             "config 5: actions of the final snapshot of those orbits",
+                             {"samples": 1000000, "epochs": 20, "seconds": ttrain5,
+                              "points": "the orbits' initial points"})
     del graph5
     if cpu:
         for line, (base, parity) in zip(out, reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5, engine_res)):
             line["cpu_baseline"] = base
             if parity is not None:
                 line["max_rel_err_vs_reference" if "max" in parity else "vs_reference"] = parity
-    return out + mixed_lines
+    return out + out5 + mixed_lines
+
+
+def timed_ms(timed):
+    """the (time, result) timer of the secondary workloads as a time-only timer with 3 warm-up
+    steps and 5 timed steps"""
+    return lambda fn, warmup=3, steps=5: timed(fn, warmup, steps)[0]
 
 
 def mixed_orbit_entry(agama_b200, timed, pot, dic, dT, Om, mx, warm, steps, name, graph64, t64):
@@ -487,29 +487,47 @@ def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
     cases.append(("config 4: 1e7 particles of the config-1 distribution, config-1 potential made axisymmetric "
                   "(lmax 6, 50 nodes)", af4, d4, J4plain, ttrain4, 2000000))
     for name, af, d, Jplain, ttrain, ntrain in cases:
-        n = d.shape[0]
-        af.use_brackets(False)
-        tp = timed(lambda: af(d))
-        af.bracket_stats(reset=True)
-        af(d)
-        plain = af.bracket_stats(reset=True)
-        af.use_brackets(True)
-        tl = timed(lambda: af(d))
-        af.bracket_stats(reset=True)
-        J = af(d)
-        learned = af.bracket_stats(reset=True)
+        out += action_mode_lines(agama_b200, timed, rel_err, af, d, Jplain, name,
+                                 {"samples": ntrain, "epochs": 20, "seconds": ttrain})
+    return out
+
+
+def action_mode_lines(agama_b200, timed, rel_err, af, d, Jplain, name, training):
+    """the same action batch in the north star's forms beside the plain FP64 one: mixed precision
+    (FP32 integrand arithmetic and compensated sums), learned root brackets (BF16 tcgen05 network +
+    FP64 searches), and both; each with its speed-up over plain FP64 and its error against it"""
+    n = d.shape[0]
+    out = []
+    af.use_brackets(False)
+    tp = timed(lambda: af(d))
+    af.bracket_stats(reset=True)
+    af(d)
+    plain = af.bracket_stats(reset=True)
+    for mode, mixed, learned in (("mixed precision (FP32 integrands, compensated FP32 sums; FP64 potential and roots)",
+                                  True, False),
+                                 ("learned root brackets (BF16 tcgen05 network + FP64 searches)", False, True),
+                                 ("mixed precision + learned root brackets", True, True)):
+        agama_b200.set_action_precision(mixed)
+        af.use_brackets(learned)
+        try:
+            tl = timed(lambda: af(d))
+            af.bracket_stats(reset=True)
+            J = af(d)
+            st = af.bracket_stats(reset=True)
+        finally:
+            agama_b200.set_action_precision(False)
+            af.use_brackets(False)
         emax, e999 = rel_err(J, Jplain)
-        out.append({"metric": "actions/s", "mode": "learned root brackets (BF16 tcgen05 network + FP64 searches)",
-                    "value": n / (tl / 1000), "unit": "actions/s", "ms_per_step": tl, "config": name,
-                    "plain_fp64": {"value": n / (tp / 1000), "ms_per_step": tp},
-                    "speedup_vs_plain": tp / tl,
-                    "max_rel_err_vs_plain": emax, "rel_err_vs_plain_q999": e999,
-                    "seeded_searches": learned["narrowed"] / max(1, learned["searches"]),
-                    "fallback_rate": learned["fallbacks"] / max(1, learned["narrowed"]),
-                    "root_iterations_vs_plain": learned["iterations"] / max(1, plain["iterations"]),
-                    "training": {"samples": ntrain, "epochs": 20, "seconds": ttrain},
-                    "steps": 5, "warmup": 3, "gpu_launches_per_step": 4})
-        af.use_brackets(False)
+        line = {"metric": "actions/s", "mode": mode, "value": n / (tl / 1000), "unit": "actions/s",
+                "ms_per_step": tl, "config": name, "plain_fp64": {"value": n / (tp / 1000), "ms_per_step": tp},
+                "speedup_vs_plain": tp / tl, "max_rel_err_vs_plain": emax, "rel_err_vs_plain_q999": e999,
+                "steps": 5, "warmup": 3, "gpu_launches_per_step": 4 if learned else 3}
+        if learned:
+            line.update({"seeded_searches": st["narrowed"] / max(1, st["searches"]),
+                         "fallback_rate": st["fallbacks"] / max(1, st["narrowed"]),
+                         "root_iterations_vs_plain": st["iterations"] / max(1, plain["iterations"]),
+                         "training": training})
+        out.append(line)
     return out
 
 

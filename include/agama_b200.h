@@ -96,6 +96,18 @@ int agama_getPotentialInfo(const agama_Potential* potential, int* lmax, int* mma
 int agama_inspectMultipoleFile(const char* file, int* lmax, int* mmax, int* symmetry,
     int* gridSizeR, int* gridSizeTau);
 
+/* reference: writePotential(fileName, potential), src/potential_factory.h:290-300, which for a
+   Multipole writes writePotentialMultipole's text (src/potential_factory.cpp:909-930): the
+   coefficient file of a potential, readable by the reference's readPotential / createPotential
+   and by agama_createPotential("file=...").  Numbers are written with 17 significant digits
+   (the reference writes 11-22), so the file reproduces the potential's coefficients exactly. */
+int agama_writePotential(const char* fileName, const agama_Potential* potential);
+
+/* The same file from coefficient arrays (layout as agama_createMultipoleFromCoefs), host-only:
+   no device is needed. */
+int agama_writeMultipoleCoefs(const char* fileName, int gridSizeR, const double* radii, int numCoefs,
+    const double* Phi, const double* dPhi);
+
 /* Batched potential / gradient / Hessian at n points, host buffers (any output may be NULL).
    Replaces n calls of agama_evalPotential (src/interface_c.cpp:68-90); the reference batches
    the same call in Python, BatchFunction over BasePotential::eval (src/interface_python.cpp:1405-1485,
@@ -150,6 +162,11 @@ int agama_integrateOrbitsMany(const agama_Potential* potential, long n, const do
    stream capture.  Applies to the orbit entry points below except the allocation-free one. */
 int agama_setOrbitLanesPerOrbit(int lanes);
 
+/* Threads per block of the orbit kernels (no reference counterpart): 32, 64 or 128, or 0
+   (default) to let the library choose together with the lanes per orbit, by the same timing trial
+   (every lane count times every block size).  Neither setting changes any result bit. */
+int agama_setOrbitBlockSize(int block);
+
 /* Mixed precision for orbit batches (no reference counterpart): 1 evaluates the non-axisymmetric
    (m != 0) harmonics of multi-harmonic Multipole potentials from an FP32 copy of the spline table,
    with the radial m = 0 part, the azimuthal sums, the integrator state, its stages and its error
@@ -160,9 +177,37 @@ int agama_setOrbitLanesPerOrbit(int lanes);
    batches launched or captured afterwards. */
 int agama_setOrbitPrecision(int mixed);
 
+/* Runtime functions of orbits: a target that accumulates each orbit's time-weighted samples into
+   the basis elements of a classic spheroidal density grid.  reference: galaxymodel::
+   TargetDensityClassic<degree> (src/galaxymodel_densitygrid.h:66-108, :149-238) as created by the
+   Python Target(type='DensityClassicTopHat' (degree 0) or 'DensityClassicLinear' (degree 1),
+   gridr, stripsPerPane, axisRatioY, axisRatioZ) (src/interface_python.cpp:7185-7205), attached to
+   each orbit by RuntimeFncTarget (src/galaxymodel_target.h:99-150; Python orbit(targets=...),
+   src/interface_python.cpp:8114-8121).  gridr: gridSize increasing radii (a leading 0 is
+   dropped); NULL with agama_getError() on invalid parameters. */
+typedef struct agama_Target agama_Target;
+agama_Target* agama_createTargetDensityClassic(int degree, int stripsPerPane, int gridSize, const double* gridr,
+    double axisRatioY, double axisRatioZ);
+void agama_deleteTarget(agama_Target* target);
+/* number of basis elements (values recorded per orbit) */
+int agama_targetNumCoefs(const agama_Target* target);
+
+/* Orbits as agama_integrateOrbitsManyDevice (work queue) with the target's runtime function:
+   every accepted step adds 10 points of its dense output, at the middles of equal sub-steps and
+   in the frame of the potential, each weighted by the sub-step's duration, to the orbit's row;
+   at the end the row is converted to FP32 and divided by the integration time
+   (RuntimeFncTarget::processTimestep and its destructor).  output: n x numCoefs floats. */
+int agama_integrateOrbitsTargetManyDevice(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, const agama_Target* target, float* output,
+    double* finalState, long* numSteps, int* status, void* stream);
+/* The same on host buffers (finalState, numSteps, status may be NULL). */
+int agama_integrateOrbitsTargetMany(const agama_Potential* potential, long n, const double* ic,
+    const double* T, double Omega, double accuracy, long maxNumSteps, const agama_Target* target, float* output,
+    double* finalState, long* numSteps, int* status);
+
 /* An orbit batch captured once in a CUDA graph (no reference counterpart): the work-counter reset
-   and the persistent DOP853 kernel over the given device buffers, with the lanes per orbit settled
-   (autotuner trial) before the capture.  Each agama_orbitGraphLaunch replays the batch on the
+   and the persistent DOP853 kernel over the given device buffers, with the lanes per orbit and
+   the block size settled (autotuner trial) before the capture.  Each agama_orbitGraphLaunch replays the batch on the
    stream, reading the current contents of ic and T: with finalState == ic every launch continues
    the orbits for another T (each orbit reads its start before writing its end).  The buffers
    must stay valid while the graph exists. */
@@ -172,6 +217,7 @@ agama_OrbitGraph* agama_orbitGraphCreate(const agama_Potential* potential, long 
     int* status);
 int agama_orbitGraphLaunch(agama_OrbitGraph* graph, void* stream);
 int agama_orbitGraphLanes(const agama_OrbitGraph* graph);
+int agama_orbitGraphBlockSize(const agama_OrbitGraph* graph);
 void agama_orbitGraphDelete(agama_OrbitGraph* graph);
 
 /* Orbits with their trajectories sampled at trajSize (>= 2) regular times t_k = k T/(trajSize-1)
@@ -214,6 +260,14 @@ int agama_integrateOrbitsManyDevice(const agama_Potential* potential, long n, co
 int agama_integrateOrbitsManyDeviceNoAlloc(const agama_Potential* potential, long n, const double* ic,
     const double* T, double Omega, double accuracy, long maxNumSteps, double* finalState,
     long* numSteps, long* numRejected, int* status, int queueSlot, void* stream);
+
+/* Mixed precision for the Staeckel-fudge action integrals (no reference counterpart): 1 computes
+   the integrand after F(tau) (p^2 = F / (2 (tau - Delta^2)^2 tau), its square root, the
+   end-point stretch) and the Gauss-Legendre sums in FP32, the sums compensated (Kahan), while the
+   potential, F(tau), the integrals of motion and the turning-point root searches stay FP64;
+   0 (default) is all FP64.  The actions then differ from FP64 by about 1e-7 relative.  Applies to
+   the action entry points without angles / frequencies called afterwards. */
+int agama_setActionPrecision(int mixed);
 
 /* ---------------------------------------------------------------------------------------
    Staeckel-fudge actions (axisymmetric potentials only).  posvel: n x 6 Cartesian points;

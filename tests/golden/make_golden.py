@@ -15,6 +15,8 @@ It writes, into tests/golden/:
   actions_<name>.npz     phase-space points with the reference's Staeckel-fudge actions (fixed
                          focal distance and through ActionFinderAxisymFudge), plus the finder's
                          focal-distance table and L_circ(E) spline;
+  target_<name>.npz      the reference's density-grid targets (runtime functions) of the golden
+                         orbits (configs 1 and 3);
   utils_<name>.npz       density at the potential_<name> points and R_circ(E), R_max(E),
                          R_from_Lz(L), peri/apocentre radii of (E, L), through the reference's
                          plain-C interface.
@@ -202,6 +204,29 @@ def make_more_orbit_vectors():
                                                             potential_fn(ic[:, :3]) + 0.5 * np.sum(ic[:, 3:] ** 2, 1))).max())
 
 
+def make_target_vectors():
+    """runtime functions of orbits: the reference's orbit(..., targets=[Target(...)]) (its
+    RuntimeFncTarget with TargetDensityClassic) on the config-1 and config-3 golden orbits:
+    target_<name>.npz holds the grid parameters and the float32 matrices (orbits x cells)"""
+    import agama
+    for name, grids in (("cfg1", [("DensityClassicTopHat", 2, 0.8, 0.6), ("DensityClassicLinear", 3, 1.0, 1.0)]),
+                        ("cfg3", [("DensityClassicTopHat", 3, 0.7, 0.5)])):
+        g = np.load(os.path.join(HERE, "orbits_%s.npz" % name))
+        pot = agama.Potential(file=coef_path(name))
+        gridr = np.array([0, 0.1, 0.25, 0.5, 1, 2, 4, 8, 16.0])
+        out = dict(ic=g["ic"], T=g["T"], Omega=g["Omega"], accuracy=g["accuracy"], gridr=gridr)
+        for k, (typ, strips, qy, qz) in enumerate(grids):
+            t = agama.Target(type=typ, gridr=gridr, stripsPerPane=strips, axisRatioY=qy, axisRatioZ=qz)
+            m = agama.orbit(potential=pot, ic=g["ic"], time=g["T"], Omega=float(g["Omega"]), targets=[t],
+                            accuracy=float(g["accuracy"]))
+            out["type%d" % k] = typ
+            out["strips%d" % k] = strips
+            out["axes%d" % k] = np.array([qy, qz])
+            out["result%d" % k] = np.asarray(m)
+            print(name, typ, np.asarray(m).shape)
+        np.savez_compressed(os.path.join(HERE, "target_%s.npz" % name), **out)
+
+
 def action_points(pot, n, seed, Rd=3.0, hz=0.3):
     """disk-like points of the benchmark distribution plus edge cases: in the plane (z = 0),
     no rotation (Lz = 0), counter-rotating, nearly circular, on the z axis, unbound"""
@@ -283,6 +308,8 @@ if __name__ == "__main__":
         make_orbit_vectors()
     if what in ("orbits", "more_orbits", "all"):
         make_more_orbit_vectors()
+    if what in ("targets", "all"):
+        make_target_vectors()
     if what in ("actions", "all"):
         make_action_vectors()
     if what in ("utils", "all"):

@@ -126,3 +126,25 @@ def test_actions_reject_non_axisymmetric():
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
     with pytest.raises(RuntimeError, match="axisymmetric"):
         agama_b200.actions(pot, np.ones((2, 6)), fd=1.0)
+
+
+@pytest.mark.parametrize("cfg", CFGS)
+def test_action_finder_mixed_precision(cfg):
+    """FP32 integrand arithmetic and compensated FP32 Gauss-Legendre sums (F(tau), the potential
+    and the roots in FP64): within the 1e-6 bound of the reference, and within 1e-6 of the FP64
+    form (measured on B200: a few 1e-7 at most, reported here per configuration)"""
+    import agama_b200
+    g = np.load(os.path.join(GOLDEN, "actions_%s.npz" % cfg))
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    af = agama_b200.ActionFinder(pot, tables=tables(g))
+    J64 = af(g["points"])
+    agama_b200.set_action_precision(True)
+    try:
+        J32 = af(g["points"])
+    finally:
+        agama_b200.set_action_precision(False)
+    assert not np.array_equal(J32, J64, equal_nan=True)          # the mixed path did run
+    check_actions(J32, g["act_finder"])
+    err = check_actions(J32, J64)
+    print(cfg, "mixed-precision actions vs FP64: max relative error %.3g" % err)
+    assert np.array_equal(af(g["points"]), J64, equal_nan=True)  # the setting is off again

@@ -69,6 +69,21 @@ def test_reference_rotating_frame_and_trajectories_reproduce_golden():
 
 
 @needs_ref
+def test_reference_targets_reproduce_golden():
+    """the reference's orbit(..., targets=[Target]) through its own Python module built here"""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(ref.__file__), "_ref"))
+    import agama
+    g = np.load(os.path.join(GOLDEN, "target_cfg1.npz"))
+    pot = agama.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
+    qy, qz = g["axes0"]
+    t = agama.Target(type=str(g["type0"]), gridr=g["gridr"], stripsPerPane=int(g["strips0"]), axisRatioY=qy,
+                     axisRatioZ=qz)
+    m = agama.orbit(potential=pot, ic=g["ic"][:4], time=g["T"][:4], targets=[t], accuracy=float(g["accuracy"]))
+    np.testing.assert_array_equal(np.asarray(m), g["result0"][:4])
+
+
+@needs_ref
 def test_reference_angles_reproduce_golden():
     g = np.load(os.path.join(GOLDEN, "actions_cfg5.npz"))
     pot = ref.Potential(file=os.path.join(GOLDEN, "cfg5.coef"))

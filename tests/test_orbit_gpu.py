@@ -73,21 +73,26 @@ def test_orbit_parity(cfg, queue, lanes):
     assert np.all(drift[ok] <= np.maximum(10 * drift_ref[ok], 1e-9)), (drift[ok].max(), drift_ref[ok].max())
 
 
-@pytest.mark.parametrize("cfg", ["cfg1", "cfg3"])
-def test_orbit_bits_independent_of_lanes(cfg):
-    """every lane count gives the same bits (the harmonics of a lane group are summed in one
-    order), so the autotuner's timing-based choice never changes a result"""
+@pytest.mark.parametrize("cfg", ["cfg1", "cfg3", "cfg5"])
+def test_orbit_bits_independent_of_launch_shape(cfg):
+    """every lane count and block size gives the same bits (the harmonics of a lane group are
+    summed in one order; the block only groups orbits), so the autotuner's timing-based choice
+    never changes a result"""
     import agama_b200
     g = np.load(os.path.join(GOLDEN, "orbits_%s.npz" % cfg))
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
     results = []
-    for lanes in (1, 2, 4, 8):
-        agama_b200.set_orbit_lanes(lanes)
-        try:
-            results.append(agama_b200.orbit(pot, g["ic"], g["T"], Omega=float(g["Omega"]),
-                                            accuracy=float(g["accuracy"]), info=True))
-        finally:
-            agama_b200.set_orbit_lanes(0)
+    lane_counts = (1, 2, 4, 8) if cfg != "cfg5" else (1,)
+    for lanes in lane_counts:
+        for block in (32, 64, 128):
+            agama_b200.set_orbit_lanes(lanes)
+            agama_b200.set_orbit_block(block)
+            try:
+                results.append(agama_b200.orbit(pot, g["ic"], g["T"], Omega=float(g["Omega"]),
+                                                accuracy=float(g["accuracy"]), info=True))
+            finally:
+                agama_b200.set_orbit_lanes(0)
+                agama_b200.set_orbit_block(0)
     for final, info in results[1:]:
         assert np.array_equal(final, results[0][0])
         assert np.array_equal(info["steps"], results[0][1]["steps"])
@@ -163,7 +168,7 @@ def test_orbit_graph_replays_and_continues():
     T = torch.tensor(g["T"][ok], device="cuda")
     direct = agama_b200.orbit(pot, ic, T)
     graph = agama_b200.OrbitGraph(pot, ic, T)
-    assert graph.lanes in (1, 2, 4, 8)
+    assert graph.lanes in (1, 2, 4, 8) and graph.block in (32, 64, 128)
     once = graph.launch()
     torch.cuda.synchronize()
     assert torch.equal(once, direct)
