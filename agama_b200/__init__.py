@@ -64,17 +64,48 @@ def _points(a, ncol):
     return a, single
 
 
+def _key_values(d):
+    """a dict of parameters as the reference's key=value string"""
+    return ", ".join("%s=%s" % (k, repr(float(v)) if isinstance(v, float) else v) for k, v in d.items())
+
+
+def multipole_coefs_from_density(density, **params):
+    """the coefficients (radii, Phi, dPhi; Phi and dPhi numCoefs x gridSizeR) of the Multipole that
+    Potential(type='Multipole', density=..., **params) builds, computed on the host (no device)"""
+    comps = density if isinstance(density, (list, tuple)) else [density]
+    dens = (ctypes.c_char_p * len(comps))(*[_key_values(d).encode() for d in comps])
+    L = _native.lib()
+    nr, nc = ctypes.c_int(0), ctypes.c_int(0)
+    mp = _key_values(params).encode()
+    check(L.agama_multipoleCoefsFromDensities(mp, len(comps), dens, ctypes.byref(nr), ctypes.byref(nc), None, None,
+                                              None))
+    r = np.zeros(nr.value)
+    P = np.zeros((nc.value, nr.value))
+    D = np.zeros_like(P)
+    check(L.agama_multipoleCoefsFromDensities(mp, len(comps), dens, ctypes.byref(nr), ctypes.byref(nc),
+                                              ptr(r), ptr(P), ptr(D)))
+    return r, P, D
+
+
 class Potential:
     """A Multipole potential resident on the current CUDA device.
 
     Potential(file='coefs.ini')                     -- coefficient file of the reference format
     Potential(type='Multipole', file='coefs.ini')
     Potential(radii=r, Phi=P, dPhi=dP)              -- arrays as in Multipole(gridRadii, Phi, dPhi)
+    Potential(type='Multipole', density=dict(type='Dehnen', mass=1, ...), lmax=6, gridSizeR=50, ...)
+                                                    -- the Poisson solve from a density model (or a
+                                                       list of them, summed), as the reference's
+                                                       Potential(type='Multipole', density=...)
     """
 
-    def __init__(self, file=None, type="Multipole", radii=None, Phi=None, dPhi=None):
+    def __init__(self, file=None, type="Multipole", radii=None, Phi=None, dPhi=None, density=None, **params):
         L = _native.lib()
-        if file is not None:
+        if density is not None:
+            comps = density if isinstance(density, (list, tuple)) else [density]
+            dens = (ctypes.c_char_p * len(comps))(*[_key_values(d).encode() for d in comps])
+            h = L.agama_createMultipoleFromDensities(_key_values(params).encode(), len(comps), dens)
+        elif file is not None:
             params = "type=%s, file=%s" % (type, file)
             h = L.agama_createPotential(params.encode())
         elif radii is not None:

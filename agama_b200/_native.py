@@ -21,6 +21,9 @@ SIGNATURES = {
     "agama_createPotential": (VP, [ctypes.c_char_p]),
     "agama_deletePotential": (None, [VP]),
     "agama_evalPotential": (ctypes.c_double, [VP, D, ctypes.c_double, D, D]),
+    "agama_createMultipoleFromDensities": (VP, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]),
+    "agama_multipoleCoefsFromDensities": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int,
+                                                         ctypes.POINTER(ctypes.c_char_p), I, I, D, D, D]),
     "agama_createMultipoleFromCoefs": (VP, [ctypes.c_int, D, ctypes.c_int, D, D]),
     "agama_getPotentialInfo": (ctypes.c_int, [VP, I, I, I, I, I]),
     "agama_inspectMultipoleFile": (ctypes.c_int, [ctypes.c_char_p, I, I, I, I, I]),

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <sstream>
 #include <cctype>
+#include <map>
 
 using namespace agb;
 
@@ -24,27 +25,66 @@ std::string trimStr(const std::string& s) {
 }
 std::string lowerStr(std::string s) { for(auto& c : s) c = static_cast<char>(tolower(c)); return s; }
 
-/// the subset of the reference's key=value potential parameters this engine accepts:
-/// "file=<Multipole coefficient file>" with an optional "type=Multipole"
-std::string coefFileFromParams(const char* params)
+/// key=value pairs of a parameter string ("key=value, key=value" or separated by newlines /
+/// semicolons), keys in lower case (the reference's KeyValueMap, case-insensitive keys)
+std::map<std::string, std::string> parseKeyValues(const char* params)
+{
+    std::map<std::string, std::string> kv;
+    std::string text = params ? params : "";
+    for(auto& c : text) if(c == ';' || c == '\n') c = ',';
+    std::stringstream ss(text);
+    std::string item;
+    while(std::getline(ss, item, ',')) {
+        const size_t eq = item.find('=');
+        if(eq == std::string::npos) continue;
+        kv[lowerStr(trimStr(item.substr(0, eq)))] = trimStr(item.substr(eq + 1));
+    }
+    return kv;
+}
+
+/// the Multipole's own parameters; every other key describes the density
+const char* const MULTIPOLE_KEYS[] = { "type", "lmax", "mmax", "gridsizer", "rmin", "rmax", "symmetry", "fixorder",
+    "density", "file" };
+
+bool isMultipoleKey(const std::string& k)
+{
+    for(const char* m : MULTIPOLE_KEYS) if(k == m) return true;
+    return false;
+}
+
+/** a potential from the reference's key=value parameters (createPotential for a single section,
+    src/potential_factory.cpp:1376-1441, as the plain-C agama_createPotential passes them,
+    src/interface_c.cpp:31-51): "file=<Multipole coefficient file>" (type=Multipole optional),
+    or "type=Multipole, density=<Dehnen|Plummer|NFW|MiyamotoNagai|Spheroid|Disk>, <density
+    parameters>, lmax, mmax, gridSizeR, rmin, rmax, symmetry" (the Poisson solve) */
+DevicePotential* potentialFromParams(const char* params)
 {
     if(!params) throw std::invalid_argument("createPotential: null parameter string");
-    std::stringstream ss(params);
-    std::string item, file, type;
-    while(std::getline(ss, item, ',')) {
-        size_t eq = item.find('=');
-        if(eq == std::string::npos) continue;
-        std::string key = lowerStr(trimStr(item.substr(0, eq))), val = trimStr(item.substr(eq + 1));
-        if(key == "file") file = val;
-        else if(key == "type") type = lowerStr(val);
-        else throw std::invalid_argument("createPotential: parameter '" + key +
-            "' is not supported by the B200 engine (supply a Multipole coefficient file)");
-    }
+    const std::map<std::string, std::string> kv = parseKeyValues(params);
+    auto typeIt = kv.find("type");
+    const std::string type = typeIt == kv.end() ? "" : lowerStr(typeIt->second);
     if(!type.empty() && type != "multipole")
-        throw std::invalid_argument("createPotential: only type=Multipole is supported");
-    if(file.empty())
-        throw std::invalid_argument("createPotential: no coefficient file given");
-    return file;
+        throw std::invalid_argument("createPotential: only type=Multipole is supported (from a coefficient file or "
+            "a density model)");
+    std::vector<double> radii;
+    std::vector<std::vector<double>> Phi, dPhi;
+    if(kv.count("file")) {
+        for(const auto& e : kv)
+            if(e.first != "file" && e.first != "type")
+                throw std::invalid_argument("createPotential: parameter '" + e.first + "' is not used with file=");
+        readMultipoleCoefFile(kv.at("file"), radii, Phi, dPhi);
+    } else if(kv.count("density")) {
+        std::map<std::string, std::string> dens, mp;
+        for(const auto& e : kv) {
+            if(e.first == "density") dens["type"] = e.second;
+            else if(isMultipoleKey(e.first)) mp[e.first] = e.second;
+            else dens[e.first] = e.second;
+        }
+        multipoleCoefsFromDensity({ dens }, mp, radii, Phi, dPhi);
+    } else
+        throw std::invalid_argument("createPotential: give a coefficient file (file=...) or a density model "
+            "(density=...)");
+    return createDevicePotential(radii, Phi, dPhi);
 }
 
 /// restores the caller's current device when an entry point returns (the entry points make the
@@ -73,14 +113,55 @@ const char* agama_getError() { return lastError(); }
 agama_Potential* agama_createPotential(const char* params)
 {
     try {
+        return new agama_Potential{ potentialFromParams(params) };
+    } catch(std::exception& e) {
+        setError(e.what());
+        return nullptr;
+    }
+}
+
+agama_Potential* agama_createMultipoleFromDensities(const char* multipoleParams, int numComponents,
+    const char* const* densityParams)
+{
+    try {
+        if(numComponents < 1 || !densityParams) throw std::invalid_argument("createMultipoleFromDensities: no density");
         std::vector<double> radii;
         std::vector<std::vector<double>> Phi, dPhi;
-        readMultipoleCoefFile(coefFileFromParams(params), radii, Phi, dPhi);
+        std::vector<std::map<std::string, std::string>> dens;
+        for(int k = 0; k < numComponents; k++) dens.push_back(parseKeyValues(densityParams[k]));
+        multipoleCoefsFromDensity(dens, parseKeyValues(multipoleParams), radii, Phi, dPhi);
         return new agama_Potential{ createDevicePotential(radii, Phi, dPhi) };
     } catch(std::exception& e) {
         setError(e.what());
         return nullptr;
     }
+}
+
+int agama_multipoleCoefsFromDensities(const char* multipoleParams, int numComponents,
+    const char* const* densityParams, int* gridSizeR, int* numCoefs, double* radii, double* Phi, double* dPhi)
+{
+    // host-only: the Poisson solve without a device; call with radii == NULL to get the sizes
+    return guarded([&] {
+        if(numComponents < 1 || !densityParams || !gridSizeR || !numCoefs)
+            throw std::invalid_argument("multipoleCoefsFromDensities: invalid arguments");
+        std::vector<double> r;
+        std::vector<std::vector<double>> P, D;
+        std::vector<std::map<std::string, std::string>> dens;
+        for(int k = 0; k < numComponents; k++) dens.push_back(parseKeyValues(densityParams[k]));
+        multipoleCoefsFromDensity(dens, parseKeyValues(multipoleParams), r, P, D);
+        const int nr = static_cast<int>(r.size()), nc = static_cast<int>(P.size());
+        if(radii) {
+            if(*gridSizeR < nr || *numCoefs < nc || !Phi || !dPhi)
+                throw std::invalid_argument("multipoleCoefsFromDensities: output arrays too small");
+            std::copy(r.begin(), r.end(), radii);
+            for(int c = 0; c < nc; c++) {
+                std::copy(P[c].begin(), P[c].end(), Phi + static_cast<size_t>(c) * nr);
+                std::copy(D[c].begin(), D[c].end(), dPhi + static_cast<size_t>(c) * nr);
+            }
+        }
+        *gridSizeR = nr;
+        *numCoefs = nc;
+    });
 }
 
 agama_Potential* agama_createMultipoleFromCoefs(int gridSizeR, const double* radii, int numCoefs,

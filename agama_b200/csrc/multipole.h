@@ -8,6 +8,7 @@
 #pragma once
 #include <vector>
 #include <string>
+#include <map>
 #include "common.cuh"
 
 namespace agb {
@@ -95,6 +96,14 @@ void readMultipoleCoefFile(const std::string& fileName, std::vector<double>& rad
 /// significant digits so that reading the file back gives the same doubles
 void writeMultipoleCoefFile(const std::string& fileName, const std::vector<double>& radii,
     const std::vector<std::vector<double>>& Phi, const std::vector<std::vector<double>>& dPhi, int symmetry);
+
+/** the coefficients of a Multipole built from density models (the Poisson solve of the
+    reference's createMultipole, src/potential_multipole.cpp:1400-1441): densities = key=value
+    parameters of each component (type, mass, scaleRadius, ...; summed), params = the Multipole's
+    own (lmax, mmax, gridSizeR, rmin, rmax, symmetry, fixOrder); keys in lower case */
+void multipoleCoefsFromDensity(const std::vector<std::map<std::string, std::string>>& densities,
+    const std::map<std::string, std::string>& params, std::vector<double>& radii,
+    std::vector<std::vector<double>>& Phi, std::vector<std::vector<double>>& dPhi);
 
 // helpers shared with the action-finder construction
 double lambertW(double x, bool lowerBranch);

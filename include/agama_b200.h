@@ -32,7 +32,9 @@ const char* agama_getError(void);
 
 /* reference: agama_createPotential, src/interface_c.h:45 (src/interface_c.cpp:31-51).
    Accepts "file=<coefficient file>" (optionally with "type=Multipole"): a Multipole potential
-   stored by the reference's writePotential (src/potential_factory.cpp:909-930). */
+   stored by the reference's writePotential (src/potential_factory.cpp:909-930); or
+   "type=Multipole, density=<model>, <model parameters>, lmax=.., gridSizeR=.., ...": a Multipole
+   built from one density model (see agama_createMultipoleFromDensities). */
 agama_Potential* agama_createPotential(const char* params);
 
 /* reference: agama_deletePotential, src/interface_c.h:51 */
@@ -85,6 +87,25 @@ void agama_findPlanarOrbitExtent(const agama_Potential* potential, double E, dou
    index c = l*(l+1)+m, numCoefs = (lmax+1)^2. */
 agama_Potential* agama_createMultipoleFromCoefs(int gridSizeR, const double* radii, int numCoefs,
     const double* Phi, const double* dPhi);
+
+/* A Multipole built from density models: the Poisson solve of the reference's createMultipole
+   (src/potential_multipole.cpp:1400-1441; chooseGridRadii :369-484, computePotentialCoefsFromSource
+   :1013-1114, restrictSphHarmCoefs :151-185) for the sum of the given densities, each a key=value
+   string as the reference's createDensity takes it (type=Dehnen | Plummer | NFW | MiyamotoNagai |
+   Spheroid | Disk, with mass, scaleRadius, gamma, axisRatioY, axisRatioZ, scaleHeight, alpha,
+   beta, densityNorm, surfaceDensity, outerCutoffRadius, cutoffStrength as they apply);
+   multipoleParams: lmax, mmax, gridSizeR, rmin, rmax (0 = chosen from the density), symmetry,
+   fixOrder.  agama_createPotential accepts the single-density form "type=Multipole,
+   density=<type>, ..." of the reference's plain-C interface (src/interface_c.cpp:31-51). */
+agama_Potential* agama_createMultipoleFromDensities(const char* multipoleParams, int numComponents,
+    const char* const* densityParams);
+
+/* The same Poisson solve on the host only (no device): the coefficients that
+   agama_createMultipoleFromDensities builds the potential from.  Call with radii == NULL to get
+   gridSizeR and numCoefs; then radii[gridSizeR], Phi and dPhi[numCoefs x gridSizeR] (index
+   c = l*(l+1)+m, as agama_createMultipoleFromCoefs takes them). */
+int agama_multipoleCoefsFromDensities(const char* multipoleParams, int numComponents,
+    const char* const* densityParams, int* gridSizeR, int* numCoefs, double* radii, double* Phi, double* dPhi);
 
 /* order, symmetry (coord::SymmetryType bit mask) and grid sizes of a Multipole potential */
 int agama_getPotentialInfo(const agama_Potential* potential, int* lmax, int* mmax, int* symmetry,

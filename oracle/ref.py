@@ -73,6 +73,39 @@ def lib():
     return _lib
 
 
+def multipole_coefs_from_density(multipole_params, densities):
+    """the reference's Multipole::create from the sum of densities (key=value strings), its
+    coefficients at full precision: (radii, Phi, dPhi) with Phi, dPhi numCoefs x gridSizeR"""
+    L = lib()
+    f = L.ref_multipole_from_density
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _I, _I,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    arr = (ctypes.c_char_p * len(densities))(*[d.encode() for d in densities])
+    nr, nc = ctypes.c_int(0), ctypes.c_int(0)
+    _check(f(multipole_params.encode(), len(densities), arr, ctypes.byref(nr), ctypes.byref(nc), None, None, None))
+    r = np.zeros(nr.value)
+    P = np.zeros((nc.value, nr.value))
+    D = np.zeros_like(P)
+    _check(f(multipole_params.encode(), len(densities), arr, ctypes.byref(nr), ctypes.byref(nc),
+             r.ctypes.data, P.ctypes.data, D.ctypes.data))
+    return r, P, D
+
+
+def multipole_potential_from_density(multipole_params, densities):
+    """the reference's Multipole from the sum of densities, in memory, as a Potential"""
+    L = lib()
+    f = L.ref_multipole_potential_from_density
+    f.restype = ctypes.c_void_p
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
+    arr = (ctypes.c_char_p * len(densities))(*[d.encode() for d in densities])
+    h = f(multipole_params.encode(), len(densities), arr)
+    if not h:
+        raise RuntimeError(L.ref_error().decode())
+    p = Potential.__new__(Potential)
+    p.h = h
+    return p
+
+
 def _p(a, t=_D):
     return None if a is None else a.ctypes.data_as(t)
 

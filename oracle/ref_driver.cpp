@@ -33,6 +33,8 @@
 #undef private
 #undef protected
 #include "potential_factory.h"
+#include "potential_composite.h"
+#include "potential_multipole.h"
 #include "potential_base.h"
 #include "orbit.h"
 #include "coord.h"
@@ -442,5 +444,88 @@ int ref_scale(int kind, double a, double b, double u, double* s)
     else if(kind == 1) *s = math::scale(math::ScalingSemiInf(a), u);
     else *s = math::scale(math::ScalingCub(a, b), u);
     return 0;
+}
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// The reference's Poisson solve (checker of the engine's Multipole construction from densities)
+
+namespace potential {
+// defined with external linkage in src/potential_multipole.cpp:1013-1114 (not in its header)
+void computePotentialCoefsFromSource(const BaseDensity& dens, const math::SphHarmIndices& ind,
+    const std::vector<double>& gridRadii, std::vector< std::vector<double> > coefs[2]);
+}
+
+extern "C" {
+/// Multipole::create (src/potential_multipole.cpp:1400-1441) from the sum of the densities given
+/// as key=value strings (createDensity, src/potential_factory.h:31-33) with the Multipole's
+/// parameters (lmax, mmax, gridSizeR, rmin, rmax, symmetry, fixOrder): its coefficients at full
+/// precision (getCoefs).  Call with radii == NULL for the sizes.
+int ref_multipole_from_density(const char* multipoleParams, int ncomp, const char* const* densityParams,
+    int* nr, int* nc, double* radii, double* Phi, double* dPhi)
+{
+    try {
+        std::vector<potential::PtrDensity> comps;
+        for(int k = 0; k < ncomp; k++)
+            comps.push_back(potential::createDensity(utils::KeyValueMap(std::string(densityParams[k]))));
+        potential::PtrDensity dens = ncomp == 1 ? comps[0] :
+            potential::PtrDensity(new potential::CompositeDensity(comps));
+        utils::KeyValueMap mp{std::string(multipoleParams)};
+        const int lmax = mp.getInt("lmax", 6);
+        std::shared_ptr<const potential::Multipole> mul = potential::Multipole::create(*dens,
+            potential::getSymmetryTypeByName(mp.getString("symmetry")), lmax, mp.getInt("mmax", lmax),
+            mp.getInt("gridSizeR", 25), mp.getDouble("rmin", 0), mp.getDouble("rmax", 0), mp.getBool("fixOrder", false));
+        std::vector<double> r;
+        std::vector<std::vector<double> > P, D;
+        mul->getCoefs(r, P, D);
+        if(mp.getBool("raw", false)) {
+            // the coefficients of the Poisson solve itself on the same grid (getCoefs returns the
+            // values re-derived from the spline interpolator), with the source's angular order
+            // (createMultipole, src/potential_multipole.cpp:1418-1432), restricted to the output terms
+            const coord::SymmetryType symSrc = dens->symmetry();
+            int lmaxSrc = std::max<int>(lmax + 6, 12), mmaxSrc = std::max<int>(mp.getInt("mmax", lmax) + 6, 12);
+            if(mp.getBool("fixOrder", false)) { lmaxSrc = lmax; mmaxSrc = mp.getInt("mmax", lmax); }
+            if(isSpherical(symSrc)) lmaxSrc = 0;
+            if(isZRotSymmetric(symSrc)) mmaxSrc = 0;
+            std::vector<std::vector<double> > coefs[2];
+            potential::computePotentialCoefsFromSource(*dens, math::SphHarmIndices(lmaxSrc, mmaxSrc, symSrc), r, coefs);
+            for(size_t c = 0; c < P.size(); c++) {
+                const bool nonzero = !(math::allZeros(P[c]) && math::allZeros(D[c]));
+                P[c] = nonzero && c < coefs[0].size() ? coefs[0][c] : std::vector<double>(r.size(), 0.);
+                D[c] = nonzero && c < coefs[1].size() ? coefs[1][c] : std::vector<double>(r.size(), 0.);
+            }
+        }
+        if(radii) {
+            for(size_t k = 0; k < r.size(); k++) radii[k] = r[k];
+            for(size_t c = 0; c < P.size(); c++)
+                for(size_t k = 0; k < r.size(); k++) {
+                    Phi[c * r.size() + k] = P[c][k];
+                    dPhi[c * r.size() + k] = D[c][k];
+                }
+        }
+        *nr = static_cast<int>(r.size());
+        *nc = static_cast<int>(P.size());
+        return 0;
+    } catch(std::exception& e) { g_error = e.what(); return -1; }
+}
+
+/// the reference's Multipole from the sum of densities, as a potential handle (in memory: its
+/// tables come from the Poisson solve itself, not from a coefficient file)
+void* ref_multipole_potential_from_density(const char* multipoleParams, int ncomp, const char* const* densityParams)
+{
+    try {
+        std::vector<potential::PtrDensity> comps;
+        for(int k = 0; k < ncomp; k++)
+            comps.push_back(potential::createDensity(utils::KeyValueMap(std::string(densityParams[k]))));
+        potential::PtrDensity dens = ncomp == 1 ? comps[0] :
+            potential::PtrDensity(new potential::CompositeDensity(comps));
+        utils::KeyValueMap mp{std::string(multipoleParams)};
+        const int lmax = mp.getInt("lmax", 6);
+        PotHandle* h = new PotHandle;
+        h->pot = potential::Multipole::create(*dens, potential::getSymmetryTypeByName(mp.getString("symmetry")), lmax,
+            mp.getInt("mmax", lmax), mp.getInt("gridSizeR", 25), mp.getDouble("rmin", 0), mp.getDouble("rmax", 0),
+            mp.getBool("fixOrder", false));
+        return h;
+    } catch(std::exception& e) { g_error = e.what(); return NULL; }
 }
 }  // extern "C"

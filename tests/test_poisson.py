@@ -1,0 +1,125 @@
+"""The Multipole from density models (the Poisson solve, agama_multipoleCoefsFromDensities /
+Potential(type='Multipole', density=...)) against the reference's own Multipole::create from the
+same densities (built here: oracle ref_multipole_from_density, full-precision coefficients).
+
+CPU: the radial grid equals the reference's to 1e-14 (it is chosen from the density by the same
+sweep); every coefficient Phi_lm(r_k), dPhi_lm/dr(r_k) agrees with the reference's Poisson solve
+(its computePotentialCoefsFromSource on the same grid) to 1e-12 of |Phi_00| (|dPhi_00/dr|) at that
+radius (differences come from the last bits of the quadrature rules and of the density formulas);
+the same set of non-zero harmonics.  (The reference's getCoefs, and so its coefficient files,
+return the coefficients re-derived from its spline interpolator, which differ from the Poisson
+solve by up to ~1e-7 in dPhi at the innermost node; those are compared to 1e-6.)
+GPU: potentials built from the density on the device evaluate at the golden points within 1e-10
+of the reference's potential built from the same density (outside the innermost grid cell)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+CASES = {
+    "cfg1": ("lmax=6, gridSizeR=50, rmin=1e-3, rmax=1e3, symmetry=triaxial",
+             ["type=Dehnen, mass=1, scaleRadius=1, gamma=1, axisRatioY=0.8, axisRatioZ=0.6"]),
+    "cfg2": ("lmax=8, gridSizeR=60, symmetry=axisymmetric",
+             ["type=MiyamotoNagai, mass=0.1, scaleRadius=3, scaleHeight=0.3", "type=NFW, mass=1, scaleRadius=20"]),
+    "cfg3": ("lmax=8, gridSizeR=64, symmetry=triaxial",
+             ["type=Dehnen, mass=1, scaleRadius=1, gamma=0.5, axisRatioY=0.7, axisRatioZ=0.5"]),
+    "cfg4": ("lmax=6, mmax=0, gridSizeR=50, rmin=1e-3, rmax=1e3, symmetry=axisymmetric",
+             ["type=Dehnen, mass=1, scaleRadius=1, gamma=1, axisRatioY=0.8, axisRatioZ=0.6"]),
+    "cfg5": ("lmax=12, gridSizeR=80, symmetry=axisymmetric",
+             ["type=Spheroid, mass=1, scaleRadius=1, gamma=1, beta=4, axisRatioZ=0.6",
+              "type=Disk, mass=0.05, scaleRadius=3, scaleHeight=0.3"]),
+    "quad": ("lmax=2, gridSizeR=30, symmetry=triaxial",
+             ["type=Dehnen, mass=1, scaleRadius=1, gamma=1.5, axisRatioY=0.7, axisRatioZ=0.5"]),
+    "sph": ("lmax=0, gridSizeR=25", ["type=Plummer, mass=2, scaleRadius=0.7"]),
+}
+
+
+def engine_coefs(mp, dens):
+    import ctypes
+    from agama_b200 import _native
+    L = _native.lib()
+    arr = (ctypes.c_char_p * len(dens))(*[d.encode() for d in dens])
+    nr, nc = ctypes.c_int(0), ctypes.c_int(0)
+    assert L.agama_multipoleCoefsFromDensities(mp.encode(), len(dens), arr, ctypes.byref(nr), ctypes.byref(nc),
+                                               None, None, None) == 0, _native.error()
+    r = np.zeros(nr.value)
+    P = np.zeros((nc.value, nr.value))
+    D = np.zeros_like(P)
+    assert L.agama_multipoleCoefsFromDensities(mp.encode(), len(dens), arr, ctypes.byref(nr), ctypes.byref(nc),
+                                               _native.ptr(r), _native.ptr(P), _native.ptr(D)) == 0
+    return r, P, D
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_poisson_solve_matches_reference(name):
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    mp, dens = CASES[name]
+    r, P, D = engine_coefs(mp, dens)
+    rr, PP, DD = ref.multipole_coefs_from_density(mp + ", raw=1", dens)
+    _, PF, DF = ref.multipole_coefs_from_density(mp, dens)
+    assert P.shape == PP.shape, (P.shape, PP.shape)
+    assert np.max(np.abs(P - PF) / np.abs(PF[0])[None, :]) <= 1e-6
+    assert np.max(np.abs(D - DF) / np.abs(DF[0])[None, :]) <= 1e-6
+    assert np.max(np.abs(r / rr - 1)) <= 1e-14
+    assert np.array_equal(np.any(P != 0, axis=1), np.any(PP != 0, axis=1))
+    eP = np.max(np.abs(P - PP) / np.abs(PP[0])[None, :])
+    eD = np.max(np.abs(D - DD) / np.abs(DD[0])[None, :])
+    print(name, "coefficients vs the reference: Phi %.2e, dPhi %.2e (relative to l=0)" % (eP, eD))
+    assert eP <= 1e-12 and eD <= 1e-12, (eP, eD)
+
+
+def test_poisson_solve_rejects_unknown_density():
+    import ctypes
+    from agama_b200 import _native
+    arr = (ctypes.c_char_p * 1)(b"type=King, mass=1")
+    nr, nc = ctypes.c_int(0), ctypes.c_int(0)
+    rc = _native.lib().agama_multipoleCoefsFromDensities(b"lmax=4", 1, arr, ctypes.byref(nr), ctypes.byref(nc),
+                                                         None, None, None)
+    assert rc != 0 and "not supported" in _native.error()
+
+
+def test_reference_in_memory_potential_matches_its_file():
+    """the reference's potential built from the density in memory (the checker of the GPU test
+    below) against the same potential loaded from its coefficient file (golden vectors): they differ
+    only by the file's re-derived coefficients (1e-7 near the centre at most)"""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    mp, dens = CASES["cfg1"]
+    g = np.load(os.path.join(GOLDEN, "potential_cfg1.npz"))
+    phi = ref.multipole_potential_from_density(mp, dens).eval(g["points"], nthreads=1)[0]
+    assert np.max(np.abs(phi / g["phi"] - 1)) <= 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cfg1", "cfg2", "cfg3", "cfg5", "quad", "sph"])
+def test_potential_from_density_on_device(name):
+    """the device potential built from the density against the reference's Multipole built from the
+    same density in memory: potential to 1e-12 and force to 1e-11 (relative) at the golden points
+    outside the innermost grid cell, where the log-scaled monopole amplifies the 1e-15 differences
+    of the coefficients (inside it: 1e-8)"""
+    import agama_b200
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    mp, dens = CASES[name]
+    g = np.load(os.path.join(GOLDEN, "potential_%s.npz" % name))
+    kv = lambda s: dict((x.split("=")[0].strip(), x.split("=")[1].strip()) for x in s.split(","))
+    pot = agama_b200.Potential(type="Multipole", density=[kv(d) for d in dens], **kv(mp))
+    rpot = ref.multipole_potential_from_density(mp, dens)
+    pts = g["points"]
+    phi, acc = pot.eval(pts, pot=True, acc=True)
+    rphi, rgrad, _ = rpot.eval(pts, nthreads=1)
+    r, _, _ = agama_b200.multipole_coefs_from_density([kv(d) for d in dens], **kv(mp))
+    rad = np.linalg.norm(pts, axis=1)
+    ephi = np.abs(phi - rphi) / np.abs(rphi)
+    egrad = np.linalg.norm(-acc - rgrad, axis=1) / np.linalg.norm(rgrad, axis=1)
+    out = rad > r[1]
+    print(name, "potential from the density vs the reference's: phi %.2e grad %.2e outside r_1; inside %.2e %.2e"
+          % (ephi[out].max(), egrad[out].max(), ephi[~out].max(initial=0), egrad[~out].max(initial=0)))
+    assert ephi[out].max() <= 1e-12 and egrad[out].max() <= 1e-11
+    assert ephi[~out].max(initial=0) <= 1e-8 and egrad[~out].max(initial=0) <= 1e-8
