@@ -985,7 +985,12 @@ extern "C" int agama_gemmBf16Device(int M, int N, int K, const void* A, const vo
         if(M < 0 || N < 0 || K < 0 || (M > 0 && N > 0 && K > 0 && (!A || !B || !C)))
             throw std::invalid_argument("gemmBf16Device: invalid arguments");
         requireDevice();
-        launchGemmBf16(M, N, K, A, B, C, ldc, accumulate != 0, static_cast<cudaStream_t>(stream));
+        // a workspace for the split-K form of outputs with few tiles (released in stream order)
+        const size_t wsFloats = static_cast<size_t>(16) * M * N;
+        const bool few = M > 0 && N > 0 && (M / 128) * (N / 128) <= 32;
+        Scratch ws(few ? wsFloats * sizeof(float) : 256, static_cast<cudaStream_t>(stream));
+        launchGemmBf16(M, N, K, A, B, C, ldc, accumulate != 0, static_cast<cudaStream_t>(stream),
+            few ? static_cast<float*>(ws.ptr) : nullptr, few ? wsFloats : 0);
     });
 }
 

@@ -71,10 +71,12 @@ __global__ void biasActKernel(int B, float* __restrict__ z, const float* __restr
 
 /// y = h3 W4^T + b4; loss terms and dy = 2 m (y - t) / S
 __global__ void outputLossKernel(int B, const float* __restrict__ h3, const float* __restrict__ p,
-    const float* __restrict__ t, const float* __restrict__ m, float invS, float* __restrict__ dy, float* __restrict__ loss)
+    const float* __restrict__ t, const float* __restrict__ m, const float* __restrict__ maskSum, float* __restrict__ dy,
+    float* __restrict__ loss)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if(idx >= B * NOUT) return;
+    const float invS = 1.f / fmaxf(*maskSum, 1.f);
     const int b = idx / NOUT, j = idx % NOUT;
     float s = p[OFF_B4 + j];
     for(int c = 0; c < H; c++) s += h3[static_cast<size_t>(b) * H + c] * p[OFF_W4 + j * H + c];
@@ -192,26 +194,81 @@ __global__ void standardiseKernel(long n, int ncol, const float* __restrict__ in
     out[idx] = (in[idx] - mean[c]) / stdv[c];
 }
 
-/// Adam (Kingma & Ba 2015) on the FP32 parameters
+/// device-side state of a training run, advanced by the kernels of each step, so that a step
+/// replays from a CUDA graph without the host: the batch of the epoch's permutation, the Adam step
+/// count, the batch's mask sum, the learning rate of the epoch and the loss sums
+struct TrainState {
+    int batchIndex;
+    int adamStep;
+    float maskSum;
+    float lr;
+    float loss;
+    float lossSum;
+};
+
+/// the batch's rows by the epoch's permutation (x: NIN, t and m: NOUT columns) and the sum of its
+/// masks (the loss normalisation)
+__global__ void gatherBatchKernel(int B, const int* __restrict__ perm, TrainState* __restrict__ st,
+    const float* __restrict__ xs, const float* __restrict__ ts, const float* __restrict__ ms,
+    float* __restrict__ x, float* __restrict__ t, float* __restrict__ m)
+{
+    __shared__ float red[256];
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    float msum = 0;
+    if(b < B) {
+        const size_t row = static_cast<size_t>(perm[static_cast<size_t>(st->batchIndex) * B + b]);
+        for(int k = 0; k < NIN; k++) x[b * NIN + k] = xs[row * NIN + k];
+        for(int j = 0; j < NOUT; j++) {
+            t[b * NOUT + j] = ts[row * NOUT + j];
+            const float mv = ms[row * NOUT + j];
+            m[b * NOUT + j] = mv;
+            msum += mv;
+        }
+    }
+    red[threadIdx.x] = msum;
+    __syncthreads();
+    for(int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if(threadIdx.x < s2) red[threadIdx.x] += red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) atomicAdd(&st->maskSum, red[0]);      // integer-valued: exact in any order
+}
+
+/// the end of a step: loss into the epoch's sum, counters advanced, the mask sum cleared
+__global__ void finishStepKernel(TrainState* st)
+{
+    st->lossSum += st->loss;
+    st->loss = 0;
+    st->maskSum = 0;
+    st->batchIndex++;
+    st->adamStep++;
+}
+
+/// the start of an epoch: learning rate, batch counter and loss sum
+__global__ void startEpochKernel(TrainState* st, float lr)
+{
+    st->lr = lr;
+    st->batchIndex = 0;
+    st->lossSum = 0;
+    st->loss = 0;
+    st->maskSum = 0;
+}
+
+/// Adam (Kingma & Ba 2015) on the FP32 parameters; the step count and learning rate come from the
+/// training state (bias corrections 1 - beta^t for the step t = adamStep + 1)
 __global__ void adamKernel(int np, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
-    float* __restrict__ v, float lr, float beta1, float beta2, float eps, float c1, float c2)
+    float* __restrict__ v, const TrainState* __restrict__ st, float beta1, float beta2, float eps)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= np) return;
+    const float step = static_cast<float>(st->adamStep + 1), lr = st->lr;
+    const float c1 = 1 - powf(beta1, step), c2 = 1 - powf(beta2, step);
     const float gi = g[i];
     m[i] = beta1 * m[i] + (1 - beta1) * gi;
     v[i] = beta2 * v[i] + (1 - beta2) * gi * gi;
     p[i] -= lr * (m[i] / c1) / (sqrtf(v[i] / c2) + eps);
 }
 
-/// gather a batch of rows by index
-__global__ void gatherKernel(int B, int ncol, const int* __restrict__ idx, const float* __restrict__ src,
-    float* __restrict__ dst)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if(k >= B * ncol) return;
-    dst[k] = src[static_cast<size_t>(idx[k / ncol]) * ncol + k % ncol];
-}
 
 // ---------------------------------------------------------------- fused inference
 
@@ -416,12 +473,15 @@ void Mlp::refreshWeights(cudaStream_t s)
 /// the per-batch work buffers of the training pass (B rows)
 struct MlpBatch {
     int B;
-    float *x, *t, *m, *z1, *z2, *z3, *h3, *dy, *dh, *loss;
+    float *x, *t, *m, *z1, *z2, *z3, *h3, *dy, *dh, *loss, *maskSum, *ws;
     __nv_bfloat16 *h1b, *h1bT, *h2b, *h2bT, *dzb, *dzbT;
+    static constexpr size_t WS_FLOATS = 16 * H * H;      // split-K partial tiles of the weight gradients
     Scratch mem;
     MlpBatch(int b, cudaStream_t s) : B(b), mem(bytes(b), s) {
         char* q = static_cast<char*>(mem.ptr);
         auto take = [&](size_t n) { char* r = q; q += (n + 255) / 256 * 256; return r; };
+        ws = reinterpret_cast<float*>(take(WS_FLOATS * 4));
+        maskSum = reinterpret_cast<float*>(take(4));
         x = reinterpret_cast<float*>(take(B * NIN * 4)); t = reinterpret_cast<float*>(take(B * NOUT * 4));
         m = reinterpret_cast<float*>(take(B * NOUT * 4));
         z1 = reinterpret_cast<float*>(take(B * H * 4)); z2 = reinterpret_cast<float*>(take(B * H * 4));
@@ -432,15 +492,18 @@ struct MlpBatch {
         h2b = reinterpret_cast<__nv_bfloat16*>(take(B * H * 2)); h2bT = reinterpret_cast<__nv_bfloat16*>(take(B * H * 2));
         dzb = reinterpret_cast<__nv_bfloat16*>(take(B * H * 2)); dzbT = reinterpret_cast<__nv_bfloat16*>(take(B * H * 2));
     }
-    static size_t bytes(int B) { return static_cast<size_t>(B) * (NIN * 4 + 3 * NOUT * 4 + 5 * H * 4 + 6 * H * 2) + 17 * 256; }
+    static size_t bytes(int B) {
+        return static_cast<size_t>(B) * (NIN * 4 + 3 * NOUT * 4 + 5 * H * 4 + 6 * H * 2) + WS_FLOATS * 4 + 19 * 256;
+    }
 };
 
 namespace {
 inline int blocks(long n, int b) { return static_cast<int>((n + b - 1) / b); }
 }
 
-/// loss and gradient of one batch already in bt.x / bt.t / bt.m (standardised); grad: NPARAM floats
-void Mlp::lossGrad(MlpBatch& bt, float invS, float* grad, cudaStream_t s)
+/// loss and gradient of one batch already in bt.x / bt.t / bt.m (standardised); grad: NPARAM
+/// floats; the loss is normalised by the mask sum at maskSum and added to loss (device pointers)
+void Mlp::lossGrad(MlpBatch& bt, const float* maskSum, float* loss, float* grad, cudaStream_t s)
 {
     const int B = bt.B;
     // forward
@@ -449,19 +512,18 @@ void Mlp::lossGrad(MlpBatch& bt, float invS, float* grad, cudaStream_t s)
     biasActKernel<<<blocks(B * H, 256), 256, 0, s>>>(B, bt.z2, params.ptr + OFF_B2, bt.h2b, bt.h2bT, nullptr);
     launchGemmBf16(B, H, H, bt.h2b, w3.ptr, bt.z3, H, false, s);
     biasActKernel<<<blocks(B * H, 256), 256, 0, s>>>(B, bt.z3, params.ptr + OFF_B3, nullptr, nullptr, bt.h3);
-    AGB_CUDA(cudaMemsetAsync(bt.loss, 0, sizeof(float), s));
-    outputLossKernel<<<blocks(B * NOUT, 256), 256, 0, s>>>(B, bt.h3, params.ptr, bt.t, bt.m, invS, bt.dy, bt.loss);
+    outputLossKernel<<<blocks(B * NOUT, 256), 256, 0, s>>>(B, bt.h3, params.ptr, bt.t, bt.m, maskSum, bt.dy, loss);
     // backward: output layer
     reduceGradKernel<<<H, 256, 0, s>>>(B, 0, bt.dy, bt.h3, grad, OFF_W4, 0);
     outputBiasGradKernel<<<1, 256, 0, s>>>(B, bt.dy, grad);
     backOutputKernel<<<blocks(B * H, 256), 256, 0, s>>>(B, bt.dy, params.ptr, bt.z3, bt.dh, bt.dzb, bt.dzbT);
     // layer 3: dW3 = dz3^T h2, db3, dh2 = dz3 W3
-    launchGemmBf16(H, H, B, bt.dzbT, bt.h2bT, grad + OFF_W3, H, false, s);
+    launchGemmBf16(H, H, B, bt.dzbT, bt.h2bT, grad + OFF_W3, H, false, s, bt.ws, MlpBatch::WS_FLOATS);
     reduceGradKernel<<<H, 256, 0, s>>>(B, 1, bt.dh, nullptr, grad, 0, OFF_B3);
     launchGemmBf16(B, H, H, bt.dzb, w3T.ptr, bt.dh, H, false, s);
     backActKernel<<<blocks(B * H, 256), 256, 0, s>>>(B, bt.dh, bt.z2, bt.dzb, bt.dzbT);
     // layer 2: dW2 = dz2^T h1, db2, dh1 = dz2 W2
-    launchGemmBf16(H, H, B, bt.dzbT, bt.h1bT, grad + OFF_W2, H, false, s);
+    launchGemmBf16(H, H, B, bt.dzbT, bt.h1bT, grad + OFF_W2, H, false, s, bt.ws, MlpBatch::WS_FLOATS);
     reduceGradKernel<<<H, 256, 0, s>>>(B, 1, bt.dh, nullptr, grad, 0, OFF_B2);
     launchGemmBf16(B, H, H, bt.dzb, w2T.ptr, bt.dh, H, false, s);
     backActKernel<<<blocks(B * H, 256), 256, 0, s>>>(B, bt.dh, bt.z1, nullptr, nullptr);
@@ -480,9 +542,11 @@ float Mlp::lossGradDevice(int B, const float* x, const float* t, const float* m,
     std::vector<float> hm(B * NOUT);
     AGB_CUDA(cudaMemcpyAsync(hm.data(), m, sizeof(float) * B * NOUT, cudaMemcpyDefault, s));
     AGB_CUDA(cudaStreamSynchronize(s));
-    double S = 0;
+    float S = 0;
     for(float v : hm) S += v;
-    lossGrad(bt, static_cast<float>(1 / std::max(S, 1.0)), grad, s);
+    AGB_CUDA(cudaMemcpyAsync(bt.maskSum, &S, sizeof(float), cudaMemcpyHostToDevice, s));
+    AGB_CUDA(cudaMemsetAsync(bt.loss, 0, sizeof(float), s));
+    lossGrad(bt, bt.maskSum, bt.loss, grad, s);
     float loss = 0;
     AGB_CUDA(cudaMemcpyAsync(&loss, bt.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
     AGB_CUDA(cudaStreamSynchronize(s));
@@ -516,11 +580,10 @@ std::vector<float> Mlp::train(long n, const float* x, const float* t, const floa
     }
     AGB_CUDA(cudaMemcpy(scaling.ptr, sc.data(), sizeof(float) * sc.size(), cudaMemcpyHostToDevice));
     // standardised copies of the whole set on the device
-    Scratch data(sizeof(float) * n * (NIN + 2 * NOUT) + 1024 + sizeof(int) * batch + 256, s);
+    Scratch data(sizeof(float) * n * (NIN + 2 * NOUT) + 1024, s);
     float* xs = static_cast<float*>(data.ptr);
     float* ts = xs + n * NIN;
     float* ms = ts + n * NOUT;
-    int* idx = reinterpret_cast<int*>(reinterpret_cast<char*>(ms + n * NOUT) + 512);
     AGB_CUDA(cudaMemcpyAsync(ms, m, sizeof(float) * n * NOUT, cudaMemcpyDefault, s));
     Scratch raw(sizeof(float) * n * (NIN + NOUT), s);
     float* rx = static_cast<float*>(raw.ptr);
@@ -533,36 +596,57 @@ std::vector<float> Mlp::train(long n, const float* x, const float* t, const floa
 
     MlpBatch bt(batch, s);
     DevBuf<float> grad(NPARAM);
+    DevBuf<int> perm(n);
+    DevBuf<TrainState> state(1);
+    {
+        TrainState init{ 0, static_cast<int>(adamStep), 0.f, lr, 0.f, 0.f };
+        AGB_CUDA(cudaMemcpyAsync(state.ptr, &init, sizeof(TrainState), cudaMemcpyHostToDevice, s));
+    }
     std::mt19937_64 rng(seed);
-    std::vector<int> perm(n);
-    for(long i = 0; i < n; i++) perm[i] = static_cast<int>(i);
+    std::vector<int> hperm(n);
+    for(long i = 0; i < n; i++) hperm[i] = static_cast<int>(i);
     std::vector<float> history;
     const long steps = n / batch;
-    std::vector<float> hmb(batch * NOUT);
-    for(int e = 0; e < epochs; e++) {
-        std::shuffle(perm.begin(), perm.end(), rng);
-        double lossSum = 0;
-        const float lrE = lr * 0.5f * (1 + std::cos(static_cast<float>(M_PI) * e / std::max(1, epochs)));   // cosine decay
-        for(long st = 0; st < steps; st++) {
-            AGB_CUDA(cudaMemcpyAsync(idx, perm.data() + st * batch, sizeof(int) * batch, cudaMemcpyHostToDevice, s));
-            gatherKernel<<<blocks(batch * NIN, 256), 256, 0, s>>>(batch, NIN, idx, xs, bt.x);
-            gatherKernel<<<blocks(batch * NOUT, 256), 256, 0, s>>>(batch, NOUT, idx, ts, bt.t);
-            gatherKernel<<<blocks(batch * NOUT, 256), 256, 0, s>>>(batch, NOUT, idx, ms, bt.m);
-            double S = 0;
-            for(int k = 0; k < batch; k++) for(int j = 0; j < NOUT; j++) S += hm[static_cast<size_t>(perm[st * batch + k]) * NOUT + j];
-            lossGrad(bt, static_cast<float>(1 / std::max(S, 1.0)), grad.ptr, s);
-            adamStep++;
-            const float c1 = 1 - std::pow(0.9f, static_cast<float>(adamStep)), c2 = 1 - std::pow(0.999f, static_cast<float>(adamStep));
-            adamKernel<<<blocks(NPARAM, 256), 256, 0, s>>>(NPARAM, params.ptr, grad.ptr, adamM.ptr, adamV.ptr, lrE, 0.9f,
-                0.999f, 1e-8f, c1, c2);
-            refreshWeights(s);
-            float l = 0;
-            AGB_CUDA(cudaMemcpyAsync(&l, bt.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
-            AGB_CUDA(cudaStreamSynchronize(s));
-            lossSum += l;
+    // one Adam step (gather, forward, backward, update, BF16 weight copies, counters) captured once
+    // and replayed: it reads its batch index, mask sum, learning rate and step count from the state
+    prepareGemm();
+    cudaStream_t cs;
+    AGB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    AGB_CUDA(cudaStreamSynchronize(s));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    try {
+        AGB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        gatherBatchKernel<<<blocks(batch, 256), 256, 0, cs>>>(batch, perm.ptr, state.ptr, xs, ts, ms, bt.x, bt.t, bt.m);
+        lossGrad(bt, &state.ptr->maskSum, &state.ptr->loss, grad.ptr, cs);
+        adamKernel<<<blocks(NPARAM, 256), 256, 0, cs>>>(NPARAM, params.ptr, grad.ptr, adamM.ptr, adamV.ptr, state.ptr,
+            0.9f, 0.999f, 1e-8f);
+        refreshWeights(cs);
+        finishStepKernel<<<1, 1, 0, cs>>>(state.ptr);
+        AGB_CUDA(cudaStreamEndCapture(cs, &graph));
+        AGB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        for(int e = 0; e < epochs; e++) {
+            std::shuffle(hperm.begin(), hperm.end(), rng);
+            AGB_CUDA(cudaMemcpyAsync(perm.ptr, hperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, cs));
+            const float lrE = lr * 0.5f * (1 + std::cos(static_cast<float>(M_PI) * e / std::max(1, epochs)));   // cosine decay
+            startEpochKernel<<<1, 1, 0, cs>>>(state.ptr, lrE);
+            AGB_CUDA(cudaGetLastError());
+            for(long st = 0; st < steps; st++) AGB_CUDA(cudaGraphLaunch(exec, cs));
+            TrainState h;
+            AGB_CUDA(cudaMemcpyAsync(&h, state.ptr, sizeof(TrainState), cudaMemcpyDeviceToHost, cs));
+            AGB_CUDA(cudaStreamSynchronize(cs));
+            history.push_back(static_cast<float>(h.lossSum / steps));
+            adamStep = h.adamStep;
         }
-        history.push_back(static_cast<float>(lossSum / steps));
+    } catch(...) {
+        if(exec) cudaGraphExecDestroy(exec);
+        if(graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        throw;
     }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    AGB_CUDA(cudaStreamDestroy(cs));
     AGB_CUDA(cudaStreamSynchronize(s));
     checkGemmError();
     return history;

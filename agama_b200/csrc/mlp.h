@@ -38,13 +38,16 @@ struct Mlp {
     /// throws if an inference kernel gave up waiting for its tensor cores
     void checkError() const;
 private:
-    void lossGrad(MlpBatch& bt, float invS, float* grad, cudaStream_t s);
+    void lossGrad(MlpBatch& bt, const float* maskSum, float* loss, float* grad, cudaStream_t s);
 };
 
 /// C[M x N] (FP32, leading dimension ldc) = A[M x K] * B[N x K]^T (+ C), A and B BF16 row-major;
-/// M, N multiples of 128, K a multiple of 64 (tcgen05 MMAs, mlp_gemm.cu)
+/// M, N multiples of 128, K a multiple of 64 (tcgen05 MMAs, mlp_gemm.cu).  With a workspace
+/// (workspaceFloats floats), outputs of few tiles are split over K across CTAs.
 void launchGemmBf16(int M, int N, int K, const void* A, const void* B, float* C, int ldc, bool accumulate,
-    cudaStream_t stream);
+    cudaStream_t stream, float* workspace = nullptr, size_t workspaceFloats = 0);
+/// set up the GEMM's per-device state (error flag, shared-memory limit) before a stream capture
+void prepareGemm();
 /// throws if a GEMM launched since the process started gave up waiting for its tensor cores
 void checkGemmError();
 

@@ -21,25 +21,33 @@ namespace {
 
 constexpr int GEMM_BM = 128, GEMM_BN = 128, GEMM_BK = 64;
 constexpr int TILE_BYTES = GEMM_BM * GEMM_BK * 2;            // 16 KB per operand tile
-// 64 KB of shared memory per CTA keeps at most 3 CTAs (384 tensor-memory columns) on an SM, so an
-// allocation never waits for another CTA's columns
-constexpr int GEMM_SMEM = 64 * 1024;
+constexpr int GEMM_STAGES = 2;
+// two stages of (A, B) tiles, 64 KB, plus alignment: at most 3 CTAs (384 tensor-memory columns)
+// on an SM, so an allocation never waits for another CTA's columns
+constexpr int GEMM_SMEM = GEMM_STAGES * 2 * TILE_BYTES + 1024;
 constexpr long MBAR_MAX_POLLS = 1L << 22;
+constexpr int GEMM_MAX_SPLITS = 16;
 
-__global__ void __launch_bounds__(128) gemmBf16Kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
-    const __nv_bfloat16* __restrict__ B, float* __restrict__ C, int ldc, int accumulate, int* __restrict__ error)
+/** One 128 x 128 tile of C = A B^T over this CTA's part of K (blockIdx.z of gridDim.z equal parts of
+    Ksplit columns each; A and B rows have stride lda), written to C + blockIdx.z * splitStride.
+    The K-chunks go through two shared-memory stages: the threads stage chunk j + 1 while the
+    tensor cores run the MMAs of chunk j, and a stage is overwritten only after the mbarrier of the
+    MMAs that read it has completed. */
+__global__ void __launch_bounds__(128) gemmBf16Kernel(int Ksplit, int lda, const __nv_bfloat16* __restrict__ A,
+    const __nv_bfloat16* __restrict__ B, float* __restrict__ C, int ldc, long splitStride, int accumulate,
+    int* __restrict__ error)
 {
     extern __shared__ unsigned char smemRaw[];
-    __shared__ uint64_t mbar;
+    __shared__ uint64_t mbar[GEMM_STAGES];
     __shared__ uint32_t tmemBase;
     unsigned char* tiles = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-    unsigned char* tileA = tiles;
-    unsigned char* tileB = tiles + TILE_BYTES;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int bm = blockIdx.y * GEMM_BM, bn = blockIdx.x * GEMM_BN;
+    const int kBegin = blockIdx.z * Ksplit, kEnd = kBegin + Ksplit;
+    C += blockIdx.z * splitStride;
 
     if(warp == 0) umma::tmemAlloc(&tmemBase, 128);
-    if(threadIdx.x == 0) umma::mbarInit(&mbar, 1);
+    if(threadIdx.x == 0) for(int st = 0; st < GEMM_STAGES; st++) umma::mbarInit(&mbar[st], 1);
     umma::fenceBeforeSync();
     __syncthreads();
     umma::fenceAfterSync();
@@ -47,17 +55,28 @@ __global__ void __launch_bounds__(128) gemmBf16Kernel(int M, int N, int K, const
     constexpr uint32_t idesc = umma::instrDescBf16(GEMM_BM, GEMM_BN);
     constexpr uint32_t SBO = GEMM_BK / 8 * umma::CORE_BYTES;
 
-    uint32_t parity = 0;
+    uint32_t parity[GEMM_STAGES] = { 0, 0 };
     bool ok = true;
-    for(int k0 = 0; k0 < K && ok; k0 += GEMM_BK) {
+    int chunk = 0;
+    for(int k0 = kBegin; k0 < kEnd; k0 += GEMM_BK, chunk++) {
+        const int st = chunk % GEMM_STAGES;
+        unsigned char* tileA = tiles + st * 2 * TILE_BYTES;
+        unsigned char* tileB = tileA + TILE_BYTES;
+        if(chunk >= GEMM_STAGES) {
+            // the MMAs of chunk - GEMM_STAGES read this stage: wait for them before overwriting it
+            const bool done = umma::mbarWait(&mbar[st], parity[st], MBAR_MAX_POLLS);
+            parity[st] ^= 1;
+            ok = __syncthreads_and(done);
+            if(!ok) break;
+        }
         // stage the 128 x 64 chunks of A and B: 16-byte vectors = one row of one core matrix
         for(int v = threadIdx.x; v < GEMM_BM * GEMM_BK / 8; v += blockDim.x) {
             const int r = v / (GEMM_BK / 8), kc = v % (GEMM_BK / 8);
             const uint32_t off = umma::tileOffset(r, kc * 8, GEMM_BK);
             *reinterpret_cast<uint4*>(tileA + off) =
-                *reinterpret_cast<const uint4*>(A + static_cast<size_t>(bm + r) * K + k0 + kc * 8);
+                *reinterpret_cast<const uint4*>(A + static_cast<size_t>(bm + r) * lda + k0 + kc * 8);
             *reinterpret_cast<uint4*>(tileB + off) =
-                *reinterpret_cast<const uint4*>(B + static_cast<size_t>(bn + r) * K + k0 + kc * 8);
+                *reinterpret_cast<const uint4*>(B + static_cast<size_t>(bn + r) * lda + k0 + kc * 8);
         }
         umma::fenceSmemForAsync();
         __syncthreads();
@@ -66,14 +85,20 @@ __global__ void __launch_bounds__(128) gemmBf16Kernel(int M, int N, int K, const
             for(int kk = 0; kk < GEMM_BK / 16; kk++) {
                 const uint64_t da = umma::smemDescriptor(umma::smemAddr(tileA) + kk * 2 * umma::LBO, umma::LBO, SBO);
                 const uint64_t db = umma::smemDescriptor(umma::smemAddr(tileB) + kk * 2 * umma::LBO, umma::LBO, SBO);
-                umma::mmaBf16(tmem, da, db, idesc, k0 > 0 || kk > 0);
+                umma::mmaBf16(tmem, da, db, idesc, k0 > kBegin || kk > 0);
             }
-            umma::commitTo(&mbar);
+            umma::commitTo(&mbar[st]);
         }
-        // every thread waits for the MMAs of this chunk before the tiles are overwritten
-        const bool done = umma::mbarWait(&mbar, parity, MBAR_MAX_POLLS);
-        parity ^= 1;
-        ok = __syncthreads_and(done);
+    }
+    // the chunks whose completion has not been waited for yet (the last GEMM_STAGES), in order
+    if(ok) {
+        for(int j = chunk > GEMM_STAGES ? chunk - GEMM_STAGES : 0; j < chunk; j++) {
+            const int st = j % GEMM_STAGES;
+            const bool done = umma::mbarWait(&mbar[st], parity[st], MBAR_MAX_POLLS);
+            parity[st] ^= 1;
+            ok = __syncthreads_and(done);
+            if(!ok) break;
+        }
     }
     umma::fenceAfterSync();
     if(ok) {
@@ -91,6 +116,18 @@ __global__ void __launch_bounds__(128) gemmBf16Kernel(int M, int N, int K, const
     umma::fenceBeforeSync();
     __syncthreads();
     if(warp == 0) umma::tmemFree(tmem, 128);
+}
+
+/// C (+)= the sum of the split-K partial products, added in split order (deterministic)
+__global__ void splitReduceKernel(int M, int N, int ldc, int splits, const float* __restrict__ part, float* __restrict__ C,
+    int accumulate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= M * N) return;
+    const int r = i / N, c = i % N;
+    float s = accumulate ? C[static_cast<size_t>(r) * ldc + c] : 0.f;
+    for(int z = 0; z < splits; z++) s += part[static_cast<size_t>(z) * M * N + i];
+    C[static_cast<size_t>(r) * ldc + c] = s;
 }
 
 /// per-device state of the GEMM: its completion-timeout flag (device memory of that device) and
@@ -123,17 +160,34 @@ GemmDeviceState& gemmState()
 }  // namespace
 
 void launchGemmBf16(int M, int N, int K, const void* A, const void* B, float* C, int ldc, bool accumulate,
-    cudaStream_t stream)
+    cudaStream_t stream, float* workspace, size_t workspaceFloats)
 {
     if(M <= 0 || N <= 0 || K <= 0) return;
     if(M % GEMM_BM || N % GEMM_BN || K % GEMM_BK || ldc < N)
         throw std::invalid_argument("gemmBf16: M, N must be multiples of 128, K of 64, ldc >= N");
     GemmDeviceState& st = gemmState();
-    const dim3 grid(N / GEMM_BN, M / GEMM_BM);
-    gemmBf16Kernel<<<grid, 128, GEMM_SMEM, stream>>>(M, N, K, static_cast<const __nv_bfloat16*>(A),
-        static_cast<const __nv_bfloat16*>(B), C, ldc, accumulate ? 1 : 0, st.flag);
+    // split K over several CTAs when the output has few tiles (the weight gradients: one 128 x 128
+    // tile with K = batch): each split writes its partial tile to the workspace, then one kernel
+    // sums them in order
+    const int tiles = (M / GEMM_BM) * (N / GEMM_BN), chunks = K / GEMM_BK;
+    int splits = 1;
+    while(splits * 2 <= GEMM_MAX_SPLITS && tiles * splits * 2 <= 64 && chunks % (splits * 2) == 0 &&
+          chunks / (splits * 2) >= 2 && workspace &&
+          static_cast<size_t>(splits) * 2 * M * N <= workspaceFloats)
+        splits *= 2;
+    const dim3 grid(N / GEMM_BN, M / GEMM_BM, splits);
+    if(splits == 1) {
+        gemmBf16Kernel<<<grid, 128, GEMM_SMEM, stream>>>(K, K, static_cast<const __nv_bfloat16*>(A),
+            static_cast<const __nv_bfloat16*>(B), C, ldc, 0, accumulate ? 1 : 0, st.flag);
+    } else {
+        gemmBf16Kernel<<<grid, 128, GEMM_SMEM, stream>>>(K / splits, K, static_cast<const __nv_bfloat16*>(A),
+            static_cast<const __nv_bfloat16*>(B), workspace, N, static_cast<long>(M) * N, 0, st.flag);
+        splitReduceKernel<<<(M * N + 255) / 256, 256, 0, stream>>>(M, N, ldc, splits, workspace, C, accumulate ? 1 : 0);
+    }
     AGB_CUDA(cudaGetLastError());
 }
+
+void prepareGemm() { gemmState(); }
 
 void checkGemmError()
 {

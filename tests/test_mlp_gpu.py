@@ -5,10 +5,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 192), (512, 128, 1024)])
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 192), (512, 128, 1024), (128, 128, 2048),
+                                   (2048, 128, 128)])
 def test_gemm_bf16_tensor_cores(M, N, K):
-    """C = A B^T on tcgen05 (BF16 operands, FP32 accumulation) equals the FP32 product of the
-    same BF16 values to FP32 summation-order round-off; accumulate adds to C"""
+    """C = A B^T on tcgen05 (BF16 operands, FP32 accumulation, two shared-memory stages; outputs of
+    few tiles split over K across CTAs and summed in order: (512, 128, 1024) in 8 splits,
+    (128, 128, 2048) -- the weight-gradient shape -- in 16) equals the FP32 product of the same BF16
+    values to FP32 summation-order round-off; accumulate adds to C"""
     import torch
     from agama_b200 import _native
     g = torch.Generator(device="cpu").manual_seed(M + N + K)
