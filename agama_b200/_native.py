@@ -81,6 +81,7 @@ SIGNATURES = {
     "agama_actionFinderPredictBrackets": (ctypes.c_int, [VP, ctypes.c_long, F, F]),
     "agama_actionFinderUseBrackets": (ctypes.c_int, [VP, ctypes.c_int]),
     "agama_actionFinderBracketStats": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    "agama_actionFinderCountBrackets": (ctypes.c_int, [VP, ctypes.c_int]),
     "agama_mlpCreate": (VP, [ctypes.c_ulonglong]),
     "agama_mlpDelete": (None, [VP]),
     "agama_mlpNumParams": (ctypes.c_int, []),

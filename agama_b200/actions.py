@@ -106,6 +106,11 @@ class ActionFinder:
     def use_brackets(self, on=True):
         check(_native.lib().agama_actionFinderUseBrackets(self._h, 1 if on else 0))
 
+    def count_brackets(self, on=True):
+        """keep (True, the default) or stop the root-search counters of bracket_stats(); without
+        them the searches run in a kernel compiled without the counters"""
+        check(_native.lib().agama_actionFinderCountBrackets(self._h, 1 if on else 0))
+
     def bracket_stats(self, reset=False):
         """{searches, narrowed, fallbacks, iterations} of the root searches since the last reset:
         narrowed = searches started from a predicted root, fallbacks = plain searches after a

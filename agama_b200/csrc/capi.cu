@@ -817,7 +817,8 @@ const BracketPlan* planOf(const DeviceActionFinder& F, BracketPlan& tmp)
     if(!F.bracketStats.ptr) return nullptr;     // no predictor trained: plain searches, no counters
     tmp.net = F.useBrackets ? F.brackets : nullptr;
     for(int k = 0; k < 3; k++) tmp.widths[k] = F.bracketWidths[k];
-    tmp.stats = F.bracketStats.ptr;
+    tmp.stats = F.countBrackets ? F.bracketStats.ptr : nullptr;
+    if(!tmp.net && !tmp.stats) return nullptr;  // plain searches without counters
     return &tmp;
 }
 }  // namespace
@@ -1093,6 +1094,14 @@ extern "C" int agama_actionFinderUseBrackets(agama_ActionFinder* a, int on)
         if(!a) throw std::invalid_argument("actionFinderUseBrackets: null finder");
         if(on && !a->af->brackets) throw std::invalid_argument("actionFinderUseBrackets: no bracket predictor trained");
         a->af->useBrackets = on != 0;
+    });
+}
+
+extern "C" int agama_actionFinderCountBrackets(agama_ActionFinder* a, int on)
+{
+    return guarded([&] {
+        if(!a) throw std::invalid_argument("actionFinderCountBrackets: null finder");
+        a->af->countBrackets = on != 0;
     });
 }
 

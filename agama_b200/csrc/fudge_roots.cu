@@ -90,9 +90,10 @@ __device__ __forceinline__ bool predictedBracket(const FudgeRecord& r, int kind,
     one, and the root is accepted only if it lies inside that predicted bracket and F is negative
     half-way from it to the plain end where F is negative (one more evaluation); otherwise F may
     have more roots there and the plain search, which may end on any of them, decides.  stats (may be null) accumulates {searches, seeded searches,
-    plain searches after a failed check, iterations}.  LEARNED = false (no predictions, no stats)
-    compiles the plain searches alone, without that state and the counters (fewer registers). */
-template<bool LEARNED>
+    plain searches after a failed check, iterations} when STATS.  LEARNED = false (no predictions,
+    no stats) compiles the plain searches alone, without that state and the counters (fewer
+    registers); STATS = false leaves the counters out of the learned searches. */
+template<bool LEARNED, bool STATS>
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
     FudgeRecord* __restrict__ rec, const FudgeEnds* __restrict__ ends, int* __restrict__ iters,
     unsigned long long* __restrict__ counter, const float* __restrict__ pred, const BracketWidths widths,
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                                 if(isFinite(guess)) seeded = s.seed(guess, &x);
                             }
                         }
-                        if(LEARNED) {
+                        if(STATS) {
                             nSearch++;
                             nSeeded += seeded;
                         }
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                 // scaled variable; lambda_min: towards D2; nu_max: towards D2), where it is
                 // negative; otherwise F has more roots there and the plain search decides
                 verifying = false;
-                nIter++;
+                if(STATS) nIter++;
                 const FudgeRecord& r = rec[point];
                 if(fx < 0) {
                     busy = false;
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                     if(iters) atomicAdd(iters + point, s.iter + 1);
                 } else {
                     seeded = false;
-                    nFallback++;
+                    if(STATS) nFallback++;
                     const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
                     const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
                     if(startPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
@@ -195,7 +196,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                     }
                 }
             } else if(s.feed(fx, dx, &x)) {
-                if(LEARNED) nIter += s.iter;
+                if(STATS) nIter += s.iter;
                 bool check = false;     // the search goes on (a check evaluation or a plain search)
                 if(LEARNED && seeded) {
                     // a seeded root is a candidate only inside the predicted bracket (it may have
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? lo : hi));
                     } else {
                         seeded = false;
-                        nFallback++;
+                        if(STATS) nFallback++;
                         check = true;       // handled: the plain search runs from here
                         if(startPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
                                       u0, fnc.D2, fnc.E, &x)) {
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
             }
         }
     }
-    if(LEARNED && stats) {     // one atomic per warp and counter
+    if(STATS && stats) {       // one atomic per warp and counter
         nSearch = __reduce_add_sync(FULL_MASK, nSearch);
         nSeeded = __reduce_add_sync(FULL_MASK, nSeeded);
         nFallback = __reduce_add_sync(FULL_MASK, nFallback);
@@ -262,7 +263,7 @@ __global__ void bracketTargetKernel(long n, const FudgeRecord* __restrict__ rec,
 }
 
 /// resident blocks of a root-kernel variant on the current device (cached per device and variant)
-template<bool LEARNED>
+template<bool LEARNED, bool STATS>
 int rootGridSize()
 {
     static std::mutex mutex;
@@ -274,7 +275,7 @@ int rootGridSize()
     if(it != cache.end()) return it->second;
     int sms = 0, perSM = 0;
     AGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fudgeRootKernel<LEARNED>, ROOT_BLOCK, 0));
+    AGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fudgeRootKernel<LEARNED, STATS>, ROOT_BLOCK, 0));
     const int grid = std::max(1, sms * std::max(1, perSM));
     cache[dev] = grid;
     return grid;
@@ -289,12 +290,16 @@ void launchFudgeRoots(const MultipoleView& M, long n, FudgeRecord* rec, const Fu
     if(n <= 0) return;
     AGB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream));
     const long tasks = (3 * n + ROOT_BLOCK - 1) / ROOT_BLOCK;
-    if(pred || stats) {
-        const long grid = std::min<long>(rootGridSize<true>(), tasks);
-        fudgeRootKernel<true><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, pred, widths, stats);
+    if(stats) {              // learned or plain searches with the counters
+        const long grid = std::min<long>(rootGridSize<true, true>(), tasks);
+        fudgeRootKernel<true, true><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, pred, widths, stats);
+    } else if(pred) {
+        const long grid = std::min<long>(rootGridSize<true, false>(), tasks);
+        fudgeRootKernel<true, false><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, pred, widths,
+            nullptr);
     } else {
-        const long grid = std::min<long>(rootGridSize<false>(), tasks);
-        fudgeRootKernel<false><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, nullptr, widths,
+        const long grid = std::min<long>(rootGridSize<false, false>(), tasks);
+        fudgeRootKernel<false, false><<<grid, ROOT_BLOCK, 0, stream>>>(M, n, rec, ends, iters, counter, nullptr, widths,
             nullptr);
     }
     AGB_CUDA(cudaGetLastError());

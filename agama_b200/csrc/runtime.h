@@ -70,6 +70,7 @@ struct DeviceActionFinder {
     Mlp* brackets = nullptr;          // owned; null until a predictor is trained
     float bracketWidths[3] = { 0, 0, 0 };
     bool useBrackets = false;
+    bool countBrackets = true;        // the search counters are kept (bracketStats)
     DevBuf<unsigned long long> bracketStats;
     ~DeviceActionFinder();
 };

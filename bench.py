@@ -499,7 +499,9 @@ def action_mode_lines(agama_b200, timed, rel_err, af, d, Jplain, name, training)
     n = d.shape[0]
     out = []
     af.use_brackets(False)
+    af.count_brackets(False)          # timings without the search counters (the plain kernel)
     tp = timed(lambda: af(d))
+    af.count_brackets(True)
     af.bracket_stats(reset=True)
     af(d)
     plain = af.bracket_stats(reset=True)
@@ -510,7 +512,9 @@ def action_mode_lines(agama_b200, timed, rel_err, af, d, Jplain, name, training)
         agama_b200.set_action_precision(mixed)
         af.use_brackets(learned)
         try:
+            af.count_brackets(False)
             tl = timed(lambda: af(d))
+            af.count_brackets(True)
             af.bracket_stats(reset=True)
             J = af(d)
             st = af.bracket_stats(reset=True)

@@ -395,7 +395,9 @@ int agama_evalActionsAnglesFrequenciesStandaloneManyDevice(const agama_Potential
    widths[3]), attaches it and switches it on; lossHistory (epochs floats) may be NULL.
    agama_actionFinderUseBrackets: switches the trained predictor on or off.
    agama_actionFinderBracketStats: {root searches, searches started from a predicted root, failed
-   checks (plain searches after them), root-finder iterations} since the last reset. */
+   checks (plain searches after them), root-finder iterations} since the last reset.
+   agama_actionFinderCountBrackets: keeps (1, the default once a network is trained) or stops (0)
+   those counters; without them the searches run in a kernel compiled without the counters. */
 int agama_actionFinderBracketSamples(const agama_ActionFinder* actionFinder, long n, const double* posvel,
     float* features, float* target, float* mask);
 int agama_actionFinderTrainBrackets(agama_ActionFinder* actionFinder, long n, const double* posvel, int epochs,
@@ -405,6 +407,7 @@ int agama_actionFinderPredictBrackets(const agama_ActionFinder* actionFinder, lo
     float* prediction);
 int agama_actionFinderUseBrackets(agama_ActionFinder* actionFinder, int on);
 int agama_actionFinderBracketStats(agama_ActionFinder* actionFinder, long long* stats, int reset);
+int agama_actionFinderCountBrackets(agama_ActionFinder* actionFinder, int on);
 
 /* ---------------------------------------------------------------------------------------
    Tensor-core GEMM of the bracket-predictor network (no reference counterpart; the reference has
