@@ -330,31 +330,49 @@ struct RootSearch {
     AGB_HD bool startKnownEnds(double xlower, double xupper, double tol, double flower, double dlower,
         double fupper, double dupper, double* xnext)
     {
+        if(setupKnownEnds(xlower, xupper, tol, flower, dlower, fupper, dupper)) return true;
+        return propose(xnext);
+    }
+
+    /// the same set-up without the first iterate: true when it has finished at once; otherwise
+    /// propose() gives the first point to evaluate
+    AGB_HD bool setupKnownEnds(double xlower, double xupper, double tol, double flower, double dlower,
+        double fupper, double dupper)
+    {
         startAbs(xlower, xupper, tol);
         fa = flower; da = dlower; fb = fupper; db = dupper;
-        return begin(xnext);
+        return setup();
     }
 
     /// take f and f' at the requested point; true when the search has finished (result set),
     /// otherwise *xnext is the next point to evaluate
     AGB_HD bool feed(double fx, double dx, double* xnext)
     {
+        const int r = take(fx, dx, xnext);
+        return r == 0 ? true : r == 2 ? false : propose(xnext);
+    }
+
+    /// feed without the proposal of the next iterate: 0 when the search has finished (result set),
+    /// 1 when the next point is due from propose(), 2 when *xnext already holds it (an end of the
+    /// bracket to evaluate); feed = take followed by propose when it returns 1
+    AGB_HD int take(double fx, double dx, double* xnext)
+    {
         if(phase == 0) {
             fa = fx; da = dx;
             phase = 1;
             *xnext = b;
-            return false;
+            return 2;
         }
         if(phase == 1) {
             fb = fx; db = dx;
-            return begin(xnext);
+            return setup() ? 0 : 1;
         }
         if(phase == 3) {
             fa = fx; da = dx;
-            return begin(xnext);
+            return setup() ? 0 : 1;
         }
         fb = fx; db = dx;
-        if(!isFinite(fb)) { result = NAN; return true; }
+        if(!isFinite(fb)) { result = NAN; return 0; }
         if((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) {
             c = a; fc = fa; dc = da; d = b - c; e = b - c;
         }
@@ -367,13 +385,13 @@ struct RootSearch {
             if((off > 0 && off < c - b) || (off < 0 && off > c - b))
                 b += off;
             result = b;
-            return true;
+            return 0;
         }
         const double off = -fb / db;
         const bool inside = (off > 0 && off < c - b) || (off < 0 && off > c - b);
-        if(inside && fabs(off) < abstol) { result = b + off; return true; }
-        if(iter >= ROOT_MAXITER) { result = b; return true; }
-        return propose(xnext);
+        if(inside && fabs(off) < abstol) { result = b + off; return 0; }
+        if(iter >= ROOT_MAXITER) { result = b; return 0; }
+        return 1;
     }
 
     /// replace the first iterate, just proposed after both end values were known (phase 2, the
@@ -391,6 +409,13 @@ struct RootSearch {
     /// both end values known: the bracket checks and the first iterate
     AGB_HD bool begin(double* xnext)
     {
+        if(setup()) return true;
+        return propose(xnext);
+    }
+
+    /// both end values known: the bracket checks and the initial state (true when finished)
+    AGB_HD bool setup()
+    {
         if((fa < 0 && fb < 0) || (fa > 0 && fb > 0) || !isFinite(fa + fb)) { result = NAN; return true; }
         if(fa == 0) { result = fb == 0 ? 0.5 * (a + b) : a; return true; }
         if(fb == 0) { result = b; return true; }
@@ -399,7 +424,7 @@ struct RootSearch {
             a = b; b = c; c = a;  fa = fb; fb = fc; fc = fa;  da = db; db = dc; dc = da;
         }
         phase = 2;
-        return propose(xnext);
+        return false;
     }
 
     /// the head of one iteration: convergence test and the next iterate

@@ -311,16 +311,22 @@ static __device__ double fudgeMomentumNode(const FudgeFunction& fnc, double lo, 
 
 /** The same node with the integrand's arithmetic in FP32 (the mixed-precision form of the action
     quadrature): F(tau) and the point tau come from FP64 (the potential and the cancellation in
-    F stay FP64), then p^2 = F / (2 (tau - D2)^2 tau), its square root (the hardware reciprocal
-    square root) and the product with du/ds are FP32; the caller accumulates the weighted terms with
-    compensation. */
+    F stay FP64), then p = sqrt(F / (2 tau)) / |tau - D2| (the square root through the hardware
+    reciprocal square root) and the product with du/ds are FP32; the caller accumulates the weighted
+    terms with compensation. */
 static __device__ float fudgeMomentumNode32(const FudgeFunction& fnc, double lo, double hi, double s)
 {
     double duds;
     const double tau = unscaleCub(lo, hi, s, &duds);
+    const double F = fnc.value(tau);
+    // p = sqrt(F / (2 tau)) / |tau - D2|: the square root before the division by (tau - D2)^2
+    // keeps every FP32 intermediate in range for tau up to ~1e18 (the product (tau - D2)^2 tau
+    // overflows FP32 already at tau ~ 1e12, where loosely bound orbits reach); a value of F
+    // beyond the FP32 range takes the FP64 form
+    if(!(fabs(F) < 1e37)) return static_cast<float>(fudgeMomentumNode(fnc, lo, hi, s));
     const float tmd = static_cast<float>(tau - fnc.D2), t = static_cast<float>(tau);
-    const float p2 = static_cast<float>(fnc.value(tau)) / (2.f * tmd * tmd * t);
-    float v = p2 > 0.f ? p2 * rsqrtf(p2) : 0.f;
+    const float q = static_cast<float>(F) / (2.f * t);
+    float v = q > 0.f ? q * rsqrtf(q) / fabsf(tmd) : 0.f;
     if(!(v < INFINITY)) v = 0.f;
     return v * static_cast<float>(duds);
 }

@@ -23,28 +23,32 @@ __device__ __forceinline__ void storePlainLimit(FudgeRecord& r, int kind, const 
     else r.lambdaMax = unscaleSemiInf(u0, s.result, nullptr);
 }
 
-/** Start a plain search on its bracket [lo, hi] with F and F' at the ends taken from phase 1
+/// what a lane does next with its search
+enum { LANE_IDLE = 0, LANE_PROPOSE = 1, LANE_EVAL = 2, LANE_VERIFY = 3 };
+
+/** Set up a plain search on its bracket [lo, hi] with F and F' at the ends taken from phase 1
     (e may be null: the ends are then evaluated by the search): lambda_pos (shared by the lambda
     brackets), Delta^2 and |nu|; the far end of lambda_max (s = 1, lambda = inf) needs no
-    evaluation either (limitRootEval's values there).  True when the search has finished at once
-    (no sign change, or a root at an end); otherwise *x is the first point to evaluate. */
-__device__ __forceinline__ bool startPlain(RootSearch& s, int kind, const FudgeEnds* e, double lo, double hi,
+    evaluation either (limitRootEval's values there).  Returns LANE_IDLE when the search has
+    finished at once (no sign change, or a root at an end), LANE_PROPOSE when both ends are known
+    and the first iterate is due from RootSearch::propose, LANE_EVAL when *x is an end to evaluate. */
+__device__ __forceinline__ int setupPlain(RootSearch& s, int kind, const FudgeEnds* e, double lo, double hi,
     double tol, double u0, double D2, double E, double* x)
 {
-    if(!e) { *x = s.startAbs(lo, hi, tol); return false; }
+    if(!e) { *x = s.startAbs(lo, hi, tol); return LANE_EVAL; }
     if(kind == ROOT_NU_MAX) {
-        if(hi == D2) return s.startKnownEnds(lo, hi, tol, e->fNu, e->dfNu, e->fD2, e->dfD2, x);
+        if(hi == D2) return s.setupKnownEnds(lo, hi, tol, e->fNu, e->dfNu, e->fD2, e->dfD2) ? LANE_IDLE : LANE_PROPOSE;
         *x = s.startAbs(lo, hi, tol);
-        s.feed(e->fNu, e->dfNu, x);         // the lower end known; the upper one is evaluated next
-        return false;
+        s.take(e->fNu, e->dfNu, x);         // the lower end known; the upper one is evaluated next
+        return LANE_EVAL;
     }
     if(kind == ROOT_LAMBDA_MIN) {
-        if(lo == D2) return s.startKnownEnds(lo, hi, tol, e->fD2, e->dfD2, e->fPos, e->dfPos, x);
+        if(lo == D2) return s.setupKnownEnds(lo, hi, tol, e->fD2, e->dfD2, e->fPos, e->dfPos) ? LANE_IDLE : LANE_PROPOSE;
         *x = s.startKnownUpper(lo, hi, tol, e->fPos, e->dfPos);
-        return false;
+        return LANE_EVAL;
     }
     const double fa = e->fPos / pow2(u0), da = (e->dfPos - 2 * e->fPos / u0) / pow2(u0) * u0;
-    return s.startKnownEnds(lo, hi, tol, fa, da, E, NAN, x);
+    return s.setupKnownEnds(lo, hi, tol, fa, da, E, NAN) ? LANE_IDLE : LANE_PROPOSE;
 }
 
 /** The predicted bracket of a search: the predicted fraction tp -+ the half-width w (the units of
@@ -79,7 +83,12 @@ __device__ __forceinline__ bool predictedBracket(const FudgeRecord& r, int kind,
     nu_max, lambda_min, lambda_max of point i) drained from one work counter by a persistent grid.
     Each lane runs one search as a RootSearch state machine and takes the next task as soon as
     its search ends, so that the lanes of a warp meet at one potential evaluation per step instead
-    of waiting for the warp's longest search.
+    of waiting for the warp's longest search.  A step of the warp has four sections, each run by
+    the lanes it concerns: idle lanes take new searches and set them up; the lanes whose search
+    wants its next iterate (the first one of a new search or the next one of a running search)
+    propose it together; the lanes with a point evaluate F there; they feed the value to their
+    search.  Proposing the iterates of new and running searches in one section keeps the
+    interpolation steps of both in one instruction stream.
 
     With bracket predictions (pred != null: per point, in the order of the kinds, the fractions
     (nu_max - |nu|)/(D2 - |nu|), (lambda_min - D2)/(lambda - D2), (lambda - D2)/(lambda_max - D2),
@@ -89,10 +98,11 @@ __device__ __forceinline__ bool predictedBracket(const FudgeRecord& r, int kind,
     tolerance.  Seeding needs the predicted bracket (predictedBracket) strictly inside the plain
     one, and the root is accepted only if it lies inside that predicted bracket and F is negative
     half-way from it to the plain end where F is negative (one more evaluation); otherwise F may
-    have more roots there and the plain search, which may end on any of them, decides.  stats (may be null) accumulates {searches, seeded searches,
-    plain searches after a failed check, iterations} when STATS.  LEARNED = false (no predictions,
-    no stats) compiles the plain searches alone, without that state and the counters (fewer
-    registers); STATS = false leaves the counters out of the learned searches. */
+    have more roots there and the plain search, which may end on any of them, decides.  stats (may
+    be null) accumulates {searches, seeded searches, plain searches after a failed check,
+    iterations} when STATS.  LEARNED = false (no predictions, no stats) compiles the plain searches
+    alone, without that state and the counters (fewer registers); STATS = false leaves the
+    counters out of the learned searches. */
 template<bool LEARNED, bool STATS>
 __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_constant__ MultipoleView M, long n,
     FudgeRecord* __restrict__ rec, const FudgeEnds* __restrict__ ends, int* __restrict__ iters,
@@ -101,23 +111,61 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
 {
     const long total = 3 * n;
     const unsigned lane = threadIdx.x & 31;
-    bool busy = false, drained = false, seeded = false, verifying = false;
+    bool drained = false, seeded = false, fresh = false;
+    int mode = LANE_IDLE;
     long point = 0;
     int kind = 0;
     double x = 0, u0 = 0, verified = 0;
     unsigned nSearch = 0, nSeeded = 0, nFallback = 0, nIter = 0;
     FudgeFunction fnc;
     RootSearch s;
+    // a plain search on the point's bracket again (after a seeded root failed its check)
+    auto restartPlain = [&]() {
+        const FudgeRecord& r = rec[point];
+        const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
+        const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
+        seeded = false;
+        fresh = false;
+        if(STATS) nFallback++;
+        mode = setupPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
+                          u0, fnc.D2, fnc.E, &x);
+        if(mode == LANE_IDLE) storePlainLimit(rec[point], kind, s, u0, fnc.nu);
+    };
+    // the search has ended with s.result: store the limit, or (a seeded search) check its root
+    auto finishSearch = [&]() {
+        if(STATS) nIter += s.iter;
+        if(LEARNED && seeded) {
+            // a seeded root is a candidate only inside the predicted bracket (it may have come from
+            // another root of F in the plain bracket otherwise)
+            const FudgeRecord& r = rec[point];
+            const int k = kind == ROOT_NU_MAX ? 0 : kind == ROOT_LAMBDA_MIN ? 1 : 2;
+            const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
+            const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
+            double nlo, nhi;
+            predictedBracket(r, kind, pred[3 * point + k], widths.w[k], u0, lo, hi, &nlo, &nhi);
+            if(isFinite(s.result) && s.result >= nlo && s.result <= nhi) {
+                mode = LANE_VERIFY;
+                verified = s.result;
+                x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? lo : hi));
+            } else
+                restartPlain();
+            return;
+        }
+        mode = LANE_IDLE;
+        storePlainLimit(rec[point], kind, s, u0, fnc.nu);
+        if(iters) atomicAdd(iters + point, s.iter);
+    };
     while(true) {
-        // give every idle lane of the warp a new search (one atomic per warp and round)
+        // 1. every idle lane of the warp takes a new search (one atomic per warp and round) and
+        //    sets it up
         while(true) {
-            const unsigned need = __ballot_sync(FULL_MASK, !busy && !drained);
+            const unsigned need = __ballot_sync(FULL_MASK, mode == LANE_IDLE && !drained);
             if(!need) break;
             const int leader = __ffs(need) - 1;
             unsigned long long base = 0;
             if(static_cast<int>(lane) == leader) base = atomicAdd(counter, static_cast<unsigned long long>(__popc(need)));
             base = __shfl_sync(FULL_MASK, base, leader);
-            if(!busy && !drained) {
+            if(mode == LANE_IDLE && !drained) {
                 const long t = static_cast<long>(base) + __popc(need & ((1u << lane) - 1));
                 if(t >= total) drained = true;
                 else {
@@ -132,103 +180,75 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                         const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
                         const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
                         const double tol = fabs(lo - hi) * FUDGE_ACCURACY_RANGE;
-                        busy = true;
                         seeded = false;
-                        const bool done = startPlain(s, kind, ends ? ends + i : nullptr, lo, hi, tol, u0, r.D2, r.E, &x);
-                        if(done) {      // no sign change or a root at an end
-                            busy = false;
+                        mode = setupPlain(s, kind, ends ? ends + i : nullptr, lo, hi, tol, u0, r.D2, r.E, &x);
+                        fresh = mode == LANE_PROPOSE;
+                        if(mode == LANE_IDLE)       // no sign change or a root at an end
                             storePlainLimit(rec[i], kind, s, u0, fnc.nu);
-                        } else if(LEARNED && pred && s.phase == 2) {
-                            // points predicted near the focal line (nu_max or lambda_min within two
-                            // bracket half-widths of D2) keep the plain searches for all limits:
-                            // there the GL action integrals resolve the integrands poorly and depend
-                            // on the limits to the last bits of the plain searches
-                            const bool nearFocal = pred[3 * i] + 2 * widths.w[0] >= 1 || pred[3 * i + 1] - 2 * widths.w[1] <= 0;
-                            double nlo, nhi;
-                            if(!nearFocal && predictedBracket(r, kind, pred[3 * i + k], widths.w[k], u0, lo, hi, &nlo, &nhi)) {
-                                const double tp = pred[3 * i + k], lmd = r.lambda - r.D2;
-                                double guess;
-                                if(kind == ROOT_NU_MAX) guess = fabs(r.nu) + tp * (r.D2 - fabs(r.nu));
-                                else if(kind == ROOT_LAMBDA_MIN) guess = r.D2 + tp * lmd;
-                                else {          // in the semi-infinite scaling about lambda_pos
-                                    const double L0 = log(fmax(r.D2 + lmd / tp, u0) / u0);
-                                    guess = L0 / (1 + L0);
-                                }
-                                if(isFinite(guess)) seeded = s.seed(guess, &x);
-                            }
-                        }
-                        if(STATS) {
-                            nSearch++;
-                            nSeeded += seeded;
-                        }
+                        if(STATS) nSearch++;
                     }
                 }
             }
         }
-        if(!__any_sync(FULL_MASK, busy)) break;
-        if(busy) {
-            double fx, dx;
-            limitRootEval(fnc, kind, u0, x, &fx, &dx);
-            if(LEARNED && verifying) {
-                // a root from a seeded search: F must have the sign of the plain bracket's end
-                // half-way between the root and that end (lambda_max: towards infinity in the
-                // scaled variable; lambda_min: towards D2; nu_max: towards D2), where it is
-                // negative; otherwise F has more roots there and the plain search decides
-                verifying = false;
-                if(STATS) nIter++;
-                const FudgeRecord& r = rec[point];
-                if(fx < 0) {
-                    busy = false;
-                    FudgeRecord& w = rec[point];
-                    if(kind == ROOT_NU_MAX) w.nuMax = verified;
-                    else if(kind == ROOT_LAMBDA_MIN) w.lambdaMin = verified;
-                    else w.lambdaMax = unscaleSemiInf(u0, verified, nullptr);
-                    if(iters) atomicAdd(iters + point, s.iter + 1);
-                } else {
-                    seeded = false;
-                    if(STATS) nFallback++;
-                    const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
-                    const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
-                    if(startPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
-                                  u0, fnc.D2, fnc.E, &x)) {
-                        busy = false;
-                        storePlainLimit(rec[point], kind, s, u0, fnc.nu);
-                    }
-                }
-            } else if(s.feed(fx, dx, &x)) {
-                if(STATS) nIter += s.iter;
-                bool check = false;     // the search goes on (a check evaluation or a plain search)
-                if(LEARNED && seeded) {
-                    // a seeded root is a candidate only inside the predicted bracket (it may have
-                    // come from another root of F in the plain bracket otherwise)
+        if(!__any_sync(FULL_MASK, mode != LANE_IDLE)) break;
+        // 2. the next iterate of every search that wants one: the first of a new search (replaced
+        //    by the predicted root when the prediction is usable) or the next of a running one
+        if(mode == LANE_PROPOSE) {
+            if(s.propose(&x))
+                finishSearch();
+            else {
+                mode = LANE_EVAL;
+                if(LEARNED && pred && fresh) {
+                    // points predicted near the focal line (nu_max or lambda_min within two
+                    // bracket half-widths of D2) keep the plain searches for all limits:
+                    // there the GL action integrals resolve the integrands poorly and depend
+                    // on the limits to the last bits of the plain searches
                     const FudgeRecord& r = rec[point];
                     const int k = kind == ROOT_NU_MAX ? 0 : kind == ROOT_LAMBDA_MIN ? 1 : 2;
+                    const bool nearFocal = pred[3 * point] + 2 * widths.w[0] >= 1 ||
+                                           pred[3 * point + 1] - 2 * widths.w[1] <= 0;
                     const double lo = kind == ROOT_NU_MAX ? fabs(r.nu) : kind == ROOT_LAMBDA_MIN ? r.lambdaLower : 0;
                     const double hi = kind == ROOT_NU_MAX ? r.nuUpper : kind == ROOT_LAMBDA_MIN ? r.lambdaPos : 1;
                     double nlo, nhi;
-                    predictedBracket(r, kind, pred[3 * point + k], widths.w[k], u0, lo, hi, &nlo, &nhi);
-                    if(isFinite(s.result) && s.result >= nlo && s.result <= nhi) {
-                        check = true;
-                        verifying = true;
-                        verified = s.result;
-                        x = 0.5 * (s.result + (kind == ROOT_LAMBDA_MIN ? lo : hi));
-                    } else {
-                        seeded = false;
-                        if(STATS) nFallback++;
-                        check = true;       // handled: the plain search runs from here
-                        if(startPlain(s, kind, ends ? ends + point : nullptr, lo, hi, fabs(lo - hi) * FUDGE_ACCURACY_RANGE,
-                                      u0, fnc.D2, fnc.E, &x)) {
-                            busy = false;
-                            storePlainLimit(rec[point], kind, s, u0, fnc.nu);
+                    if(!nearFocal && predictedBracket(r, kind, pred[3 * point + k], widths.w[k], u0, lo, hi, &nlo, &nhi)) {
+                        const double tp = pred[3 * point + k], lmd = r.lambda - r.D2;
+                        double guess;
+                        if(kind == ROOT_NU_MAX) guess = fabs(r.nu) + tp * (r.D2 - fabs(r.nu));
+                        else if(kind == ROOT_LAMBDA_MIN) guess = r.D2 + tp * lmd;
+                        else {          // in the semi-infinite scaling about lambda_pos
+                            const double L0 = log(fmax(r.D2 + lmd / tp, u0) / u0);
+                            guess = L0 / (1 + L0);
                         }
+                        if(isFinite(guess)) seeded = s.seed(guess, &x);
                     }
-                }
-                if(!check) {
-                    busy = false;
-                    storePlainLimit(rec[point], kind, s, u0, fnc.nu);
-                    if(iters) atomicAdd(iters + point, s.iter);
+                    if(STATS) nSeeded += seeded;
                 }
             }
+            fresh = false;
+        }
+        // 3. F (and F') at the points of the lanes that have one
+        double fx = 0, dx = 0;
+        if(mode == LANE_EVAL || mode == LANE_VERIFY) limitRootEval(fnc, kind, u0, x, &fx, &dx);
+        // 4. the values fed to the searches
+        if(mode == LANE_EVAL) {
+            const int r = s.take(fx, dx, &x);
+            if(r == 0) finishSearch();
+            else mode = r == 1 ? LANE_PROPOSE : LANE_EVAL;
+        } else if(LEARNED && mode == LANE_VERIFY) {
+            // a root from a seeded search: F must have the sign of the plain bracket's end
+            // half-way between the root and that end (lambda_max: towards infinity in the
+            // scaled variable; lambda_min: towards D2; nu_max: towards D2), where it is
+            // negative; otherwise F has more roots there and the plain search decides
+            if(STATS) nIter++;
+            if(fx < 0) {
+                mode = LANE_IDLE;
+                FudgeRecord& w = rec[point];
+                if(kind == ROOT_NU_MAX) w.nuMax = verified;
+                else if(kind == ROOT_LAMBDA_MIN) w.lambdaMin = verified;
+                else w.lambdaMax = unscaleSemiInf(u0, verified, nullptr);
+                if(iters) atomicAdd(iters + point, s.iter + 1);
+            } else
+                restartPlain();
         }
     }
     if(STATS && stats) {       // one atomic per warp and counter

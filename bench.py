@@ -551,7 +551,7 @@ def reference_secondary(pts1, ic1, T1, ic3, T3, ic5, T5, engine=None):
         res = []
         p1.eval(pts1[:1000], nthreads=cores)
         t0 = time.perf_counter()
-        phi, grad, _ = p1.eval(pts1, nthreads=cores)
+        phi, grad = p1.eval(pts1, nthreads=cores)
         dt = time.perf_counter() - t0
         parity = None
         if engine is not None:
@@ -720,7 +720,10 @@ TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 61.37e6
 TRAFFIC_PER_STEP_CFG2 = 5 * 103.02e6
 # executed FP64 flops (dadd + dmul + 2 dfma, ncu) per unit of the secondary workloads: per force
 # evaluation, per accepted DOP853 step (the rejected attempts' work included), per action
-FLOPS = {"forces1": None, "orbits1": None, "orbits3": None, "orbits5": None, "actions5": None}
+# (bench.py --profile-case under ncu; profiles/secondary_workloads_flops.md): forces 1.856e8 / 1e5,
+# orbits 1.105e11 / 3 307 982, 3.917e11 / 9 784 415, 9.331e11 / 68 712 155 accepted steps, actions of
+# the config-5 snapshot (prepare + roots + integrals) 5.215e8 / 20 000
+FLOPS = {"forces1": 1856.0, "orbits1": 33404.0, "orbits3": 40033.0, "orbits5": 13580.0, "actions5": 26075.0}
 FLOPS_SOURCE = "ncu FP64 instruction counts of the kernel on a case of this workload (bench.py --profile-case)"
 
 
@@ -733,12 +736,14 @@ def run_profile_case():
     """one launch of each workload's kernels on a small case, in a fixed order, with the units
     each launch processed (force evaluations, accepted steps, actions) printed as one JSON line:
     the ncu instruction counts of these launches divided by these units give the FLOPS table.
-    Lanes per orbit are fixed to 1 (the autotuner's trial would add launches of its own)."""
+    Lanes per orbit and the block size are fixed (1, 64: the autotuner's trial would add launches of
+    its own; neither changes the arithmetic of an orbit)."""
     import torch
     import agama_b200
     from agama_b200 import workloads
     dev = torch.device("cuda", 0)
     agama_b200.set_orbit_lanes(1)
+    agama_b200.set_orbit_block(64)
     units = {}
     pot1 = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg1.coef"))
     pts1 = workloads.dehnen_positions(100000, 1.0, q=(0.8, 0.6), seed=workloads.SEEDS["points1"])
@@ -760,6 +765,7 @@ def run_profile_case():
             torch.cuda.synchronize()
             units["actions5"] = n
     agama_b200.set_orbit_lanes(0)
+    agama_b200.set_orbit_block(0)
     print(json.dumps({"profile_case_units": units, "order": ["forces1", "orbits1", "orbits3", "orbits5", "actions5"]}))
 
 

@@ -113,7 +113,7 @@ def test_potential_from_density_on_device(name):
     rpot = ref.multipole_potential_from_density(mp, dens)
     pts = g["points"]
     phi, acc = pot.eval(pts, pot=True, acc=True)
-    rphi, rgrad, _ = rpot.eval(pts, nthreads=1)
+    rphi, rgrad = rpot.eval(pts, nthreads=1)
     r, _, _ = agama_b200.multipole_coefs_from_density([kv(d) for d in dens], **kv(mp))
     rad = np.linalg.norm(pts, axis=1)
     ephi = np.abs(phi - rphi) / np.abs(rphi)
