@@ -148,3 +148,28 @@ def test_action_finder_mixed_precision(cfg):
     err = check_actions(J32, J64)
     print(cfg, "mixed-precision actions vs FP64: max relative error %.3g" % err)
     assert np.array_equal(af(g["points"]), J64, equal_nan=True)  # the setting is off again
+
+
+@pytest.mark.parametrize("cfg", ["cfg4", "cfg5"])
+def test_mixed_precision_loosely_bound_orbits(cfg):
+    """the mixed-precision integrand on orbits reaching far out (apocentres up to ~1e6, where
+    (tau - Delta^2)^2 tau exceeds the FP32 range): within 1e-6 of the FP64 form"""
+    import agama_b200
+    pot = agama_b200.Potential(file=os.path.join(GOLDEN, cfg + ".coef"))
+    af = agama_b200.ActionFinder(pot)
+    rng = np.random.default_rng(17)
+    R = 10 ** rng.uniform(-1, 4, 400)
+    pos = np.column_stack([R, np.zeros_like(R), 0.3 * R * rng.uniform(-1, 1, 400)])
+    vesc = np.sqrt(-2 * pot.potential(pos))
+    u = rng.uniform(0.3, 0.995, 400)
+    d = rng.normal(size=(400, 3))
+    vel = d / np.linalg.norm(d, axis=1)[:, None] * (u * vesc)[:, None]
+    pts = np.hstack([pos, vel])
+    J64 = af(pts)
+    agama_b200.set_action_precision(True)
+    try:
+        J32 = af(pts)
+    finally:
+        agama_b200.set_action_precision(False)
+    err = check_actions(J32, J64)
+    print(cfg, "loosely bound orbits, mixed vs FP64: %.3g" % err)
