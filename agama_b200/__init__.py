@@ -182,6 +182,16 @@ class Potential:
             out.append(hess)
         return out[0] if len(out) == 1 else tuple(out)
 
+    def eval_cyl(self, points):
+        """potential, gradient (dR, dz, dphi) and Hessian (dR2, dz2, dphi2, dRdz, dzdphi, dRdphi) at
+        cylindrical points (R, z, phi), evaluated in cylindrical coordinates as the reference's
+        BasePotential::eval(PosCyl, ...) (host arrays)"""
+        p, single = _points(points, 3)
+        n = len(p)
+        phi, grad, hess = _host_empty(n), _host_empty((n, 3)), _host_empty((n, 6))
+        check(_native.lib().agama_evalPotentialCylMany(self._h, n, ptr(p), 0.0, ptr(phi), ptr(grad), ptr(hess)))
+        return (phi[0], grad[0], hess[0]) if single else (phi, grad, hess)
+
     def potential(self, points):
         return self.eval(points, pot=True)
 

@@ -31,6 +31,8 @@ SIGNATURES = {
     "agama_writeMultipoleCoefs": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, D, ctypes.c_int, D, D]),
     "agama_evalPotentialMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
     "agama_evalPotentialManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
+    "agama_evalPotentialCylMany": (ctypes.c_int, [VP, ctypes.c_long, D, ctypes.c_double, D, D, D]),
+    "agama_evalPotentialCylManyDevice": (ctypes.c_int, [VP, ctypes.c_long, VP, VP, VP, VP, VP]),
     "agama_createDensity": (VP, [ctypes.c_char_p]),
     "agama_deleteDensity": (None, [VP]),
     "agama_evalDensity": (ctypes.c_double, [VP, D, ctypes.c_double]),

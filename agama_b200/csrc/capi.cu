@@ -232,6 +232,34 @@ int agama_evalPotentialMany(const agama_Potential* p, long n, const double* pos,
     });
 }
 
+int agama_evalPotentialCylManyDevice(const agama_Potential* p, long n, const double* pos,
+    double* phi, double* deriv, double* deriv2, void* stream)
+{
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && !pos)) throw std::invalid_argument("evalPotentialCylManyDevice: invalid arguments");
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        launchEvalPotential(p->pot->view, n, pos, phi, deriv, deriv2, static_cast<cudaStream_t>(stream), true);
+    });
+}
+
+int agama_evalPotentialCylMany(const agama_Potential* p, long n, const double* pos, double time,
+    double* phi, double* deriv, double* deriv2)
+{
+    (void)time;
+    return guarded([&] {
+        if(!p || n < 0 || (n > 0 && !pos)) throw std::invalid_argument("evalPotentialCylMany: invalid arguments");
+        if(n == 0) return;
+        AGB_CUDA(cudaSetDevice(p->pot->device));
+        const MultipoleView& M = p->pot->view;
+        runChunked(n, { { pos, 3 * sizeof(double) } },
+            { { phi, sizeof(double) }, { deriv, 3 * sizeof(double) }, { deriv2, 6 * sizeof(double) } },
+            [&](long, long count, void* const* in, void* const* out, cudaStream_t s) {
+                launchEvalPotential(M, count, static_cast<const double*>(in[0]), static_cast<double*>(out[0]),
+                    static_cast<double*>(out[1]), static_cast<double*>(out[2]), s, true);
+            });
+    });
+}
+
 double agama_evalPotential(const agama_Potential* p, const double pos[3], double time,
     double deriv[3], double deriv2[6])
 {

@@ -24,6 +24,28 @@ __global__ void __launch_bounds__(256) evalPotentialKernel(const MultipoleView M
     if(NQ == 6 && hess)
         for(int k = 0; k < 6; k++) hess[6 * i + k] = h[k];
 }
+
+/// the same at n cylindrical points (R, z, phi), derivatives in cylindrical coordinates
+/// (dR, dz, dphi; dR2, dz2, dphi2, dRdz, dzdphi, dRdphi) straight from the evaluator, as the
+/// reference's BasePotentialCyl::evalCyl returns them (no round trip through Cartesian
+/// derivatives, which loses the phi derivatives to cancellation at large R)
+template<int NQ, int KIND>
+__global__ void __launch_bounds__(256) evalPotentialCylKernel(const MultipoleView M, long n,
+    const double* __restrict__ pos, double* __restrict__ phi, double* __restrict__ grad,
+    double* __restrict__ hess)
+{
+    const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+    if(i >= n) return;
+    double p;
+    CylDerivs g; CylHess h;
+    evalMultipoleCyl<NQ, KIND>(M, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], &p, &g, &h);
+    if(phi) phi[i] = p;
+    if(NQ >= 3 && grad) { grad[3 * i] = g.dR; grad[3 * i + 1] = g.dz; grad[3 * i + 2] = g.dphi; }
+    if(NQ == 6 && hess) {
+        hess[6 * i] = h.dR2; hess[6 * i + 1] = h.dz2; hess[6 * i + 2] = h.dphi2;
+        hess[6 * i + 3] = h.dRdz; hess[6 * i + 4] = h.dzdphi; hess[6 * i + 5] = h.dRdphi;
+    }
+}
 }  // namespace
 
 void setError(const std::string& msg) { g_error = msg; }
@@ -38,13 +60,15 @@ void requireDevice()
 }
 
 void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
-    double* grad, double* hess, cudaStream_t stream)
+    double* grad, double* hess, cudaStream_t stream, bool cylindrical)
 {
     if(n <= 0) return;
     const int block = 256;
     const long grid = (n + block - 1) / block;
     const int nq = hess ? 6 : grad ? 3 : 1, kind = evalKindOf(M);
-#define AGB_LAUNCH(NQ_, K_) evalPotentialKernel<NQ_, K_><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess)
+#define AGB_LAUNCH(NQ_, K_) \
+    (cylindrical ? evalPotentialCylKernel<NQ_, K_><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess) \
+                 : evalPotentialKernel<NQ_, K_><<<grid, block, 0, stream>>>(M, n, pos, phi, grad, hess))
     if(kind == EVAL_AXI)       { if(nq == 6) AGB_LAUNCH(6, EVAL_AXI);     else if(nq == 3) AGB_LAUNCH(3, EVAL_AXI);     else AGB_LAUNCH(1, EVAL_AXI); }
     else if(kind == EVAL_FAST) { if(nq == 6) AGB_LAUNCH(6, EVAL_FAST);    else if(nq == 3) AGB_LAUNCH(3, EVAL_FAST);    else AGB_LAUNCH(1, EVAL_FAST); }
     else                       { if(nq == 6) AGB_LAUNCH(6, EVAL_GENERAL); else if(nq == 3) AGB_LAUNCH(3, EVAL_GENERAL); else AGB_LAUNCH(1, EVAL_GENERAL); }

@@ -79,8 +79,9 @@ DeviceActionFinder* createDeviceActionFinder(DevicePotential* pot, const FinderT
 FinderTablesHost buildFinderTables(const DevicePotential& P);
 
 /// launch helpers (defined in the .cu files)
+/// (cylindrical: points (R, z, phi) and derivatives in cylindrical coordinates)
 void launchEvalPotential(const MultipoleView& M, long n, const double* pos, double* phi,
-    double* grad, double* hess, cudaStream_t stream);
+    double* grad, double* hess, cudaStream_t stream, bool cylindrical = false);
 /// density (Laplacian / 4 pi inside the grid, closed form outside) at n Cartesian points
 void launchDensity(const MultipoleView& M, long n, const double* pos, double* rho, cudaStream_t stream);
 /// radius queries in the equatorial plane of the azimuthally averaged potential: a = E (or L for

@@ -140,6 +140,19 @@ int agama_evalPotentialMany(const agama_Potential* potential, long n, const doub
 int agama_evalPotentialManyDevice(const agama_Potential* potential, long n, const double* pos,
     double* phi, double* deriv, double* deriv2, void* stream);
 
+/* Batched potential / gradient / Hessian at n cylindrical points, host buffers: pos is n x 3 in the
+   order (R, z, phi) of the reference's coord::PosCyl; deriv n x 3 (dR, dz, dphi) as coord::GradCyl;
+   deriv2 n x 6 (dR2, dz2, dphi2, dRdz, dzdphi, dRdphi) as coord::HessCyl.  Replaces n calls of
+   BasePotential::eval(PosCyl, ...), which a Multipole answers natively in cylindrical coordinates
+   (BasePotentialCyl::evalCyl, src/potential_base.h:237-262; Multipole::evalCyl,
+   src/potential_multipole.cpp:1538-1548). */
+int agama_evalPotentialCylMany(const agama_Potential* potential, long n, const double* pos, double time,
+    double* phi, double* deriv, double* deriv2);
+
+/* The same on device buffers, enqueued on the given stream. */
+int agama_evalPotentialCylManyDevice(const agama_Potential* potential, long n, const double* pos,
+    double* phi, double* deriv, double* deriv2, void* stream);
+
 /* Batched density of a potential at n points (n x 3), host buffers: n calls of agama_evalDensity
    (the reference's Python Density.density batches the same, src/interface_python.cpp:2439). */
 int agama_evalDensityMany(const agama_Potential* potential, long n, const double* pos, double time,

@@ -39,11 +39,6 @@ namespace agama_b200 {
 
 namespace detail {
 inline void checkRef(int rc) { if(rc != 0) throw std::runtime_error(agama_getError()); }
-
-/// Cartesian gradient / Hessian (order xx, yy, zz, xy, yz, zx) -> cylindrical ones at angle phi
-/// (the chain rule of coord::toDeriv, src/coord.cpp:101-135)
-inline void carToCylDerivs(double R, double phi, const double g[3], const double h[6],
-    ::coord::GradCyl* gc, ::coord::HessCyl* hc);
 }  // namespace detail
 
 /** A Multipole potential evaluated on the B200 engine, usable wherever the reference takes a
@@ -98,21 +93,23 @@ public:
         }
     }
 
-    /// the same at n cylindrical points, as n calls of eval(PosCyl, ...)
+    /// the same at n cylindrical points, as n calls of eval(PosCyl, ...): evaluated in cylindrical
+    /// coordinates on the engine, as the reference's Multipole::evalCyl does
     void evalmanyCyl(size_t n, const ::coord::PosCyl pos[], double pot[],
         ::coord::GradCyl deriv[] = NULL, ::coord::HessCyl deriv2[] = NULL, double time = 0) const
     {
-        std::vector<double> x(3 * n), phi(n), g(3 * n), hh(deriv2 ? 6 * n : 0);
+        std::vector<double> x(3 * n), phi(n), g(deriv ? 3 * n : 0), hh(deriv2 ? 6 * n : 0);
+        for(size_t i = 0; i < n; i++) { x[3 * i] = pos[i].R; x[3 * i + 1] = pos[i].z; x[3 * i + 2] = pos[i].phi; }
+        detail::checkRef(agama_evalPotentialCylMany(h, static_cast<long>(n), x.data(), time, pot ? pot : phi.data(),
+            deriv ? g.data() : NULL, deriv2 ? hh.data() : NULL));
         for(size_t i = 0; i < n; i++) {
-            x[3 * i] = pos[i].R * std::cos(pos[i].phi); x[3 * i + 1] = pos[i].R * std::sin(pos[i].phi);
-            x[3 * i + 2] = pos[i].z;
+            if(deriv) { deriv[i].dR = g[3 * i]; deriv[i].dz = g[3 * i + 1]; deriv[i].dphi = g[3 * i + 2]; }
+            if(deriv2) {
+                const double* q = &hh[6 * i];
+                deriv2[i].dR2 = q[0]; deriv2[i].dz2 = q[1]; deriv2[i].dphi2 = q[2];
+                deriv2[i].dRdz = q[3]; deriv2[i].dzdphi = q[4]; deriv2[i].dRdphi = q[5];
+            }
         }
-        detail::checkRef(agama_evalPotentialMany(h, static_cast<long>(n), x.data(), time, pot ? pot : phi.data(),
-            (deriv || deriv2) ? g.data() : NULL, deriv2 ? hh.data() : NULL));
-        for(size_t i = 0; i < n; i++)
-            if(deriv || deriv2)
-                detail::carToCylDerivs(pos[i].R, pos[i].phi, &g[3 * i], deriv2 ? &hh[6 * i] : NULL,
-                    deriv ? &deriv[i] : NULL, deriv2 ? &deriv2[i] : NULL);
     }
 
     /// batched density (overrides the reference's per-point loop)
@@ -224,23 +221,6 @@ private:
     std::shared_ptr<const MultipoleB200> pot;
     agama_ActionFinder* h;
 };
-
-inline void detail::carToCylDerivs(double R, double phi, const double g[3], const double h[6],
-    ::coord::GradCyl* gc, ::coord::HessCyl* hc)
-{
-    const double c = std::cos(phi), s = std::sin(phi);
-    const double dR = g[0] * c + g[1] * s, dphi = R * (g[1] * c - g[0] * s);
-    if(gc) { gc->dR = dR; gc->dz = g[2]; gc->dphi = dphi; }
-    if(hc && h) {
-        const double xx = h[0], yy = h[1], zz = h[2], xy = h[3], yz = h[4], zx = h[5];
-        hc->dR2 = xx * c * c + yy * s * s + 2 * xy * c * s;
-        hc->dz2 = zz;
-        hc->dphi2 = R * R * (xx * s * s + yy * c * c - 2 * xy * c * s) - R * dR;
-        hc->dRdz = zx * c + yz * s;
-        hc->dzdphi = R * (yz * c - zx * s);
-        hc->dRdphi = R * ((yy - xx) * c * s + xy * (c * c - s * s)) + (g[1] * c - g[0] * s);
-    }
-}
 
 }  // namespace agama_b200
 

@@ -84,3 +84,29 @@ def test_single_point_entry(potentials):
 def test_empty_batch(potentials):
     out = potentials["cfg1"].eval(np.zeros((0, 3)))
     assert out.shape == (0,)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_cylindrical_evaluation_matches_reference(potentials, name):
+    """Potential.eval_cyl (agama_evalPotentialCylMany) against the reference's
+    BasePotential::eval(PosCyl, ...) built here, at the golden points in cylindrical coordinates:
+    the same bounds as the Cartesian evaluation (value and gradient 1e-12, 1e-11 beyond r_max;
+    Hessian 1e-9 of its norm), including the phi derivatives far out, which a conversion from
+    Cartesian derivatives would lose to cancellation (~eps R^2 of the Hessian)"""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+    g = np.load(os.path.join(GOLDEN, "potential_%s.npz" % name))
+    x = g["points"]
+    cyl = np.column_stack([np.hypot(x[:, 0], x[:, 1]), x[:, 2], np.arctan2(x[:, 1], x[:, 0])])
+    phi, grad, hess = potentials[name].eval_cyl(cyl)
+    rphi, rgrad, rhess = ref.Potential(file=os.path.join(GOLDEN, name + ".coef")).eval_cyl(cyl)
+    tol = np.where(np.linalg.norm(x, axis=1) > grid_radii(name)[-1], 1e-11, 1e-12)
+    ephi = np.abs(phi - rphi) / np.abs(rphi)
+    assert np.all(ephi <= tol), ephi.max()
+    # the phi derivative is compared in the units of the other two (dPhi/dphi / R)
+    scale = np.column_stack([np.ones(len(x)), np.ones(len(x)), np.where(cyl[:, 0] > 0, 1 / cyl[:, 0], 1.0)])
+    egrad = rel_err_vec(grad * scale, rgrad * scale)
+    assert np.all(egrad <= tol), egrad.max()
+    ehess = rel_err_vec(hess, rhess)
+    assert ehess.max() <= 1e-9, ehess.max()

