@@ -67,6 +67,33 @@ AGB_HD int binSearch(double x, const double* arr, int size)
     return lo;
 }
 
+/** binSearch with the first guess from scale = (size - 1) / (arr[size-1] - arr[0]), precomputed,
+    instead of a division: the guess only picks where the search starts, so the result is that of
+    binSearch. */
+AGB_HD int binSearchScaled(double x, const double* arr, int size, double scale)
+{
+    if(size < 1 || !(x >= arr[0]))
+        return -1;
+    if(x > arr[size-1] || size < 2)
+        return size - 1;
+    int lo = static_cast<int>((x - arr[0]) * scale);
+    if(lo >= size - 1)
+        return size - 2;
+    int hi = size - 1;
+    if(x >= arr[lo]) {
+        if(x < arr[lo+1])
+            return lo;
+    } else {
+        hi = lo;
+        lo = 0;
+    }
+    while(hi > lo + 1) {
+        int mid = (hi + lo) / 2;
+        if(arr[mid] > x) hi = mid; else lo = mid;
+    }
+    return lo;
+}
+
 /** Quintic Hermite interpolation of K functions on the segment [xl, xh] from the values and the
     first and second derivatives at both ends; returns f, f', f'' (each output may be null).
     The polynomial is written as the Taylor part at xl plus corrections in the three
@@ -74,7 +101,22 @@ AGB_HD int binSearch(double x, const double* arr, int size)
     Same interpolant and special case x == xh as evalQuinticSplines, reference
     src/math_spline.cpp:654-731. */
 template<int K, typename T = double>
+AGB_HD void quinticSegmentR(T x, T xl, T xh, T hi,
+    const T* fl, const T* fh, const T* f1l, const T* f1h,
+    const T* f2l, const T* f2h, T* f, T* df, T* d2f);
+
+template<int K, typename T = double>
 AGB_HD void quinticSegment(T x, T xl, T xh,
+    const T* fl, const T* fh, const T* f1l, const T* f1h,
+    const T* f2l, const T* f2h, T* f, T* df, T* d2f)
+{
+    quinticSegmentR<K, T>(x, xl, xh, 1 / (xh - xl), fl, fh, f1l, f1h, f2l, f2h, f, df, d2f);
+}
+
+/// the same with the reciprocal width hi = 1 / (xh - xl) given (tabulated per grid interval: the
+/// correctly rounded reciprocal, so the results are those of quinticSegment bit for bit)
+template<int K, typename T>
+AGB_HD void quinticSegmentR(T x, T xl, T xh, T hi,
     const T* fl, const T* fh, const T* f1l, const T* f1h,
     const T* f2l, const T* f2h, T* f, T* df, T* d2f)
 {
@@ -87,7 +129,7 @@ AGB_HD void quinticSegment(T x, T xl, T xh,
         }
         return;
     }
-    const T dx = x - xl, hdx2 = T(0.5) * dx * dx, h = xh - xl, hi = 1 / h, h2 = h * h;
+    const T dx = x - xl, hdx2 = T(0.5) * dx * dx, h = xh - xl, h2 = h * h;
     const T t = dx * hi, t2 = t * t, t3 = t * t2, omt = t * (1 - t);
     // basis polynomials for the three defects and their first two derivatives
     const T bf   = t3 * (10 - t * (15 - 6 * t));

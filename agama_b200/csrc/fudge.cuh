@@ -129,9 +129,13 @@ struct FudgeFunction {
         const double tmd = tau - D2;
         *val = (tmd != 0 ? (E * tau - I - Phi * mult) * tmd : 0) - Lz * Lz / 2 * tau;
         if(DER || DER2) {
-            const double dRdl = 0.5 * R / lmd, dRdn = 0.5 * R / nmd * sgn, dzdl = 0.5 * z / lam, dzdn = 0.5 * z / n;
+            // dR/dtau, dz/dtau along the coordinate that tau moves (lambda or nu): only that pair
+            // is divided out
             const bool lbranch = tau >= D2;
-            const double dPhidtau = lbranch ? g.dR * dRdl + g.dz * dzdl : g.dR * dRdn + g.dz * dzdn;
+            double dRdt, dzdt;
+            if(lbranch) { dRdt = 0.5 * R / lmd; dzdt = 0.5 * z / lam; }
+            else        { dRdt = 0.5 * R / nmd * sgn; dzdt = 0.5 * z / n; }
+            const double dPhidtau = g.dR * dRdt + g.dz * dzdt;
             if(DER)
                 *der = E * (tau + tmd) - Lz * Lz / 2 - I - (mult + tmd) * Phi -
                        (tmd != 0 ? tmd * mult * dPhidtau : 0);
@@ -139,11 +143,11 @@ struct FudgeFunction {
                 double d2;
                 if(lbranch) {
                     const double d2Rdl2 = -0.25 * R / pow2(lmd), d2zdl2 = -0.25 * z / pow2(lam);
-                    d2 = h.dR2 * pow2(dRdl) + h.dz2 * pow2(dzdl) + 2 * h.dRdz * dRdl * dzdl +
+                    d2 = h.dR2 * pow2(dRdt) + h.dz2 * pow2(dzdt) + 2 * h.dRdz * dRdt * dzdt +
                          g.dR * d2Rdl2 + g.dz * d2zdl2;
                 } else {
                     const double d2Rdn2 = -0.25 * R / pow2(nmd), d2zdn2 = -0.25 * z / pow2(n);
-                    d2 = h.dR2 * pow2(dRdn) + h.dz2 * pow2(dzdn) + 2 * h.dRdz * dRdn * dzdn +
+                    d2 = h.dR2 * pow2(dRdt) + h.dz2 * pow2(dzdt) + 2 * h.dRdz * dRdt * dzdt +
                          g.dR * d2Rdn2 + g.dz * d2zdn2;
                 }
                 *der2 = 2 * (E - Phi - (mult + tmd) * dPhidtau) - tmd * mult * d2;

@@ -24,7 +24,7 @@ constexpr unsigned FULL_MASK = 0xffffffffu;
 /// MIXED: the integrand's arithmetic after F(tau) in FP32 (fudgeMomentumNode32) and the weighted
 /// terms summed in FP32 with a compensation term (Kahan), converted to FP64 at the end.
 template<bool MIXED>
-__global__ void __launch_bounds__(INTEGRAL_BLOCK, 4) fudgeIntegralKernel(const __grid_constant__ MultipoleView M,
+__global__ void __launch_bounds__(INTEGRAL_BLOCK, 5) fudgeIntegralKernel(const __grid_constant__ MultipoleView M,
     const __grid_constant__ GLRules gl, long n, const FudgeRecord* __restrict__ rec, double* __restrict__ act,
     unsigned long long* __restrict__ counter)
 {

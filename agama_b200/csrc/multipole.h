@@ -49,6 +49,9 @@ struct MultipoleView {
     double rInnerSq, rOuterSq;   // squared switching radii to the asymptotic expansions
     int nr; const double* lnr;   // radial grid in ln r
     int nt; const double* tau;   // angular grid in tau (2-D case)
+    const double* lnrInvH;       // 1 / (lnr[k+1] - lnr[k]), k < nr - 1 (correctly rounded)
+    const double* tauInvH;       // 1 / (tau[j+1] - tau[j]), j < nt - 1
+    double lnrScale, tauScale;   // (n - 1) / (grid[n-1] - grid[0]): binSearchScaled's first guess
     int splSlot[2 * LMAX_MAX + 1];  // slot of the 2-D spline for m (index m+mmax), -1 if empty
     const double* spl2d;  // [slot][nr][nt][NODE_STRIDE]: f fx fy fxx fxy fyy fxxy fxyy fxxyy pad
     const float* spl2d32; // the same table rounded to FP32 (mixed-precision evaluation of m != 0)

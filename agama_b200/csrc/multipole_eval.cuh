@@ -211,7 +211,7 @@ __device__ void evalInterp1d(const MultipoleView& M, double R, double z, double 
     const HarmIndices& ind = M.ind;
     const double r = sqrt(R * R + z * z), logr = log(r);
     double C[9], dC[9], d2C[9];
-    const int k = binSearch(logr, M.lnr, M.nr);
+    const int k = binSearchScaled(logr, M.lnr, M.nr, M.lnrScale);
     auto spline = [&](int c, double* f, double* df, double* d2f) {
         const double* t = M.spl1d + static_cast<size_t>(c) * M.nr * 3;
         if(k < 0 || k >= M.nr - 1) {   // linear extrapolation beyond the grid
@@ -225,7 +225,7 @@ __device__ void evalInterp1d(const MultipoleView& M, double R, double z, double 
         const double* a = t + 3 * k;
         const double fl[1] = { ldg(a) }, fh[1] = { ldg(a + 3) }, f1l[1] = { ldg(a + 1) }, f1h[1] = { ldg(a + 4) },
             f2l[1] = { ldg(a + 2) }, f2h[1] = { ldg(a + 5) };
-        quinticSegment<1>(logr, M.lnr[k], M.lnr[k + 1], fl, fh, f1l, f1h, f2l, f2h, f, df, d2f);
+        quinticSegmentR<1>(logr, M.lnr[k], M.lnr[k + 1], M.lnrInvH[k], fl, fh, f1l, f1h, f2l, f2h, f, df, d2f);
     };
     spline(0, &C[0], NQ >= 3 ? &dC[0] : nullptr, NQ == 6 ? &d2C[0] : nullptr);
     if(M.logScaling) {
@@ -264,10 +264,11 @@ __device__ void evalInterp1d(const MultipoleView& M, double R, double z, double 
 
 /** 2-D quintic spline of one harmonic at (x = ln r, y = tau) inside cell (xi, yi): value and
     the requested derivatives.  Reference QuinticSpline2d::evalDeriv, src/math_spline.cpp:2535-2597
-    (corner values shifted by one corner value to limit round-off). */
+    (corner values shifted by one corner value to limit round-off).  xhi, yhi: the tabulated
+    reciprocal widths of the cell. */
 template<int NQ>
 __device__ __forceinline__ void spline2dCell(const double* tab, int nt, int xi, int yi,
-    double x, double xl, double xh, double y, double yl, double yh,
+    double x, double xl, double xh, double y, double yl, double yh, double xhi, double yhi,
     double* z, double* zx, double* zy, double* zxx, double* zxy, double* zyy)
 {
     const double* nll = tab + (static_cast<size_t>(xi) * nt + yi) * NODE_STRIDE;  // (xlow, ylow)
@@ -290,13 +291,13 @@ __device__ __forceinline__ void spline2dCell(const double* tab, int nt, int xi, 
     const double f2l[6] = { ll[5], ul[5], ll[7], ul[7], ll[8], ul[8] };
     const double f2u[6] = { lu[5], uu[5], lu[7], uu[7], lu[8], uu[8] };
     double F[6], dF[6], d2F[6];
-    quinticSegment<6>(y, yl, yh, fl, fu, f1l, f1u, f2l, f2u, F, NQ >= 3 ? dF : nullptr, NQ == 6 ? d2F : nullptr);
-    quinticSegment<1>(x, xl, xh, &F[0], &F[1], &F[2], &F[3], &F[4], &F[5], z, zx, zxx);
+    quinticSegmentR<6>(y, yl, yh, yhi, fl, fu, f1l, f1u, f2l, f2u, F, NQ >= 3 ? dF : nullptr, NQ == 6 ? d2F : nullptr);
+    quinticSegmentR<1>(x, xl, xh, xhi, &F[0], &F[1], &F[2], &F[3], &F[4], &F[5], z, zx, zxx);
     *z += off;
     if(NQ >= 3)
-        quinticSegment<1, double>(x, xl, xh, &dF[0], &dF[1], &dF[2], &dF[3], &dF[4], &dF[5], zy, zxy, nullptr);
+        quinticSegmentR<1, double>(x, xl, xh, xhi, &dF[0], &dF[1], &dF[2], &dF[3], &dF[4], &dF[5], zy, zxy, nullptr);
     if(NQ == 6)
-        quinticSegment<1, double>(x, xl, xh, &d2F[0], &d2F[1], &d2F[2], &d2F[3], &d2F[4], &d2F[5], zyy, nullptr, nullptr);
+        quinticSegmentR<1, double>(x, xl, xh, xhi, &d2F[0], &d2F[1], &d2F[2], &d2F[3], &d2F[4], &d2F[5], zyy, nullptr, nullptr);
 }
 
 /** The same cell in FP32 (the mixed-precision evaluation of the m != 0 harmonics): node values
@@ -356,10 +357,11 @@ __device__ void evalInterp2d(const MultipoleView& M, double R, double z, double 
     double Cm[6 * (2 * LMAX_MAX + 1)];
     double* Phi = Cm;  double* dlnr = Cm + nm;  double* dtau = Cm + 2 * nm;
     double* dlnr2 = Cm + 3 * nm;  double* dlnrdtau = Cm + 4 * nm;  double* dtau2 = Cm + 5 * nm;
-    const int xi = binSearch(logr, M.lnr, M.nr), yi = binSearch(tau, M.tau, M.nt);
+    const int xi = binSearchScaled(logr, M.lnr, M.nr, M.lnrScale), yi = binSearchScaled(tau, M.tau, M.nt, M.tauScale);
     const bool inside = !(xi < 0 || xi >= M.nr - 1 || yi < 0 || yi >= M.nt - 1);
     const double xl = inside ? M.lnr[xi] : 0, xh = inside ? M.lnr[xi + 1] : 0;
     const double yl = inside ? M.tau[yi] : 0, yh = inside ? M.tau[yi + 1] : 0;
+    const double xhi = inside ? M.lnrInvH[xi] : 0, yhi = inside ? M.tauInvH[yi] : 0;
     for(int mm = 0; mm < nm; mm++) {
         const int m = mm + mmin;
         if(ind.lmin(m) > ind.lmax) continue;
@@ -369,7 +371,7 @@ __device__ void evalInterp2d(const MultipoleView& M, double R, double z, double 
         }
         const double* tab = M.spl2d + static_cast<size_t>(M.splSlot[m + ind.mmax]) * M.nr * M.nt * NODE_STRIDE;
         double dummy;
-        spline2dCell<NQ>(tab, M.nt, xi, yi, logr, xl, xh, tau, yl, yh, &Phi[mm],
+        spline2dCell<NQ>(tab, M.nt, xi, yi, logr, xl, xh, tau, yl, yh, xhi, yhi, &Phi[mm],
             NQ >= 3 ? &dlnr[mm] : &dummy, NQ >= 3 ? &dtau[mm] : &dummy,
             NQ == 6 ? &dlnr2[mm] : &dummy, NQ == 6 ? &dlnrdtau[mm] : &dummy, NQ == 6 ? &dtau2[mm] : &dummy);
     }
@@ -457,10 +459,11 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
     const unsigned gmask = G > 1 ? groupMask<G>() : 0u;
     const double r = sqrt(R * R + z * z), logr = log(r), rpRinv = 1. / (r + fabs(R));
     const double tau = R == 0 ? signOf(z) : z * rpRinv;
-    const int xi = binSearch(logr, M.lnr, M.nr), yi = binSearch(tau, M.tau, M.nt);
+    const int xi = binSearchScaled(logr, M.lnr, M.nr, M.lnrScale), yi = binSearchScaled(tau, M.tau, M.nt, M.tauScale);
     const bool inside = !(xi < 0 || xi >= M.nr - 1 || yi < 0 || yi >= M.nt - 1);
     const int xs = inside ? xi : 0, ys = inside ? yi : 0;
     const double xl = M.lnr[xs], xh = M.lnr[xs + 1], yl = M.tau[ys], yh = M.tau[ys + 1];
+    const double xhi = M.lnrInvH[xs], yhi = M.tauInvH[ys];
     const size_t slotStride = static_cast<size_t>(M.nr) * M.nt * NODE_STRIDE;
     double P[MAXS], Dr[MAXS], Dt[MAXS], Drr[MAXS], Drt[MAXS], Dtt[MAXS];
 #pragma unroll
@@ -472,7 +475,7 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
                     &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
             else
                 spline2dCell<NQ>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
-                    &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
+                    xhi, yhi, &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
             if(!inside) P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = NAN;
         }
     }

@@ -87,6 +87,15 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
         const MultipoleHost& H = P->host;
         P->lnr.upload(H.lnr);
         P->tau.upload(H.tau);
+        // reciprocal interval widths (IEEE division on the host and on the device give the same
+        // correctly rounded value, so the spline segments built from them are bit-identical)
+        auto invWidths = [](const std::vector<double>& g) {
+            std::vector<double> w(g.size() > 1 ? g.size() - 1 : 1, 0.0);
+            for(size_t k = 0; k + 1 < g.size(); k++) w[k] = 1 / (g[k + 1] - g[k]);
+            return w;
+        };
+        P->lnrInvH.upload(invWidths(H.lnr));
+        P->tauInvH.upload(invWidths(H.tau));
         P->spl2d.upload(H.spl2d);
         P->spl2d32.upload(std::vector<float>(H.spl2d.begin(), H.spl2d.end()));
         P->spl1d.upload(H.spl1d);
@@ -103,6 +112,13 @@ DevicePotential* createDevicePotential(const std::vector<double>& radii,
         V.lnr = P->lnr.ptr;
         V.nt = static_cast<int>(H.tau.size());
         V.tau = P->tau.ptr;
+        V.lnrInvH = P->lnrInvH.ptr;
+        V.tauInvH = P->tauInvH.ptr;
+        auto guessScale = [](const std::vector<double>& g) {
+            return g.size() > 1 ? static_cast<double>(g.size() - 1) / (g.back() - g.front()) : 0.0;
+        };
+        V.lnrScale = guessScale(H.lnr);
+        V.tauScale = guessScale(H.tau);
         for(int i = 0; i < 2 * LMAX_MAX + 1; i++) V.splSlot[i] = H.splSlot[i];
         V.spl2d = P->spl2d.ptr;
         V.spl2d32 = P->spl2d32.ptr;

@@ -46,7 +46,7 @@ struct DevBuf {
 struct DevicePotential {
     int device = 0;
     MultipoleHost host;
-    DevBuf<double> lnr, tau, spl2d, spl1d, innerS, innerU, innerW, outerS, outerU, outerW;
+    DevBuf<double> lnr, tau, lnrInvH, tauInvH, spl2d, spl1d, innerS, innerU, innerW, outerS, outerU, outerW;
     DevBuf<float> spl2d32;
     MultipoleView view;
     /// the axisymmetric (m = 0) part, used by the action finder (same as the full potential
