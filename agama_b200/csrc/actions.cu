@@ -84,7 +84,7 @@ constexpr long POINTS_PER_PASS = 1L << 20;     // records of one pass: 128 MB of
 /// Delta used, root-finder iterations (zeroed here, counted by phase 2).  ends[i]: F and F' at the
 /// ends of the record's plain root brackets, for the root searches.
 template<bool FINDER>
-__global__ void __launch_bounds__(PREPARE_BLOCK, 4) fudgePrepareKernel(const __grid_constant__ MultipoleView M,
+__global__ void __launch_bounds__(PREPARE_BLOCK, 5) fudgePrepareKernel(const __grid_constant__ MultipoleView M,
     const __grid_constant__ FudgeTables F, long n, const double* __restrict__ posvel, const double* __restrict__ fd,
     double fd0, FudgeRecord* __restrict__ rec, double* __restrict__ act, double* __restrict__ fdOut,
     int* __restrict__ iters, float* __restrict__ features, FudgeEnds* __restrict__ ends)

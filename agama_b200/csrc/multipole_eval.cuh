@@ -275,14 +275,15 @@ __device__ __forceinline__ void spline2dCell(const double* tab, int nt, int xi, 
     const double* nlu = nll + NODE_STRIDE;                                         // (xlow, yupp)
     const double* nul = nll + static_cast<size_t>(nt) * NODE_STRIDE;               // (xupp, ylow)
     const double* nuu = nul + NODE_STRIDE;                                         // (xupp, yupp)
-    // node layout: 0 f, 1 fx, 2 fy, 3 fxx, 4 fxy, 5 fyy, 6 fxxy, 7 fxyy, 8 fxxyy
-    double ll[10], lu[10], ul[10], uu[10];
+    // node layout: 0 f, 1 fx, 2 fy, 3 fxx, 4 fxy, 5 fyy, 6 fxxy, 7 fxyy, 8 fxxyy (9: padding, not read)
+    double ll[9], lu[9], ul[9], uu[9];
 #pragma unroll
-    for(int q = 0; q < 5; q++) {
+    for(int q = 0; q < 4; q++) {
         double2 a = ldg2(nll + 2 * q), b = ldg2(nlu + 2 * q), c = ldg2(nul + 2 * q), d = ldg2(nuu + 2 * q);
         ll[2 * q] = a.x; ll[2 * q + 1] = a.y; lu[2 * q] = b.x; lu[2 * q + 1] = b.y;
         ul[2 * q] = c.x; ul[2 * q + 1] = c.y; uu[2 * q] = d.x; uu[2 * q + 1] = d.y;
     }
+    ll[8] = ldg(nll + 8); lu[8] = ldg(nlu + 8); ul[8] = ldg(nul + 8); uu[8] = ldg(nuu + 8);
     const double off = x == xh ? (y == yh ? uu[0] : ul[0]) : (y == yh ? lu[0] : ll[0]);
     const double fl[6]  = { ll[0] - off, ul[0] - off, ll[1], ul[1], ll[3], ul[3] };
     const double fu[6]  = { lu[0] - off, uu[0] - off, lu[1], uu[1], lu[3], uu[3] };

@@ -356,7 +356,15 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
                              graph5.status[:REF_SAMPLE["orbits5"]].cpu().numpy())
     af5 = agama_b200.ActionFinder(pot5)
     snap = graph5.final.clone()
+    lib = agama_b200._native.lib()
+    import ctypes
+    af5(snap)
+    torch.cuda.synchronize()
+    agama_b200._native.check(lib.agama_actionPhaseTiming(1, None, None))    # CUDA events around each phase
     ta, J5 = timed(lambda: af5(snap), 3, 5)
+    ph5, np5 = (ctypes.c_double * 4)(), ctypes.c_long(0)
+    agama_b200._native.check(lib.agama_actionPhaseTiming(0, ph5, ctypes.byref(np5)))
+    phase5 = {"prepare": ph5[0] / 8, "roots": ph5[2] / 8, "integrals": ph5[3] / 8}
     J5 = J5.clone()
     engine_res["actions5"] = (snap[:REF_SAMPLE["actions5"]].cpu().numpy(), J5[:REF_SAMPLE["actions5"]].cpu().numpy())
     out.append({"metric": "orbit-steps/s", "value": nst5 / (t5 / 1000), "unit": "accepted DOP853 steps/s",
@@ -368,7 +376,7 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
                                           FLOPS_SOURCE)})
     line5 = {"metric": "actions/s", "value": ORBIT5_ORBITS / (ta / 1000), "unit": "actions/s", "ms_per_step": ta,
              "config": "config 5: actions of the final snapshot of those orbits (action finder, plain FP64)",
-             "steps": 5, "warmup": 3, "gpu_launches_per_step": 3,
+             "steps": 5, "warmup": 3, "gpu_launches_per_step": 3, "phase_ms": phase5,
              "roofline": fp64_roofline("fudge kernels (3)", FLOPS["actions5"], "action", ORBIT5_ORBITS, ta, peak64,
                                        FLOPS_SOURCE)}
     out.append(line5)
@@ -711,19 +719,19 @@ def run_engine(args):
 # kernels per action step: prepare, root searches, integrals
 ACTION_LAUNCHES_PER_STEP = 3
 # executed FP64 flops per action (dadd + dmul + 2 dfma, ncu, config-2 workload, 200 000 particles):
-# prepare 3880, root searches 11014, integrals 9687
-FLOPS_ROOT_PER_ACTION_CFG2 = 11014.0
-FLOPS_PER_ACTION_CFG2 = 3880.0 + 11014.0 + 9687.0
-# dram read + write of one 200 000-particle step (prepare 11.21 + 4.43 MB, roots 36.06 + 25.31 MB,
-# integrals 26.01 + 0.00 MB), scaled to 1e6 particles (the traffic grows with the particles)
-TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 61.37e6
-TRAFFIC_PER_STEP_CFG2 = 5 * 103.02e6
+# prepare 3476, root searches 9962, integrals 8647
+FLOPS_ROOT_PER_ACTION_CFG2 = 9962.0
+FLOPS_PER_ACTION_CFG2 = 3476.0 + 9962.0 + 8647.0
+# dram read + write of one 200 000-particle step (prepare 11.45 + 19.11 MB, roots 35.35 + 4.06 MB,
+# integrals 26.09 + 0.02 MB), scaled to 1e6 particles (the traffic grows with the particles)
+TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 39.41e6
+TRAFFIC_PER_STEP_CFG2 = 5 * 96.08e6
 # executed FP64 flops (dadd + dmul + 2 dfma, ncu) per unit of the secondary workloads: per force
 # evaluation, per accepted DOP853 step (the rejected attempts' work included), per action
-# (bench.py --profile-case under ncu; profiles/secondary_workloads_flops.md): forces 1.856e8 / 1e5,
-# orbits 1.105e11 / 3 307 982, 3.917e11 / 9 784 415, 9.331e11 / 68 712 155 accepted steps, actions of
-# the config-5 snapshot (prepare + roots + integrals) 5.215e8 / 20 000
-FLOPS = {"forces1": 1856.0, "orbits1": 33404.0, "orbits3": 40033.0, "orbits5": 13580.0, "actions5": 26075.0}
+# (bench.py --profile-case under ncu; profiles/secondary_workloads_flops.md): forces 1.704e8 / 1e5,
+# orbits 1.022e11 / 3 307 982, 3.624e11 / 9 784 415, 8.629e11 / 68 712 155 accepted steps, actions of
+# the config-5 snapshot (prepare + roots + integrals) 4.685e8 / 20 000
+FLOPS = {"forces1": 1704.0, "orbits1": 30895.0, "orbits3": 37038.0, "orbits5": 12558.0, "actions5": 23427.0}
 FLOPS_SOURCE = "ncu FP64 instruction counts of the kernel on a case of this workload (bench.py --profile-case)"
 
 
