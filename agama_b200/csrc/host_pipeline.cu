@@ -105,11 +105,26 @@ void runChunked(long n, const std::vector<HostIn>& ins, const std::vector<HostOu
     const ChunkLaunch& launch, long chunk)
 {
     if(n <= 0) return;
-    // four chunks: each extra chunk adds the drain of its kernels (about 0.15 ms for the action
-    // phases on a B200), while the copy of the first chunk in and of the last one out stays exposed
-    if(chunk <= 0) chunk = std::min(MAX_CHUNK, std::max(MIN_CHUNK, (n + 3) / 4));
-    chunk = std::min(chunk, n);
-    const long numChunks = (n + chunk - 1) / chunk;
+    // chunk boundaries (a given chunk size, or the default below)
+    std::vector<long> bounds{ 0 };
+    if(chunk > 0) {
+        for(long f = chunk; f < n; f += chunk) bounds.push_back(f);
+    } else if(n >= 8 * MIN_CHUNK) {
+        // a short first chunk (its copy in is exposed) and chunks growing so that each copy in
+        // ends before the kernels of the previous chunk do; a short last chunk (its copy out is
+        // exposed): fractions 0.05, 0.20, 0.35, 0.30, 0.10 of n
+        const double frac[4] = { 0.05, 0.25, 0.60, 0.90 };
+        for(double f : frac) bounds.push_back(static_cast<long>(f * n));
+    } else {        // small batches: four chunks of at least MIN_CHUNK items
+        const long c = std::min(MAX_CHUNK, std::max(MIN_CHUNK, (n + 3) / 4));
+        for(long f = c; f < n; f += c) bounds.push_back(f);
+    }
+    bounds.push_back(n);
+    for(size_t k = 0; k + 1 < bounds.size(); k++)      // no chunk above the scratch bound
+        if(bounds[k + 1] - bounds[k] > MAX_CHUNK) { bounds.insert(bounds.begin() + k + 1, bounds[k] + MAX_CHUNK); }
+    const long numChunks = static_cast<long>(bounds.size()) - 1;
+    chunk = 0;
+    for(long c = 0; c < numChunks; c++) chunk = std::max(chunk, bounds[c + 1] - bounds[c]);
     const int slots = static_cast<int>(std::min<long>(NUM_STREAMS, numChunks));
     int device;
     AGB_CUDA(cudaGetDevice(&device));
@@ -130,7 +145,7 @@ void runChunked(long n, const std::vector<HostIn>& ins, const std::vector<HostOu
     std::vector<void*> dIn(ins.size()), dOut(outs.size());
     auto copyOut = [&](long c) {
         const int k = static_cast<int>(c % slots);
-        const long first = c * chunk, count = std::min(chunk, n - first);
+        const long first = bounds[c], count = bounds[c + 1] - bounds[c];
         for(size_t a = 0; a < outs.size(); a++)
             if(outs[a].host)
                 AGB_CUDA(cudaMemcpyAsync(static_cast<char*>(outs[a].host) + first * outs[a].itemBytes,
@@ -142,7 +157,7 @@ void runChunked(long n, const std::vector<HostIn>& ins, const std::vector<HostOu
     // the same stream, after its copy-out.
     for(long c = 0; c < numChunks; c++) {
         const int k = static_cast<int>(c % slots);
-        const long first = c * chunk, count = std::min(chunk, n - first);
+        const long first = bounds[c], count = bounds[c + 1] - bounds[c];
         cudaStream_t s = call.streams->s[k];
         for(size_t a = 0; a < ins.size(); a++) {
             dIn[a] = ins[a].host ? call.scratch[k] + inOff[a] : nullptr;
