@@ -380,8 +380,8 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
              "roofline": fp64_roofline("fudge kernels (3)", FLOPS["actions5"], "action", ORBIT5_ORBITS, ta, peak64,
                                        FLOPS_SOURCE)}
     out.append(line5)
-    # the north star's forms on the snapshot: the network trained on the orbits' initial points (the
-    # same distribution, other points), then used on the final points
+    # the mixed-precision and learned-bracket forms on the snapshot: the network trained on the
+    # orbits' initial points (the same distribution, other points), then used on the final points
     t0 = time.perf_counter()
     af5.train_brackets(ic5[:1000000], epochs=20, batch=2048, lr=2e-3, seed=1)
     ttrain5 = time.perf_counter() - t0
@@ -501,9 +501,9 @@ def run_bracket_modes(dev, flush, dist, af2, dpts2, J2plain):
 
 
 def action_mode_lines(agama_b200, timed, rel_err, af, d, Jplain, name, training):
-    """the same action batch in the north star's forms beside the plain FP64 one: mixed precision
-    (FP32 integrand arithmetic and compensated sums), learned root brackets (BF16 tcgen05 network +
-    FP64 searches), and both; each with its speed-up over plain FP64 and its error against it"""
+    """the same action batch in its mixed-precision and learned-bracket forms beside the plain FP64
+    one: mixed precision (FP32 integrand arithmetic and compensated sums), learned root brackets
+    (BF16 tcgen05 network + FP64 searches), and both; each with its speed-up over plain FP64 and its error against it"""
     n = d.shape[0]
     out = []
     af.use_brackets(False)
