@@ -1,6 +1,7 @@
 """Host-buffer batches are cut into chunks that overlap copies with kernels; their results must
 equal those of one device-pointer launch bit for bit, for pinned and pageable host arrays, with
-ragged last chunks and optional outputs left out."""
+ragged last chunks and optional outputs left out; batches of at least 524 288 items take five
+growing chunks, smaller ones four equal chunks."""
 import os
 
 import numpy as np
@@ -43,14 +44,16 @@ def test_potential_host_chunks_equal_device(n):
     assert np.allclose(-g, acc_h, rtol=1e-13, atol=1e-15 * np.max(np.abs(acc_h)))
 
 
-def test_actions_host_chunks_equal_device():
+@pytest.mark.parametrize("n", [65536 * 2 + 5, 600001])
+def test_actions_host_chunks_equal_device(n):
+    """n = 600001: the five growing chunks of large batches (5 % ... 10 % of the batch)"""
     import torch
     import agama_b200
     g = np.load(os.path.join(GOLDEN, "actions_cfg2.npz"))
     pot = agama_b200.Potential(file=os.path.join(GOLDEN, "cfg2.coef"))
     af = agama_b200.ActionFinder(pot)
     base = g["points"]
-    reps = (65536 * 2 + 5) // len(base) + 1
+    reps = n // len(base) + 1
     rng = np.random.default_rng(3)
     pts = np.ascontiguousarray(np.tile(base, (reps, 1)) * (1 + 1e-3 * rng.standard_normal((reps * len(base), 6))))
     J_h, fd_h = af(pts, fd=True)
