@@ -660,21 +660,27 @@ __device__ __forceinline__ void evalMultipoleCar(const MultipoleView& M, double 
     double* pot, double* grad, double* hess)
 {
     const double R2 = x * x + y * y, R = sqrt(R2);
+    // a potential with only m = 0 terms (its splines and both asymptotes): its evaluators neither
+    // read the azimuth nor give a phi derivative (exactly 0), so neither atan2 nor the azimuth's
+    // derivatives are formed (the results are the same bits)
+    const bool noAzimuth = KIND == EVAL_AXI && NQ <= 3 && M.ind.mmax == 0 && M.inner.ind.mmax == 0 &&
+                           M.outer.ind.mmax == 0;
     double phi, cphi, sphi;
-    double dRdx, dRdy, dphidx, dphidy;
+    double dRdx, dRdy, dphidx = 0, dphidy = 0;
     if(R == 0) {
         phi = 0; dRdx = dRdy = dphidx = dphidy = 1;
         cphi = sphi = 1;
     } else {
         cphi = x / R; sphi = y / R;
-        dRdx = cphi; dRdy = sphi; dphidx = -sphi / R; dphidy = cphi / R;
-        phi = atan2(y, x);
+        dRdx = cphi; dRdy = sphi;
+        if(!noAzimuth) { dphidx = -sphi / R; dphidy = cphi / R; }
+        phi = noAzimuth ? 0 : atan2(y, x);
     }
     CylDerivs g; CylHess h;
     evalMultipoleCyl<NQ, KIND, G, MIXED>(M, R, z, phi, pot, &g, &h);
     if(NQ >= 3) {
-        grad[0] = g.dR * dRdx + g.dphi * dphidx;
-        grad[1] = g.dR * dRdy + g.dphi * dphidy;
+        grad[0] = noAzimuth ? g.dR * dRdx : g.dR * dRdx + g.dphi * dphidx;
+        grad[1] = noAzimuth ? g.dR * dRdy : g.dR * dRdy + g.dphi * dphidy;
         grad[2] = g.dz;
     }
     if(NQ == 6) {
