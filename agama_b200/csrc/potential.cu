@@ -10,7 +10,7 @@ thread_local std::string g_error;
 /// One point per thread; 256 threads per block.  NQ = 1 (potential), 3 (+gradient), 6 (+Hessian);
 /// KIND = spline evaluator matching the potential (EvalKind).
 template<int NQ, int KIND>
-__global__ void __launch_bounds__(256) evalPotentialKernel(const MultipoleView M, long n,
+__global__ void __launch_bounds__(128) evalPotentialKernel(const MultipoleView M, long n,
     const double* __restrict__ pos, double* __restrict__ phi, double* __restrict__ grad,
     double* __restrict__ hess)
 {
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256) evalPotentialKernel(const MultipoleView M
 /// reference's BasePotentialCyl::evalCyl returns them (no round trip through Cartesian
 /// derivatives, which loses the phi derivatives to cancellation at large R)
 template<int NQ, int KIND>
-__global__ void __launch_bounds__(256) evalPotentialCylKernel(const MultipoleView M, long n,
+__global__ void __launch_bounds__(128) evalPotentialCylKernel(const MultipoleView M, long n,
     const double* __restrict__ pos, double* __restrict__ phi, double* __restrict__ grad,
     double* __restrict__ hess)
 {
@@ -63,7 +63,9 @@ void launchEvalPotential(const MultipoleView& M, long n, const double* pos, doub
     double* grad, double* hess, cudaStream_t stream, bool cylindrical)
 {
     if(n <= 0) return;
-    const int block = 256;
+    // 128 threads (up to 168 registers, no spills for the multi-harmonic kind): 16 % faster than
+    // blocks of 256 at 128 registers with spills (config 1 forces 0.055 against 0.065 ms)
+    const int block = 128;
     const long grid = (n + block - 1) / block;
     const int nq = hess ? 6 : grad ? 3 : 1, kind = evalKindOf(M);
 #define AGB_LAUNCH(NQ_, K_) \
