@@ -68,8 +68,10 @@ AGB_HD int binSearch(double x, const double* arr, int size)
 }
 
 /** binSearch with the first guess from scale = (size - 1) / (arr[size-1] - arr[0]), precomputed,
-    instead of a division: the guess only picks where the search starts, so the result is that of
-    binSearch. */
+    instead of a division, and up to three steps to a neighbouring segment before the bisection
+    (the grids are close to uniform: the guess is off by at most one or two segments); the guess
+    and the steps only choose where the search looks, so the result is that of binSearch (the last
+    segment whose left node is <= x). */
 AGB_HD int binSearchScaled(double x, const double* arr, int size, double scale)
 {
     if(size < 1 || !(x >= arr[0]))
@@ -79,9 +81,14 @@ AGB_HD int binSearchScaled(double x, const double* arr, int size, double scale)
     int lo = static_cast<int>((x - arr[0]) * scale);
     if(lo >= size - 1)
         return size - 2;
+    for(int step = 0; step < 3; step++) {
+        if(x < arr[lo]) lo--;                               // lo > 0 here, since x >= arr[0]
+        else if(lo < size - 2 && x >= arr[lo+1]) lo++;
+        else return lo;
+    }
     int hi = size - 1;
     if(x >= arr[lo]) {
-        if(x < arr[lo+1])
+        if(lo == size - 2 || x < arr[lo+1])
             return lo;
     } else {
         hi = lo;
