@@ -205,10 +205,14 @@ __device__ __forceinline__ void limitRootEval(const FudgeFunction& f, int kind, 
     }
 }
 
+/** The point's F(tau) from its record.  The azimuth given to the potential is 0: the fudge takes
+    only axisymmetric potentials, whose coefficients (and so the index sets of their splines and
+    asymptotes) have m = 0 alone, and their evaluators never read the azimuth; a constant leaves
+    the register free for the searches (the record keeps the point's azimuth for the angles). */
 __device__ __forceinline__ void loadFudgeFunction(const MultipoleView& M, const FudgeRecord& r, FudgeFunction& f)
 {
     f.M = &M;
-    f.lambda = r.lambda; f.nu = r.nu; f.phi = r.phi; f.D2 = r.D2;
+    f.lambda = r.lambda; f.nu = r.nu; f.phi = 0; f.D2 = r.D2;
     f.E = r.E; f.Lz = r.Lz; f.I3 = r.I3; f.flambda = r.flambda; f.fnu = r.fnu;
     f.bad = 0;
 }

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(ROOT_BLOCK, 4) fudgeRootKernel(const __grid_co
                 const long t = static_cast<long>(base) + __popc(need & ((1u << lane) - 1));
                 if(t >= total) drained = true;
                 else {
-                    const int k = static_cast<int>(t / n);
+                    const int k = t >= 2 * n ? 2 : t >= n ? 1 : 0;      // (no 64-bit division)
                     const long i = t - k * n;
                     const FudgeRecord& r = rec[i];
                     if(r.roots & (1 << k)) {
