@@ -101,7 +101,12 @@ struct FudgeFunction {
     const MultipoleView* M;
     double lambda, nu, phi, D2;     // point in prolate spheroidal coordinates (Delta^2 = D2)
     double E, Lz, I3, flambda, fnu;
+    double Ilam, Inu, L2h;          // I3 - fnu, I3 - flambda and Lz^2 / 2, formed once (derive())
     int bad;                        // set when a coordinate conversion is invalid
+
+    /// the terms of F that do not depend on tau, from the integrals of motion (the same
+    /// operations as in F itself, so the same bits)
+    __device__ void derive() { Ilam = I3 - fnu; Inu = I3 - flambda; L2h = Lz * Lz / 2; }
 
     /// F(tau) and optionally F', F'' (src/actions_staeckel.cpp:202-252); INL: the potential
     /// evaluation inlined at this call site instead of the shared out-of-line copy
@@ -109,8 +114,8 @@ struct FudgeFunction {
     __device__ void eval(double tau, double* val, double* der, double* der2) const
     {
         double lam, n, mult, I;
-        if(tau >= D2) { lam = tau; n = fabs(nu); mult = lam - n; I = I3 - fnu; }
-        else          { lam = lambda; n = tau; mult = n - lam; I = I3 - flambda; }
+        if(tau >= D2) { lam = tau; n = fabs(nu); mult = lam - n; I = Ilam; }
+        else          { lam = lambda; n = tau; mult = n - lam; I = Inu; }
         // prolate spheroidal -> cylindrical (src/coord.cpp:266-291)
         const double absnu = fabs(n), sgn = n >= 0 ? 1 : -1;
         const double lmd = lam - D2, nmd = absnu - D2;
@@ -127,7 +132,7 @@ struct FudgeFunction {
         else if(DER) evalMultipoleCylCall<3, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         else         evalMultipoleCylCall<1, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         const double tmd = tau - D2;
-        *val = (tmd != 0 ? (E * tau - I - Phi * mult) * tmd : 0) - Lz * Lz / 2 * tau;
+        *val = (tmd != 0 ? (E * tau - I - Phi * mult) * tmd : 0) - L2h * tau;
         if(DER || DER2) {
             // dR/dtau, dz/dtau along the coordinate that tau moves (lambda or nu): only that pair
             // is divided out
@@ -137,7 +142,7 @@ struct FudgeFunction {
             else        { dRdt = 0.5 * R / nmd * sgn; dzdt = 0.5 * z / n; }
             const double dPhidtau = g.dR * dRdt + g.dz * dzdt;
             if(DER)
-                *der = E * (tau + tmd) - Lz * Lz / 2 - I - (mult + tmd) * Phi -
+                *der = E * (tau + tmd) - L2h - I - (mult + tmd) * Phi -
                        (tmd != 0 ? tmd * mult * dPhidtau : 0);
             if(DER2) {
                 double d2;
@@ -214,6 +219,7 @@ __device__ __forceinline__ void loadFudgeFunction(const MultipoleView& M, const 
     f.M = &M;
     f.lambda = r.lambda; f.nu = r.nu; f.phi = 0; f.D2 = r.D2;
     f.E = r.E; f.Lz = r.Lz; f.I3 = r.I3; f.flambda = r.flambda; f.fnu = r.fnu;
+    f.derive();
     f.bad = 0;
 }
 
@@ -384,6 +390,7 @@ static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, do
     fnc.flambda = -lambda * Phi0;
     fnc.fnu = fnc.flambda + Phi * (lambda - absnu);
     fnc.I3 = lambda * (Phi - Phi0) + 0.5 * (pow2(z * vphi) + pow2(R * vz - z * vR) + pow2(vz) * D2);
+    fnc.derive();
     if(!isFinite(fnc.E + fnc.I3 + fnc.Lz) || fnc.E >= 0) { act[0] = act[1] = NAN; return; }
     rec.lambda = fnc.lambda; rec.nu = fnc.nu; rec.D2 = D2; rec.E = fnc.E; rec.Lz = Lz; rec.I3 = fnc.I3;
     rec.flambda = fnc.flambda; rec.fnu = fnc.fnu; rec.phi = phi;
