@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(PREPARE_BLOCK, 5) fudgePrepareKernel(const __g
     carToCylPosVel(w, pc);
     double Phi;
     CylDerivs g; CylHess h;
-    evalMultipoleCylCall<1, EVAL_AXI>(M, pc[0], pc[1], pc[2], &Phi, &g, &h);
+    evalMultipoleCylCall<1, EVAL_AXI>(M, pc[0], pc[1], 0, &Phi, &g, &h);   // axisymmetric: no azimuth
     const double delta = FINDER ? finderFocalDistance(F, pc, Phi) : (fd ? fd[i] : fd0);
     FudgeRecord r;
     double a[3];

@@ -378,12 +378,12 @@ static __device__ void fudgePrepare(const MultipoleView& M, const double* pc, do
     fnc.M = &M;
     fnc.lambda = lambda;
     fnc.nu = absnu * signz;
-    fnc.phi = phi;
+    fnc.phi = 0;                    // axisymmetric potential: its evaluators never read the azimuth
     fnc.D2 = D2;
     fnc.bad = 0;
     double Phi0;
     CylDerivs g; CylHess h;
-    evalMultipoleCylCall<1, EVAL_AXI>(M, sqrt(lambda - D2), 0, phi, &Phi0, &g, &h);
+    evalMultipoleCylCall<1, EVAL_AXI>(M, sqrt(lambda - D2), 0, 0, &Phi0, &g, &h);
     const double Ekin = 0.5 * (vR * vR + vz * vz + vphi * vphi);
     fnc.E = Phi + Ekin;
     fnc.Lz = Lz;

@@ -296,19 +296,28 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
     pot1, pts1, ic1, T1, pot3, ic3, T3 = secondary_workloads(Pot, lambda c: os.path.join(GOLDEN, c + ".coef"))
     stream = torch.cuda.current_stream(dev)
 
+    step_ms = {}
+
     def timed(fn, warmup, steps):
+        import gc
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         ms = []
-        for _ in range(steps):
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            r = fn()
-            b.record(stream)
-            torch.cuda.synchronize()
-            ms.append(a.elapsed_time(b))
+        gc.collect()            # no collection of the interpreter's heap inside a timed step
+        gc.disable()
+        try:
+            for _ in range(steps):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                r = fn()
+                b.record(stream)
+                torch.cuda.synchronize()
+                ms.append(a.elapsed_time(b))
+        finally:
+            gc.enable()
+        step_ms["last"] = ms
         t = float(np.mean(ms))
         t = max_over_ranks(t, dist, dev)
         return t, r
@@ -362,6 +371,7 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
     torch.cuda.synchronize()
     agama_b200._native.check(lib.agama_actionPhaseTiming(1, None, None))    # CUDA events around each phase
     ta, J5 = timed(lambda: af5(snap), 3, 5)
+    ms5 = list(step_ms["last"])
     ph5, np5 = (ctypes.c_double * 4)(), ctypes.c_long(0)
     agama_b200._native.check(lib.agama_actionPhaseTiming(0, ph5, ctypes.byref(np5)))
     phase5 = {"prepare": ph5[0] / 8, "roots": ph5[2] / 8, "integrals": ph5[3] / 8}
@@ -376,7 +386,7 @@ def run_engine_secondary(dev, flush, dist, cpu, peak64):
                                           FLOPS_SOURCE)})
     line5 = {"metric": "actions/s", "value": ORBIT5_ORBITS / (ta / 1000), "unit": "actions/s", "ms_per_step": ta,
              "config": "config 5: actions of the final snapshot of those orbits (action finder, plain FP64)",
-             "steps": 5, "warmup": 3, "gpu_launches_per_step": 3, "phase_ms": phase5,
+             "steps": 5, "warmup": 3, "gpu_launches_per_step": 3, "phase_ms": phase5, "ms_each_step": ms5,
              "roofline": fp64_roofline("fudge kernels (3)", FLOPS["actions5"], "action", ORBIT5_ORBITS, ta, peak64,
                                        FLOPS_SOURCE)}
     out.append(line5)
