@@ -127,7 +127,9 @@ struct FudgeFunction {
         const double z = sqrt(lam * absnu / D2) * sgn;
         double Phi;
         CylDerivs g; CylHess h;
-        if(INL)      evalMultipoleCyl<DER2 ? 6 : DER ? 3 : 1, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
+        // the inlined F, F' of the root searches: the cell evaluated in halves (fewer registers
+        // beside the searches' state, the same bits)
+        if(INL)      evalMultipoleCyl<DER2 ? 6 : DER ? 3 : 1, EVAL_AXI, 1, false, DER && !DER2>(*M, R, z, phi, &Phi, &g, &h);
         else if(DER2) evalMultipoleCylCall<6, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         else if(DER) evalMultipoleCylCall<3, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);
         else         evalMultipoleCylCall<1, EVAL_AXI>(*M, R, z, phi, &Phi, &g, &h);

@@ -266,7 +266,7 @@ __device__ void evalInterp1d(const MultipoleView& M, double R, double z, double 
     the requested derivatives.  Reference QuinticSpline2d::evalDeriv, src/math_spline.cpp:2535-2597
     (corner values shifted by one corner value to limit round-off).  xhi, yhi: the tabulated
     reciprocal widths of the cell. */
-template<int NQ>
+template<int NQ, bool SPLIT = false>
 __device__ __forceinline__ void spline2dCell(const double* tab, int nt, int xi, int yi,
     double x, double xl, double xh, double y, double yl, double yh, double xhi, double yhi,
     double* z, double* zx, double* zy, double* zxx, double* zxy, double* zyy)
@@ -276,23 +276,56 @@ __device__ __forceinline__ void spline2dCell(const double* tab, int nt, int xi, 
     const double* nul = nll + static_cast<size_t>(nt) * NODE_STRIDE;               // (xupp, ylow)
     const double* nuu = nul + NODE_STRIDE;                                         // (xupp, yupp)
     // node layout: 0 f, 1 fx, 2 fy, 3 fxx, 4 fxy, 5 fyy, 6 fxxy, 7 fxyy, 8 fxxyy (9: padding, not read)
-    double ll[9], lu[9], ul[9], uu[9];
-#pragma unroll
-    for(int q = 0; q < 4; q++) {
-        double2 a = ldg2(nll + 2 * q), b = ldg2(nlu + 2 * q), c = ldg2(nul + 2 * q), d = ldg2(nuu + 2 * q);
-        ll[2 * q] = a.x; ll[2 * q + 1] = a.y; lu[2 * q] = b.x; lu[2 * q + 1] = b.y;
-        ul[2 * q] = c.x; ul[2 * q + 1] = c.y; uu[2 * q] = d.x; uu[2 * q + 1] = d.y;
-    }
-    ll[8] = ldg(nll + 8); lu[8] = ldg(nlu + 8); ul[8] = ldg(nul + 8); uu[8] = ldg(nuu + 8);
-    const double off = x == xh ? (y == yh ? uu[0] : ul[0]) : (y == yh ? lu[0] : ll[0]);
-    const double fl[6]  = { ll[0] - off, ul[0] - off, ll[1], ul[1], ll[3], ul[3] };
-    const double fu[6]  = { lu[0] - off, uu[0] - off, lu[1], uu[1], lu[3], uu[3] };
-    const double f1l[6] = { ll[2], ul[2], ll[4], ul[4], ll[6], ul[6] };
-    const double f1u[6] = { lu[2], uu[2], lu[4], uu[4], lu[6], uu[6] };
-    const double f2l[6] = { ll[5], ul[5], ll[7], ul[7], ll[8], ul[8] };
-    const double f2u[6] = { lu[5], uu[5], lu[7], uu[7], lu[8], uu[8] };
     double F[6], dF[6], d2F[6];
-    quinticSegmentR<6>(y, yl, yh, yhi, fl, fu, f1l, f1u, f2l, f2u, F, NQ >= 3 ? dF : nullptr, NQ == 6 ? d2F : nullptr);
+    double off;
+    if constexpr(SPLIT) {
+        // the y-segments of the lower x nodes (components f, fx, fxx at xl) first, then those of
+        // the upper x nodes: half of the cell's values are live at a time (the upper nodes' loads
+        // wait for the lower half's first result); every component's arithmetic is unchanged.
+        // Fewer registers for callers that hold much state (the root searches); slower for the
+        // others, whose loads it serialises
+        off = x == xh ? (y == yh ? ldg(nuu) : ldg(nul)) : (y == yh ? ldg(nlu) : ldg(nll));
+        auto half = [&](const double* a0, const double* a1, int k0) {
+            double p[9], q[9];
+#pragma unroll
+            for(int m = 0; m < 4; m++) {
+                const double2 u = ldg2(a0 + 2 * m), v = ldg2(a1 + 2 * m);
+                p[2 * m] = u.x; p[2 * m + 1] = u.y; q[2 * m] = v.x; q[2 * m + 1] = v.y;
+            }
+            p[8] = ldg(a0 + 8); q[8] = ldg(a1 + 8);
+            const double fl[3]  = { p[0] - off, p[1], p[3] }, fu[3]  = { q[0] - off, q[1], q[3] };
+            const double f1l[3] = { p[2], p[4], p[6] },       f1u[3] = { q[2], q[4], q[6] };
+            const double f2l[3] = { p[5], p[7], p[8] },       f2u[3] = { q[5], q[7], q[8] };
+            double G[3], dG[3], d2G[3];
+            quinticSegmentR<3>(y, yl, yh, yhi, fl, fu, f1l, f1u, f2l, f2u, G, NQ >= 3 ? dG : nullptr, NQ == 6 ? d2G : nullptr);
+#pragma unroll
+            for(int c = 0; c < 3; c++) {
+                F[2 * c + k0] = G[c];
+                if(NQ >= 3) dF[2 * c + k0] = dG[c];
+                if(NQ == 6) d2F[2 * c + k0] = d2G[c];
+            }
+        };
+        half(nll, nlu, 0);
+        asm volatile("" : "+l"(nul), "+l"(nuu) : "d"(F[0]));
+        half(nul, nuu, 1);
+    } else {
+        double ll[9], lu[9], ul[9], uu[9];
+#pragma unroll
+        for(int q = 0; q < 4; q++) {
+            double2 a = ldg2(nll + 2 * q), b = ldg2(nlu + 2 * q), c = ldg2(nul + 2 * q), d = ldg2(nuu + 2 * q);
+            ll[2 * q] = a.x; ll[2 * q + 1] = a.y; lu[2 * q] = b.x; lu[2 * q + 1] = b.y;
+            ul[2 * q] = c.x; ul[2 * q + 1] = c.y; uu[2 * q] = d.x; uu[2 * q + 1] = d.y;
+        }
+        ll[8] = ldg(nll + 8); lu[8] = ldg(nlu + 8); ul[8] = ldg(nul + 8); uu[8] = ldg(nuu + 8);
+        off = x == xh ? (y == yh ? uu[0] : ul[0]) : (y == yh ? lu[0] : ll[0]);
+        const double fl[6]  = { ll[0] - off, ul[0] - off, ll[1], ul[1], ll[3], ul[3] };
+        const double fu[6]  = { lu[0] - off, uu[0] - off, lu[1], uu[1], lu[3], uu[3] };
+        const double f1l[6] = { ll[2], ul[2], ll[4], ul[4], ll[6], ul[6] };
+        const double f1u[6] = { lu[2], uu[2], lu[4], uu[4], lu[6], uu[6] };
+        const double f2l[6] = { ll[5], ul[5], ll[7], ul[7], ll[8], ul[8] };
+        const double f2u[6] = { lu[5], uu[5], lu[7], uu[7], lu[8], uu[8] };
+        quinticSegmentR<6>(y, yl, yh, yhi, fl, fu, f1l, f1u, f2l, f2u, F, NQ >= 3 ? dF : nullptr, NQ == 6 ? d2F : nullptr);
+    }
     quinticSegmentR<1>(x, xl, xh, xhi, &F[0], &F[1], &F[2], &F[3], &F[4], &F[5], z, zx, zxx);
     *z += off;
     if(NQ >= 3)
@@ -452,7 +485,7 @@ __device__ __forceinline__ unsigned groupMask()
     broadcast from lane 0, every scaled harmonic is then broadcast from the lane that evaluated
     it, and every lane forms the Fourier sums itself in the order m = 0, then ascending m.  The
     arithmetic of each harmonic and of the sums is that of G = 1, so every G gives the same bits. */
-template<int NQ, int MAXS, int G = 1, bool MIXED = false>
+template<int NQ, int MAXS, int G = 1, bool MIXED = false, bool SPLIT = false>
 __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
@@ -475,7 +508,7 @@ __device__ __forceinline__ void evalInterp2dFast(const MultipoleView& M, double 
                 spline2dCell32<NQ>(M.spl2d32 + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
                     &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
             else
-                spline2dCell<NQ>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
+                spline2dCell<NQ, SPLIT>(M.spl2d + M.fastSlot[s] * slotStride, M.nt, xs, ys, logr, xl, xh, tau, yl, yh,
                     xhi, yhi, &P[s], &Dr[s], &Dt[s], &Drr[s], &Drt[s], &Dtt[s]);
             if(!inside) P[s] = Dr[s] = Dt[s] = Drr[s] = Drt[s] = Dtt[s] = NAN;
         }
@@ -615,7 +648,7 @@ enum EvalKind {
     asymptote by radius (reference src/potential_multipole.cpp:1538-1548).
     NQ = 1 (value), 3 (+ gradient) or 6 (+ Hessian); KIND selects the spline evaluator
     (the host picks the instantiation that matches the potential). */
-template<int NQ, int KIND = EVAL_GENERAL, int G = 1, bool MIXED = false>
+template<int NQ, int KIND = EVAL_GENERAL, int G = 1, bool MIXED = false, bool SPLIT = false>
 __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double R, double z, double phi,
     double* pot, CylDerivs* g, CylHess* h)
 {
@@ -627,7 +660,7 @@ __device__ __forceinline__ void evalMultipoleCyl(const MultipoleView& M, double 
         evalPowerLaw<NQ>(M.outer, R, z, phi, pot, g, h);
     else if(M.is2d) {
         if(KIND == EVAL_AXI)
-            evalInterp2dFast<NQ, 1>(M, R, z, phi, pot, g, h);
+            evalInterp2dFast<NQ, 1, 1, false, SPLIT>(M, R, z, phi, pot, g, h);
         else if(KIND == EVAL_FAST)
             evalInterp2dFast<NQ, FAST_MAX_HARMONICS, G, MIXED>(M, R, z, phi, pot, g, h);
         else
