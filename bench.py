@@ -731,19 +731,19 @@ def run_engine(args):
 # kernels per action step: prepare, root searches, integrals
 ACTION_LAUNCHES_PER_STEP = 3
 # executed FP64 flops per action (dadd + dmul + 2 dfma, ncu, config-2 workload, 200 000 particles):
-# prepare 3476, root searches 9962, integrals 8647
-FLOPS_ROOT_PER_ACTION_CFG2 = 9962.0
-FLOPS_PER_ACTION_CFG2 = 3476.0 + 9962.0 + 8647.0
-# dram read + write of one 200 000-particle step (prepare 11.45 + 19.11 MB, roots 35.35 + 4.06 MB,
-# integrals 26.09 + 0.02 MB), scaled to 1e6 particles (the traffic grows with the particles)
-TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 39.41e6
-TRAFFIC_PER_STEP_CFG2 = 5 * 96.08e6
+# prepare 3485, root searches 10463, integrals 8612
+FLOPS_ROOT_PER_ACTION_CFG2 = 10463.0
+FLOPS_PER_ACTION_CFG2 = 3485.0 + 10463.0 + 8612.0
+# dram read + write of one 200 000-particle step (prepare 11.60 + 50.42 MB, roots 35.31 + 0.62 MB,
+# integrals 26.08 + 0.00 MB), scaled to 1e6 particles (the traffic grows with the particles)
+TRAFFIC_ROOT_PER_LAUNCH_CFG2 = 5 * 35.94e6
+TRAFFIC_PER_STEP_CFG2 = 5 * 124.03e6
 # executed FP64 flops (dadd + dmul + 2 dfma, ncu) per unit of the secondary workloads: per force
 # evaluation, per accepted DOP853 step (the rejected attempts' work included), per action
 # (bench.py --profile-case under ncu; profiles/secondary_workloads_flops.md): forces 1.704e8 / 1e5,
-# orbits 1.022e11 / 3 307 982, 3.624e11 / 9 784 415, 8.629e11 / 68 712 155 accepted steps, actions of
-# the config-5 snapshot (prepare + roots + integrals) 4.685e8 / 20 000
-FLOPS = {"forces1": 1704.0, "orbits1": 30895.0, "orbits3": 37038.0, "orbits5": 12558.0, "actions5": 23427.0}
+# orbits 1.022e11 / 3 307 982, 3.624e11 / 9 784 415, 7.621e11 / 68 712 155 accepted steps, actions of
+# the config-5 snapshot (prepare + roots + integrals) 4.802e8 / 20 000
+FLOPS = {"forces1": 1704.0, "orbits1": 30895.0, "orbits3": 37038.0, "orbits5": 11091.0, "actions5": 24009.0}
 FLOPS_SOURCE = "ncu FP64 instruction counts of the kernel on a case of this workload (bench.py --profile-case)"
 
 
