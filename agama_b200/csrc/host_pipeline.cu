@@ -64,6 +64,13 @@ cudaMemPool_t poolFor(int device)
     AGB_CUDA(cudaMemPoolCreate(&pool, &props));
     uint64_t threshold = UINT64_MAX;
     AGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    // a block freed on one stream is not handed to an allocation on another: such reuse makes
+    // the allocating stream wait for the freeing one, which serialised the chunks of a host-buffer
+    // call (each chunk's scratch on its own stream) instead of overlapping their kernels
+    int off = 0;
+    AGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseFollowEventDependencies, &off));
+    AGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &off));
+    AGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &off));
     g_pools[device] = pool;
     return pool;
 }
